@@ -1,0 +1,385 @@
+#!/usr/bin/env python
+"""Benchmark of the prox_rigid_bodies time step on B200: one JSON line on stdout (rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Workloads (synthetic, seeded; the shapes go through the reference-compatible set-up chain):
+  batch1024  1024 independent scenes, 8..256 bodies each (log-uniform), random boxes (side U(0.5, 2)) and spheres
+             (radius U(0.25, 1), 16 x 16 sweep) drawn from a 64 + 64 size pool, random orientations, density 1000,
+             mu U(0.2, 0.8) per scene, on a fixed ground box; SDF resolution 32; dt 0.01 (default)
+  mixed4096  one scene of 4096 bodies (16^3 lattice, spacing 1.2): alternating unit boxes and r = 0.5 spheres,
+             random orientations, density 1000, on a fixed ground box; SDF resolution 64
+  boxes64    one scene of 64 unit boxes (4^3 lattice, spacing 1.05, jitter +-0.02) on a 20 x 1 x 20 ground
+A step advances every scene of the workload by one semi-implicit time step.  Bodies start in the air; a
+pre-roll of --pre-roll untimed steps lets them land before warm-up and timing.  Every solve runs to the same
+complementarity residual (--tolerance, FP64) unless --termination merit selects the reference's merit test.
+The metric is scene-steps/s with the p50/p99 step latency.  Scenes do not exchange data: with --gpus N every
+rank steps its own copy of the workload (weak scaling, no collective on the data path) and the value is the
+total over the max-over-ranks time.
+
+--impl reference times the CPU restatement of the reference step (oracle/rb_oracle.c) on a bounded sample of
+the same workload on the host cores (one process per core for multi-scene workloads).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LAUNCHES_PER_STEP = 38          # kernels issued by one rb_step without post-stabilisation (rb_step.cu)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="batch1024", choices=["batch1024", "mixed4096", "boxes64"])
+    ap.add_argument("--scheme", default="rigid_gauss_seidel")
+    ap.add_argument("--termination", default="residual", choices=["residual", "merit"])
+    ap.add_argument("--tolerance", type=float, default=1e-6)
+    ap.add_argument("--pre-roll", type=int, default=60)
+    ap.add_argument("--plain-scenes", type=int, default=32, help="scenes of the one-scene-per-launch baseline")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
+    ap.add_argument("--cpu-scenes", type=int, default=16, help="scenes in the CPU baseline sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------------------------------------------
+# workloads
+# --------------------------------------------------------------------------------------------------------------
+def build_workload(name, device):
+    from rainbow_b200 import engine_io, scenes
+    if name == "batch1024":
+        arrays, params = scenes.batch_arrays(n_scenes=1024, seed=0, pool=64, resolution=32, device=device)
+        bodies = sum(len(a["body_mass"]) for a in arrays)
+        cfg = {"workload": "batch_1024_scenes", "scenes": 1024, "bodies": int(bodies), "bodies_per_scene": "8..256",
+               "shapes": "boxes side U(0.5,2), spheres r U(0.25,1) 16x16, pool 64+64", "sdf_resolution": 32,
+               "dt": 0.01}
+        return arrays, params, cfg, None
+    if name == "mixed4096":
+        engine = scenes.mixed_lattice(n=16, spacing=1.2, resolution=64, seed=0, device=device)
+        cfg = {"workload": "mixed_lattice_4096", "scenes": 1, "bodies": 4097,
+               "shapes": "box 1x1x1 / sphere r=0.5 16x16", "sdf_resolution": 64, "dt": 0.01}
+    else:
+        engine = scenes.box_lattice(n=4, spacing=1.05, jitter=0.02, resolution=32, seed=0, device=device)
+        cfg = {"workload": "box_lattice_64", "scenes": 1, "bodies": 65, "shapes": "box 1x1x1", "sdf_resolution": 32,
+               "dt": 0.01}
+    return [engine_io.scene_arrays(engine)], engine.params, cfg, engine
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.samples.append([v.strip() for v in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        num = lambda v: v.replace(".", "", 1).isdigit()  # noqa: E731
+        sm = [float(s[1]) for s in self.samples if len(s) > 2 and num(s[1])]
+        mx = [float(s[2]) for s in self.samples if len(s) > 2 and num(s[2])]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 5 + i and s[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# --------------------------------------------------------------------------------------------------------------
+# CPU baseline: the oracle (C restatement of the reference step), bounded sample
+# --------------------------------------------------------------------------------------------------------------
+def _cpu_worker(job):
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    scenes, scheme, tol_mode, tol, pre_roll, seconds = job
+    objs = [O.OracleScene(a) for a in scenes]
+    for sc in objs:
+        for _ in range(pre_roll):
+            sc.step(scheme=scheme, tol_mode=tol_mode, tol=tol)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        for sc in objs:
+            sc.step(scheme=scheme, tol_mode=tol_mode, tol=tol)
+            steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or steps >= 400:
+            break
+    return steps, el
+
+
+def cpu_baseline(arrays, args, workers):
+    """scene-steps/s of the oracle on the host: `workers` processes, each stepping its share of the sample."""
+    import multiprocessing as mp
+    from oracle import oracle as O
+    O.build()
+    tol_mode = 1 if args.termination == "residual" else 0
+    sample = arrays[:max(1, min(len(arrays), args.cpu_scenes))]
+    workers = max(1, min(workers, len(sample)))
+    jobs = [(sample[w::workers], args.scheme, tol_mode, args.tolerance, args.pre_roll, args.cpu_seconds)
+            for w in range(workers)]
+    if workers == 1:
+        res = [_cpu_worker(jobs[0])]
+    else:
+        with mp.get_context("spawn").Pool(workers) as pool:
+            res = pool.map(_cpu_worker, jobs)
+    steps = sum(r[0] for r in res)
+    el = max(r[1] for r in res)
+    return steps / el, {"cores": workers, "kind": "port",
+                        "sample": "%d scene(s) of the workload after a %d-step pre-roll, %d scene-steps in %.1f s on "
+                                  "%d process(es)" % (len(sample), args.pre_roll, steps, el, workers)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    workers = os.cpu_count() or 1
+    import torch
+    dev = "cuda:0" if torch.cuda.is_available() else "cpu"
+    arrays, params, cfg, _ = build_workload(args.workload, dev)
+    value, info = cpu_baseline(arrays, args, workers if len(arrays) > 1 else 1)
+    cfg.update({"scheme": args.scheme, "termination": args.termination, "tolerance": args.tolerance})
+    line = {
+        "impl": "reference", "metric": "scene-steps/s", "value": value, "unit": "scene-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": cfg,
+        "cpu_baseline": dict(value=value, unit="scene-steps/s", **info),
+        "e2e": {"value": value, "unit": "scene-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------------------------------------------
+# GPU
+# --------------------------------------------------------------------------------------------------------------
+def timed_steps(world, rp, steps, stream, flush):
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        flush.zero_()                      # evict L2 (126 MB) between timed steps
+        ev[k][0].record(stream)
+        world.launch(rp)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    return np.array([a.elapsed_time(b) for a, b in ev])   # ms
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    # the CPU baseline pool must exist before the first CUDA call
+    cpu_pool_workers = os.cpu_count() or 1
+    torch.cuda.set_device(local)
+    dev = "cuda:%d" % local
+    if world_size > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device(dev))
+    from rainbow_b200 import engine_io, world as W
+    from rainbow_b200.stepper import GpuStepper
+    arrays, params, cfg, engine = build_workload(args.workload, dev)
+    max_it = int(params.max_iterations)
+    world = W.DeviceWorld(arrays, device=dev, max_iterations=max_it)
+    kw = dict(scheme=args.scheme, termination=args.termination, residual_tolerance=args.tolerance)
+    rp = W.make_rb_params(params, **kw)
+    rp_prof = W.make_rb_params(params, profiling=True, **kw)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.pre_roll):
+        world.step(rp)
+    x0, u0 = world.state()                 # state the timed region (and every baseline) starts from
+    for _ in range(max(3, args.warmup)):
+        world.step(rp)
+    world.step(rp_prof)                    # phase split and byte accounting (outside the timed region)
+    phases = world.profile_times()
+    stats = world.stats()
+    world.set_state(x0, u0)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    if world_size > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    world.t_status.zero_()
+    with ClockSampler(local) as clocks:
+        times = timed_steps(world, rp, args.steps, stream, flush)
+    if world_size > 1:
+        dist.barrier()
+    status = int(world.t_status[0].item())
+    after = world.stats()
+    total_ms = float(times.sum())
+    if world_size > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    n_scenes = world.n_scenes
+    value = world_size * n_scenes * args.steps / (total_ms / 1000.0)
+    residuals = np.array([s.residual for s in after if s.n_contacts > 0])
+    unconverged = int(sum(1 for s in after if s.n_contacts > 0 and s.exitcode != 3)) \
+        if args.termination == "residual" else None
+
+    # plain one-scene-per-launch FP64 baseline (same scheme, same tolerance, same starting states)
+    plain = None
+    if n_scenes > 1:
+        x0r, u0r = x0.reshape(-1, 7), u0.reshape(-1, 6)
+        pts = []
+        for s in range(min(args.plain_scenes, n_scenes)):
+            b0, b1 = world.scene_start[s], world.scene_start[s + 1]
+            w1 = W.DeviceWorld(arrays[s], device=dev, max_iterations=max_it)
+            w1.set_state(x0r[b0:b1], u0r[b0:b1])
+            w1.step(rp)                    # sizes its work lists
+            w1.set_state(x0r[b0:b1], u0r[b0:b1])
+            torch.cuda.synchronize()
+            pts.append(timed_steps(w1, rp, args.steps, stream, flush))
+        pt = np.concatenate(pts)
+        plain = {"value": len(pt) / (pt.sum() / 1000.0), "unit": "scene-steps/s", "scenes_sampled": len(pts),
+                 "p50_ms": float(np.percentile(pt, 50)), "p99_ms": float(np.percentile(pt, 99)),
+                 "method": "each scene alone: one rb_step launch sequence per scene-step, FP64"}
+
+    # end to end through the public API, host buffers in and out every step
+    e2e = None
+    if not args.no_e2e:
+        if engine is not None:
+            engine_io.write_back(engine, x0.reshape(-1, 7), u0.reshape(-1, 6))
+            engine.stepper = GpuStepper(device=dev, termination=args.termination,
+                                        residual_tolerance=args.tolerance)
+            engine.params.proximal_solver = None if args.scheme == "rigid_gauss_seidel" else args.scheme
+            engine.stepper.step(engine.params.time_step, engine, False)
+            engine_io.write_back(engine, x0.reshape(-1, 7), u0.reshape(-1, 6))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                engine.stepper.step(engine.params.time_step, engine, False)
+            torch.cuda.synchronize()
+            el = time.perf_counter() - t0
+            K = len(engine.contact_points)
+            d2h = 13 * 8 * world.n_bodies + K * 64 + 8
+        else:
+            world.set_state(x0, u0)
+            hx, hu = x0.copy(), u0.copy()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                world.set_state(hx, hu)    # pinned host -> device
+                world.launch(rp)
+                hx, hu = world.state()     # device -> pinned host (synchronises)
+                st = world.t_stats.cpu()
+            el = time.perf_counter() - t0
+            d2h = 13 * 8 * world.n_bodies + st.numel()
+        if world_size > 1:
+            t = torch.tensor([el], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        e2e = {"value": world_size * n_scenes * args.steps / el, "unit": "scene-steps/s",
+               "h2d_bytes_per_step": 13 * 8 * world.n_bodies, "d2h_bytes_per_step": int(d2h),
+               "api": "GpuStepper.step via engine" if engine is not None else "DeviceWorld set_state/launch/state"}
+
+    # roofline of the dominant phase from the profiled step (event times on the launching stream)
+    K = sum(s.n_contacts for s in stats)
+    sweeps = sum(s.n_contacts * ((s.iterations + 1) if 0 <= s.iterations < max_it else max_it) for s in stats)
+    cand = sum(s.n_candidates for s in stats)
+    lookups = sum(s.n_grid_lookups for s in stats)
+    npairs = sum(s.n_pairs for s in stats)
+    resid_passes = sweeps if args.termination == "residual" else 0
+    alg = {
+        "contact_search": (phases[2], cand * (72 + 64) + lookups * 64,
+                           "per candidate triangle: 3 world vertices (72 B) + result record (64 B); 8 grid values "
+                           "(64 B) per signed distance lookup, lookups counted on the device"),
+        "solve": (phases[4], sweeps * 137 * 8 + resid_passes * 106 * 8,
+                  "per contact per sweep: J 48 + WJT 48 + b 4 + r 4 + mu 1 + x 8 + body w 24 doubles (1096 B); "
+                  "residual pass: J 48 + WJT 48 + b 4 + x 4 + mu 1 + w 1 doubles"),
+        "pairs_and_candidates": (phases[1], npairs * 2 * 48 + cand * 8,
+                                 "per body pair: 2 boxes (96 B); per candidate 8 B"),
+    }
+    dom = max(alg, key=lambda k: alg[k][0])
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        peaks = {}
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    dt_s, nbytes, model = alg[dom]
+    achieved = nbytes / dt_s / 1e9 if dt_s > 0 else 0.0
+
+    cpu = None
+    if rank == 0:
+        cv, info = cpu_baseline(arrays, args, cpu_pool_workers if n_scenes > 1 else 1)
+        cpu = dict(value=cv, unit="scene-steps/s", **info)
+
+    cfg.update({"scheme": args.scheme, "termination": args.termination, "tolerance": args.tolerance,
+                "precision": "fp64", "pre_roll_steps": args.pre_roll, "contacts_per_step": int(K),
+                "sweeps_per_step_contacts": int(sweeps), "l2": "256 MB buffer written between timed steps",
+                "parallelism": "replicas" if world_size > 1 else "single"})
+    line = {
+        "metric": "scene-steps/s", "value": value, "unit": "scene-steps/s", "n_gpus": world_size,
+        "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,
+        "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": cfg,
+        "plain": plain,
+        "speedup_vs_plain": (value / world_size) / plain["value"] if plain else None,
+        "residual": {"max": float(residuals.max()) if len(residuals) else 0.0,
+                     "median": float(np.median(residuals)) if len(residuals) else 0.0,
+                     "unconverged_scenes": unconverged},
+        "roofline": {"bound": "hbm", "kernel_phase": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "algorithmic_bytes": int(nbytes),
+                     "bytes_model": model, "phase_ms": dt_s * 1000.0,
+                     "peak_source": "of measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "of fallback 6650 GB/s"},
+        "phases_ms": {k: v * 1000.0 for k, v in zip(["bodies_bvh", "pairs_candidates", "contact_search", "dedup",
+                                                     "contact_setup_solve", "integrate", "total"], phases)},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+        "clocks": clocks.summary(),
+        "status": status,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world_size > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

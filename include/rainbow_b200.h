@@ -1,0 +1,209 @@
+/*
+ * rainbow_b200.h -- C ABI of the B200 (sm_100a) implementation of RAINBOW's prox_rigid_bodies time step.
+ *
+ * The reference step is the Python call chain
+ *     rainbow/simulators/prox_rigid_bodies/api.py:676 simulate(engine, T)
+ *       -> steppers.py:47 SemiImplicitStepper.step(dt, engine, profiling_on)
+ * A Python engine drives this library through ctypes (rainbow_b200/stepper.py, GpuStepper).  Every pointer
+ * inside the structs below is a DEVICE pointer owned by the caller (torch tensors in the Python host); the
+ * structs themselves live in host memory and are read during the call.  No entry point allocates device
+ * memory: per-step temporaries live in a caller-provided workspace of rb_workspace_bytes() bytes.
+ *
+ * All entry points return RB_OK (0) or a positive RB_ERR_* code; rb_last_error() describes the last failure
+ * of the calling thread.  Launch-time failures are reported synchronously; conditions only known on the
+ * device (capacity overflow, non-finite state, a solver that gave up) are written to rb_outputs.status and
+ * to the per-scene statistics, which the caller reads after synchronising the stream.
+ */
+#ifndef RAINBOW_B200_H
+#define RAINBOW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RB_ABI_VERSION 1
+
+/* return codes */
+#define RB_OK 0
+#define RB_ERR_ARG 1          /* a null pointer, a negative size or an inconsistent descriptor */
+#define RB_ERR_CUDA 2         /* a CUDA launch or API call failed */
+#define RB_ERR_WORKSPACE 3    /* workspace too small for the requested capacities */
+#define RB_ERR_UNSUPPORTED 4  /* a parameter combination this build does not implement */
+
+/* device status bits (rb_outputs.status[0]) */
+#define RB_STATUS_PAIR_OVERFLOW 1
+#define RB_STATUS_ITEM_OVERFLOW 2
+#define RB_STATUS_CONTACT_OVERFLOW 4
+#define RB_STATUS_NONFINITE 8
+#define RB_STATUS_NONUNIT_NORMAL 16
+#define RB_STATUS_MESH_TOO_LARGE 32   /* a shape has more than 16384 triangles */
+
+/* solver schemes (engine.params.proximal_solver) */
+#define RB_SCHEME_RIGID_GS 0          /* gauss_seidel_solver.py:14 + contacts.py:66 (the reference stepper) */
+#define RB_SCHEME_GS 1                /* proximal_contact/gauss_seidel_solver.py:8 GaussSeidelSolver */
+#define RB_SCHEME_JACOBI 2            /* proximal_contact/jacobi_solver.py:41 ParallelJacobiSolver */
+#define RB_SCHEME_JACOBI_HYBRID 3     /* proximal_contact/jacobi_solver.py:60 ParallelJacobiHybridSolver */
+#define RB_SCHEME_COLOURED_GS 4       /* graph-coloured Gauss-Seidel (proximal_contact/gauss_seidel_solver.py:89) */
+
+/* termination rules */
+#define RB_TERMINATE_MERIT 0          /* the reference's iterate-change merit (problem.py:53) */
+#define RB_TERMINATE_RESIDUAL 1       /* complementarity residual <= residual_tolerance */
+
+/* Shapes (rainbow/simulators/prox_rigid_bodies/types.py:82 Shape): body-frame mesh and signed distance grid. */
+typedef struct rb_shapes {
+    int32_t n_shapes;
+    const double* V;            /* 3 doubles per vertex, body frame (api.py:228-230) */
+    const int32_t* v_off;       /* n_shapes+1 vertex offsets */
+    const int32_t* T;           /* 3 shape-local vertex indices per triangle */
+    const int32_t* t_off;       /* n_shapes+1 triangle offsets */
+    const double* grid;         /* SDF node values, index i + I*(j + J*k) (grid3.py:71) */
+    const int64_t* g_off;       /* n_shapes+1 value offsets */
+    const double* grid_meta;    /* 12 doubles per shape: min[3], max[3], spacing[3], I, J, K (grid3.py:16) */
+} rb_shapes;
+
+/* Bodies of one or more independent scenes; scene s owns bodies scene_start[s] .. scene_start[s+1]-1 in the
+   reference's body order (engine.bodies insertion order = RigidBody.idx, api.py:67). */
+typedef struct rb_bodies {
+    int32_t n_bodies;
+    int32_t n_scenes;
+    const int32_t* scene_start;   /* n_scenes+1 */
+    const int32_t* shape;         /* shape index per body */
+    const double* mass;           /* types.py:111 RigidBody.mass */
+    const double* inertia;        /* 3 per body: body-frame principal inertia */
+    const uint8_t* fixed;         /* RigidBody.is_fixed */
+    const int32_t* material;      /* material index per body */
+    const int32_t* force_ptr;     /* n_bodies+1: connected forces per body (api.py:331 connect_force order) */
+    const int32_t* force_list;    /* global force indices */
+    int32_t n_forces;
+    const int32_t* scene_force_start; /* n_scenes+1: scene s owns forces scene_force_start[s].. (engine.forces) */
+    const int32_t* force_kind;    /* 0 = Gravity (types.py:189), 1 = Damping (types.py:224) */
+    const double* force_params;   /* 4 per force: gravity (g, up[3]); damping (alpha, beta, 0, 0) */
+    /* materials: body material indices are local to the scene; scene s owns an M_s x M_s interaction table
+       starting at entry scene_material_offset[s] (SurfacesInteractionLibrary.get_interaction, types.py:42) */
+    const int32_t* scene_material_offset;
+    const int32_t* scene_material_count;
+    const double* material_mu;    /* 3 per table entry: SurfacesInteraction.mu */
+    const double* material_eps;   /* 1 per table entry: SurfacesInteraction.epsilon */
+    /* topology derived from the shapes, fixed for the life of the scene (see rb_topology_sizes) */
+    int32_t n_body_vertices;      /* sum over bodies of their shape's vertex count */
+    int32_t n_body_triangles;     /* sum over bodies of their shape's triangle count */
+    int32_t n_clusters;           /* sum over bodies of ceil(triangles / 32) */
+    const int32_t* body_v0;       /* n_bodies+1 prefix sums of per-body vertex counts */
+    const int32_t* body_t0;       /* n_bodies+1 prefix sums of per-body triangle counts */
+    const int32_t* body_c0;       /* n_bodies+1 prefix sums of per-body 32-triangle cluster counts */
+    const int32_t* vert_body;     /* owning body of each body-vertex */
+    const int32_t* tri_body;      /* owning body of each body-triangle */
+    const int32_t* clu_body;      /* owning body of each cluster */
+    /* state, read at the start and written at the end of a step (state_storage.py:43-68 layout) */
+    double* x;                    /* 7 per body: r[3], q[4] */
+    double* u;                    /* 6 per body: v[3], w[3] */
+} rb_bodies;
+
+/* Capacities of the per-step work lists.  Exceeding one sets a status bit; the step then leaves x and u
+   untouched so the caller can grow the workspace and repeat it. */
+typedef struct rb_caps {
+    int32_t pair_capacity;        /* body pairs whose bounding boxes overlap */
+    int32_t item_capacity;        /* candidate triangles sent to the Frank-Wolfe search */
+    int32_t contact_capacity;     /* contacts before duplicate removal */
+    int32_t max_iterations;       /* solver iteration cap (length of each scene's residual history) */
+} rb_caps;
+
+/* Parameters (types.py:356 Parameters) plus the solver options of this implementation. */
+typedef struct rb_params {
+    double dt;
+    int32_t max_iterations;
+    int32_t use_bounce;
+    int32_t use_pre_stabilization;
+    int32_t use_post_stabilization;
+    double gap_reduction;
+    double min_gap_value;
+    double max_gap_value;
+    double absolute_tolerance;
+    double relative_tolerance;
+    double nu_reduce;
+    double nu_increase;
+    double too_small_merit_change;
+    int32_t contact_optimization_max_iterations;
+    double contact_optimization_tolerance;
+    double envelope;
+    int32_t scheme;               /* RB_SCHEME_* */
+    int32_t termination;          /* RB_TERMINATE_* */
+    double residual_tolerance;    /* used by RB_TERMINATE_RESIDUAL */
+    int32_t profiling;            /* nonzero: fill energies and residual histories */
+} rb_params;
+
+/* Per-scene results of one step. */
+typedef struct rb_scene_stats {
+    int32_t n_contacts;           /* after duplicate removal (collision_detection.py:255) */
+    int32_t contact_start;        /* first contact of this scene in the contact outputs */
+    int32_t iterations;           /* gauss_seidel_solver.py:471-489 'iterations' */
+    int32_t exitcode;             /* 0 not converged, 1 absolute, 2 relative, 3 residual */
+    int32_t post_iterations;
+    int32_t post_exitcode;
+    int32_t n_pairs;              /* body pairs with overlapping bounding boxes */
+    int32_t n_candidates;         /* triangles searched */
+    int32_t n_leaf_overlaps;      /* overlapping leaf (triangle) pairs: the profile key number_of_overlaps */
+    int32_t n_grid_lookups;       /* signed distance lookups of the contact search (profiling only) */
+    double merit;                 /* last global merit */
+    double residual;              /* complementarity residual of the returned solution (when computed) */
+    double kinetic_energy;        /* state_storage.py:188 (profiling only) */
+    double potential_energy;
+    double max_penetration;       /* contacts.py:222 */
+} rb_scene_stats;
+
+/* Outputs: device buffers sized by rb_caps.contact_capacity / n_scenes / max_iterations. */
+typedef struct rb_outputs {
+    int32_t* contact_ids;         /* 2 per contact: bodyA (SDF owner), bodyB (mesh owner), global body indices */
+    double* contact_p;            /* 3 per contact, world frame */
+    double* contact_n;            /* 3 per contact, unit normal */
+    double* contact_g;            /* gap (SDF value) */
+    double* contact_sol;          /* 4 per contact: solver result (n, s, t, tau impulses) */
+    rb_scene_stats* stats;        /* n_scenes */
+    double* residuals;            /* n_scenes * max_iterations (profiling), may be NULL */
+    int32_t* status;              /* 1 int32: RB_STATUS_* bits, OR-ed by the step (caller zeroes it) */
+    int32_t* n_contacts_total;    /* 1 int32 */
+} rb_outputs;
+
+/* Library ABI version (RB_ABI_VERSION). */
+int rb_abi_version(void);
+
+/* Description of the last error on the calling thread. */
+const char* rb_last_error(void);
+
+/* Sizes of the derived topology arrays of rb_bodies for the given per-body shape assignment (host arrays):
+   out[0] = total body-vertices, out[1] = total body-triangles, out[2] = total clusters. */
+int rb_topology_sizes(int32_t n_bodies, const int32_t* body_shape_host, int32_t n_shapes,
+                      const int32_t* v_off_host, const int32_t* t_off_host, int64_t* out);
+
+/* Workspace bytes needed by rb_step for these bodies and capacities.
+   Replaces the host-side temporaries the reference builds each step (state_storage.py:43, contacts.py:31). */
+int rb_workspace_bytes(const rb_bodies* bodies, const rb_caps* caps, size_t* bytes);
+
+/* One semi-implicit time step of every scene in `bodies` on `stream` (a cudaStream_t, NULL = default).
+   Replaces steppers.py:47 SemiImplicitStepper.step: forces and inverse mass (state_storage.py:43), collision
+   detection (collision_detection.py:293), contact problem (contacts.py:31), proximal solve
+   (gauss_seidel_solver.py:14 or the proximal_contact scheme in params->scheme), velocity and position update
+   (state_storage.py:239-302) and optional post-stabilisation (steppers.py:15).  Asynchronous. */
+int rb_step(const rb_shapes* shapes, const rb_bodies* bodies, const rb_caps* caps, const rb_params* params,
+            const rb_outputs* out, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Phase times (milliseconds) of the last rb_step issued with params->profiling on this thread, after waiting
+   for it: out[0] bounding volumes (steppers.py 'update_bvh'), out[1] body pairs and triangle candidates
+   ('narrow_phase'), out[2] Frank-Wolfe contact search ('contact_determination'), out[3] duplicate removal
+   ('contact_point_reduction'), out[4] contact problem set-up and solve ('solver_time'), out[5] integration and
+   post-stabilisation, out[6] the whole step.  Returns RB_ERR_ARG if no profiled step was issued. */
+int rb_profile_times(float* out, int32_t n);
+
+/* Signed distance grid of a closed triangle mesh (replaces grid3.py:320 create_signed_distance's call to
+   igl.signed_distance at grid3.py:338): values[i + I*(j + J*k)] for nodes min + spacing*(i,j,k).
+   Unsigned distance by closest point on each triangle, sign by the generalized winding number. */
+int rb_signed_distance_grid(const double* V, int32_t n_vertices, const int32_t* T, int32_t n_triangles,
+                            const double* grid_meta, double* values, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RAINBOW_B200_H */

@@ -453,13 +453,18 @@ static void run_collision_detection(const OScene* sc, const double* params, cons
             /* The tandem traversal reports exactly the overlapping leaf pairs, because every inner volume is the
                exact union of its children.  np.unique of each column gives the ascending triangle sets. */
             uint8_t* hitB = (uint8_t*)calloc((size_t)tb + 1, 1);
+            /* only leaves that overlap the other body's root can overlap one of its leaves */
+            int nbr = 0;
+            for (int64_t j = 0; j < tb; ++j)
+                if (aabb_overlap(leaf + body_t0[B] + j, root + A)) candB[nbr++] = (int32_t)j;
             int na = 0;
             int64_t overlaps = 0;
             for (int64_t i = 0; i < ta; ++i) {
                 const AABB* la = leaf + body_t0[A] + i;
                 if (!aabb_overlap(la, root + B)) continue;
                 int hit = 0;
-                for (int64_t j = 0; j < tb; ++j) {
+                for (int e = 0; e < nbr; ++e) {
+                    const int64_t j = candB[e];
                     if (aabb_overlap(la, leaf + body_t0[B] + j)) { hit = 1; hitB[j] = 1; ++overlaps; }
                 }
                 if (hit) candA[na++] = (int32_t)i;
@@ -848,7 +853,8 @@ static inline double merit_inf(const double* x, const double* sol, int n) {
 
 /* gauss_seidel_solver.py:14 solve, for a single problem (contacts or post-stabilisation) */
 static void solve_rigid(const Problem* P, const double* params, double* r, const double* b, const double* mu,
-                        double* x, double* sol, double* residuals, int* iterations, int* exitcode, int normal_only) {
+                        double* x, double* sol, double* residuals, int* iterations, int* exitcode, int normal_only,
+                        int tol_mode, double tol) {
     const int n = 4 * P->K, max_it = (int)params[P_MAX_ITER];
     double* w = (double*)malloc(sizeof(double) * 6 * (P->N ? P->N : 1));
     double last_merit = INFINITY, global_last = INFINITY;
@@ -857,6 +863,21 @@ static void solve_rigid(const Problem* P, const double* params, double* r, const
         double global_merit = 0.0;
         sweep_gs(P, r, b, mu, x, w, normal_only);
         double merit = merit_inf(x, sol, n);
+        if (tol_mode == 1) {   /* stop on the complementarity residual only; merit still adapts r */
+            double res = complementarity_residual(P, b, mu, x, w);
+            if (residuals) residuals[it] = res;
+            if (res <= tol) { memcpy(sol, x, sizeof(double) * n); *iterations = it; *exitcode = 3; break; }
+            if (merit > last_merit) {
+                for (int i = 0; i < n; ++i) r[i] = params[P_NU_REDUCE] * r[i];
+                memcpy(x, sol, sizeof(double) * n);
+            } else {
+                memcpy(sol, x, sizeof(double) * n);
+                if (last_merit - merit < params[P_TOO_SMALL])
+                    for (int i = 0; i < n; ++i) r[i] = params[P_NU_INCREASE] * r[i];
+                last_merit = merit;
+            }
+            continue;
+        }
         if (merit > last_merit) {
             for (int i = 0; i < n; ++i) r[i] = params[P_NU_REDUCE] * r[i];
             memcpy(x, sol, sizeof(double) * n);
@@ -1094,7 +1115,7 @@ int rbo_step(const OScene* sc, const double* params, double dt, double* r, doubl
 
         int iters = 0, exitc = 0;
         if (out->scheme == S_RIGID_GS) {
-            solve_rigid(&P, params, rr, b, mu, x, sol, out->residuals, &iters, &exitc, 0);
+            solve_rigid(&P, params, rr, b, mu, x, sol, out->residuals, &iters, &exitc, 0, tol_mode, tol);
         } else {
             int32_t* colour = NULL; int32_t* cptr = NULL; int32_t* clist = NULL; int nc = 0;
             if (out->scheme == S_COLOURED_GS) {
@@ -1134,7 +1155,7 @@ int rbo_step(const OScene* sc, const double* params, double dt, double* r, doubl
             double* ps = (double*)calloc((size_t)4 * K, sizeof(double));
             for (int i = 0; i < 4 * K; ++i) pr[i] = 1.0 / diag[i];
             int it2 = 0, ex2 = 0;
-            solve_rigid(&P, params, pr, g, mu, px, ps, NULL, &it2, &ex2, 1);
+            solve_rigid(&P, params, pr, g, mu, px, ps, NULL, &it2, &ex2, 1, 0, 0.0);
             out->post_iterations = it2; out->post_exitcode = ex2;
             double* dr = (double*)malloc(sizeof(double) * 6 * N);
             wjt_dot(&P, ps, dr);

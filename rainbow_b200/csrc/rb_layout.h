@@ -1,0 +1,90 @@
+// rb_layout.h -- carving of the caller-provided workspace into the per-step arrays.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <type_traits>
+
+#include "rainbow_b200.h"
+
+namespace rb {
+
+constexpr int kMaxClustersPerShape = 512;   // 16384 triangles per shape (mid-phase cluster masks in shared memory)
+constexpr int kScanBlocks = 1024;           // partial sums of the device-wide scans
+
+struct Workspace {
+    // per body
+    double* Winv;        // 9N world-frame inverse inertia
+    double* dux;         // 6N  W f_ext
+    double* du;          // 6N  velocity change of the step
+    double* root;        // 6N  body bounding box (lo, hi)
+    double* w;           // 6N  WJT x accumulator of the solver
+    double* w2;          // 6N  second accumulator (Jacobi / residual)
+    int32_t* pair_cnt;   // N+1 overlapping pairs per body -> offsets
+    int32_t* bc_ptr;     // N+1 contacts per body -> offsets
+    int32_t* bc_fill;    // N
+    // per body-vertex / triangle / cluster
+    double* Vw;          // 3 NV world vertices
+    double* leaf;        // 6 NT leaf boxes
+    double* clu;         // 6 NC cluster boxes
+    // pairs
+    int32_t* pairs;      // 2P
+    int32_t* pair_items; // P+1 candidate triangles per pair -> offsets
+    int32_t* pair_itemsA;// P   of which from side A
+    int32_t* pair_cont;  // P+1 contacts per pair -> offsets
+    int32_t* pair_ovl;   // P   overlapping leaf pairs per pair (profiling statistic)
+    // items
+    int32_t* item_pair;  // C
+    int32_t* item_tri;   // C  side << 31 | triangle
+    int32_t* item_flag;  // C
+    double* item_p;      // 3C
+    double* item_n;      // 3C
+    double* item_g;      // C
+    // contacts
+    int32_t* lohi;       // 2K
+    int32_t* c_scene;    // K
+    int32_t* bc_list;    // 2K
+    double* J;           // 48K
+    double* WJT;         // 48K
+    double* b;           // 4K
+    double* diag;        // 4K
+    double* r;           // 4K
+    double* x;           // 4K
+    double* xold;        // 4K
+    double* mu;          // K
+    // scans and counters
+    int32_t* scan_tmp;   // kScanBlocks + 1
+    int32_t* counters;   // 16
+};
+
+enum Counter { kNPairs = 0, kNItems = 1, kNRaw = 2, kNContacts = 3 };
+
+inline size_t align_up(size_t v) { return (v + 255) & ~size_t(255); }
+
+// Computes (and, when base != nullptr, assigns) every array; returns the total bytes.
+inline size_t layout(Workspace* ws, char* base, int64_t N, int64_t NV, int64_t NT, int64_t NC, int64_t P,
+                     int64_t C, int64_t K) {
+    size_t off = 0;
+    auto take = [&](auto*& ptr, int64_t count) {
+        using T = std::remove_reference_t<decltype(*ptr)>;
+        size_t bytes = align_up(sizeof(T) * (size_t)(count > 0 ? count : 1));
+        if (base) ptr = reinterpret_cast<T*>(base + off);
+        off += bytes;
+    };
+    Workspace dummy;
+    Workspace* w = ws ? ws : &dummy;
+    take(w->Winv, 9 * N); take(w->dux, 6 * N); take(w->du, 6 * N); take(w->root, 6 * N);
+    take(w->w, 6 * N); take(w->w2, 6 * N);
+    take(w->pair_cnt, N + 1); take(w->bc_ptr, N + 1); take(w->bc_fill, N);
+    take(w->Vw, 3 * NV); take(w->leaf, 6 * NT); take(w->clu, 6 * NC);
+    take(w->pairs, 2 * P); take(w->pair_items, P + 1); take(w->pair_itemsA, P); take(w->pair_cont, P + 1); take(w->pair_ovl, P);
+    take(w->item_pair, C); take(w->item_tri, C); take(w->item_flag, C);
+    take(w->item_p, 3 * C); take(w->item_n, 3 * C); take(w->item_g, C);
+    take(w->lohi, 2 * K); take(w->c_scene, K); take(w->bc_list, 2 * K);
+    take(w->J, 48 * K); take(w->WJT, 48 * K);
+    take(w->b, 4 * K); take(w->diag, 4 * K); take(w->r, 4 * K); take(w->x, 4 * K); take(w->xold, 4 * K);
+    take(w->mu, K);
+    take(w->scan_tmp, kScanBlocks + 1); take(w->counters, 16);
+    return off;
+}
+
+}  // namespace rb

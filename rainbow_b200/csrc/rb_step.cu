@@ -1,0 +1,1257 @@
+// rb_step.cu -- the prox_rigid_bodies semi-implicit time step on sm_100a.
+//
+// One rb_step call advances every scene of an rb_bodies batch by one step.  The pipeline (one kernel per
+// stage, all on the caller's stream, no host synchronisation, so a sequence of steps can be captured in a
+// CUDA graph) follows steppers.py:47 SemiImplicitStepper.step:
+//
+//   k_bodies          forces, gyroscopic torque, world inverse inertia, W f_ext      state_storage.py:43-185
+//   k_world_vertices  rotate_array(q, V) + r for every body vertex                   collision_detection.py:32
+//   k_clusters        leaf boxes (k-DOP K=3 + envelope), 32-leaf cluster boxes        kdop_bvh.py:52, kdop.py:53
+//   k_roots           body boxes (the BVH root)                                         kdop_bvh.py:215
+//   k_pairs           body pairs in combinations() order whose roots overlap           collision_detection.py:70
+//   k_mid             per pair, the triangles of each side whose leaf overlaps a leaf   kdop_bvh.py:127, :234
+//                     of the other side (ascending, = np.unique of the traversal)      collision_detection.py:234
+//   k_narrow          Frank-Wolfe deepest point on each candidate triangle in the       collision_detection.py:87
+//                     other body's SDF, contact emission
+//   k_dedup           first-occurrence duplicate removal and compaction                 collision_detection.py:255
+//   k_contacts        contact frame, Jacobian, W J^T, b, Delassus diagonal, r, mu        contacts.py:31-55
+//   k_solve           proximal solver (one block per scene)                             gauss_seidel_solver.py:14
+//   k_integrate       u += dt W f + W J^T sol; r, q update                               state_storage.py:239-302
+//   k_post_*          post-stabilisation                                                steppers.py:15
+//
+// Counts that are only known on the device (pairs, candidates, contacts) are read by the consumers from
+// device counters; kernels that depend on them run grid-stride loops over those counters.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "rainbow_b200.h"
+#include "rb_device.cuh"
+#include "rb_layout.h"
+
+namespace rb {
+
+constexpr int kWarpsPerBlock = 4;
+constexpr int kBlock = 32 * kWarpsPerBlock;
+constexpr int kAbort = 15;   // counters[kAbort]: nonzero once a capacity was exceeded
+
+// ---------------------------------------------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ int scene_of(const int32_t* scene_start, int n_scenes, int body) {
+    int lo = 0, hi = n_scenes;   // find s with scene_start[s] <= body < scene_start[s+1]
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(scene_start + mid) <= body) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// device-wide exclusive scan of int32 counts (three phases; the element count may live on the device)
+// data[0..n) -> exclusive prefix sums, data[n] = total, *total_out = total
+// ---------------------------------------------------------------------------------------------------------
+// with a device count, n_host is the capacity the count is clamped to
+__device__ __forceinline__ int scan_n(const int32_t* n_dev, int n_host) { return n_dev ? min(*n_dev, n_host) : n_host; }
+
+__global__ void k_scan_reduce(const int32_t* __restrict__ data, const int32_t* n_dev, int n_host,
+                              int32_t* __restrict__ partial) {
+    const int n = scan_n(n_dev, n_host);
+    const int chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int start = blockIdx.x * chunk, end = min(n, start + chunk);
+    int s = 0;
+    for (int i = start + threadIdx.x; i < end; i += blockDim.x) s += data[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ int ws[32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += ws[w];
+        partial[blockIdx.x] = t;
+    }
+}
+__global__ void k_scan_top(int32_t* __restrict__ partial, int nblocks, int32_t* total_out) {
+    // single block of 1024 threads, nblocks <= 1024
+    __shared__ int s[1024];
+    const int t = threadIdx.x;
+    int v = t < nblocks ? partial[t] : 0;
+    s[t] = v;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        int a = t >= o ? s[t - o] : 0;
+        __syncthreads();
+        s[t] += a;
+        __syncthreads();
+    }
+    if (t < nblocks) partial[t] = s[t] - v;
+    if (t == 1023) { partial[nblocks] = s[t]; if (total_out) *total_out = s[t]; }
+}
+__global__ void k_scan_down(int32_t* __restrict__ data, const int32_t* n_dev, int n_host,
+                            const int32_t* __restrict__ partial) {
+    const int n = scan_n(n_dev, n_host);
+    const int chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int start = blockIdx.x * chunk, end = min(n, start + chunk);
+    __shared__ int ws[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = partial[blockIdx.x];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int base = start; base < end; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int v = i < end ? data[i] : 0;
+        int incl = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            int a = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += a;
+        }
+        if (lane == 31) ws[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            int wv = lane < nw ? ws[lane] : 0;
+            int wi = wv;
+            for (int o = 1; o < 32; o <<= 1) {
+                int a = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += a;
+            }
+            if (lane < nw) ws[lane] = wi - wv;
+        }
+        __syncthreads();
+        const int c = carry;
+        if (i < end) data[i] = c + ws[wid] + incl - v;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = c + ws[wid] + incl;
+        __syncthreads();
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) data[n] = partial[gridDim.x];
+}
+static void scan(int32_t* data, const int32_t* n_dev, int n_host, int32_t* partial, int32_t* total_out,
+                 cudaStream_t st) {
+    const int G = 592;   // 4 x 148 SMs
+    k_scan_reduce<<<G, 256, 0, st>>>(data, n_dev, n_host, partial);
+    k_scan_top<<<1, 1024, 0, st>>>(partial, G, total_out);
+    k_scan_down<<<G, 256, 0, st>>>(data, n_dev, n_host, partial);
+}
+
+__global__ void k_zero_i32(int32_t* p, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = 0;
+}
+struct StepArgs;
+// capacity check after a scan: a total above the capacity aborts the rest of the step
+__global__ void k_check(int32_t* counters, int which, int cap, int bit, int32_t* status) {
+    if (counters[which] > cap) {
+        atomicOr(counters + kAbort, bit);
+        atomicOr(status, bit);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// bodies: state_storage.py:108 _compute_total_external_forces, :158 _compute_inverse_mass_matrix, :53
+// ---------------------------------------------------------------------------------------------------------
+struct StepArgs {
+    rb_shapes sh;
+    rb_bodies bd;
+    rb_caps caps;
+    rb_params pr;
+    rb_outputs out;
+    Workspace ws;
+};
+
+__global__ void k_bodies(const StepArgs a) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= a.bd.n_bodies) return;
+    double* d = a.ws.dux + 6 * b;
+    double* du = a.ws.du + 6 * b;
+    double* Wi = a.ws.Winv + 9 * b;
+    if (a.bd.fixed[b]) {
+        for (int i = 0; i < 6; ++i) { d[i] = 0.0; du[i] = 0.0; }
+        for (int i = 0; i < 9; ++i) Wi[i] = 0.0;
+        return;
+    }
+    const double* q = a.bd.x + 7 * b + 3;
+    const d3 v = ld3(a.bd.u + 6 * b), w = ld3(a.bd.u + 6 * b + 3);
+    double R[9], Iw[9], Ib[3], Binv[3];
+    quat_to_matrix(q, R);
+    for (int i = 0; i < 3; ++i) Ib[i] = a.bd.inertia[3 * b + i];
+    update_inertia_tensor(R, Ib, Iw);
+    const d3 c = cross_np(w, gemv3_np(Iw, w));
+    double T[3] = {-c.x, -c.y, -c.z}, F[3] = {0.0, 0.0, 0.0};
+    const double mass = a.bd.mass[b];
+    for (int e = a.bd.force_ptr[b]; e < a.bd.force_ptr[b + 1]; ++e) {
+        const int f = a.bd.force_list[e];
+        const double* fp = a.bd.force_params + 4 * f;
+        double Fi[3], Ti[3];
+        if (a.bd.force_kind[f] == 0) {          // types.py:204 Gravity.compute: F = -m g up
+            const double s = -mass * fp[0];
+            Fi[0] = s * fp[1]; Fi[1] = s * fp[2]; Fi[2] = s * fp[3];
+            Ti[0] = 0.0; Ti[1] = 0.0; Ti[2] = 0.0;
+        } else {                                 // types.py:239 Damping.compute: F = -v alpha, T = -w beta
+            Fi[0] = -v.x * fp[0]; Fi[1] = -v.y * fp[0]; Fi[2] = -v.z * fp[0];
+            Ti[0] = -w.x * fp[1]; Ti[1] = -w.y * fp[1]; Ti[2] = -w.z * fp[1];
+        }
+        for (int i = 0; i < 3; ++i) { F[i] = F[i] + Fi[i]; T[i] = T[i] + Ti[i]; }
+    }
+    const double m = 1.0 / mass;
+    for (int i = 0; i < 3; ++i) Binv[i] = 1.0 / Ib[i];
+    update_inertia_tensor(R, Binv, Wi);
+    const double dt = a.pr.dt;
+    for (int i = 0; i < 3; ++i) {   // bsr_matvec over the 3x3 blocks of W
+        double s = 0.0;
+        s += (i == 0 ? m : 0.0) * F[0];
+        s += (i == 1 ? m : 0.0) * F[1];
+        s += (i == 2 ? m : 0.0) * F[2];
+        double t = 0.0;
+        t += Wi[3 * i] * T[0];
+        t += Wi[3 * i + 1] * T[1];
+        t += Wi[3 * i + 2] * T[2];
+        d[i] = s; d[3 + i] = t;
+        du[i] = dt * s; du[3 + i] = dt * t;   // steppers.py:64 delta_u = dt * delta_u_ext
+    }
+}
+
+__global__ void k_zero_stats(const StepArgs a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < a.bd.n_scenes) { a.out.stats[s].n_grid_lookups = 0; a.out.stats[s].n_leaf_overlaps = 0; }
+}
+
+// collision_detection.py:32 V_world = rotate_array(q, V) + r
+__global__ void k_world_vertices(const StepArgs a, int n_verts) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_verts) return;
+    const int b = a.bd.vert_body[g];
+    const int local = g - a.bd.body_v0[b];
+    const int s = a.bd.shape[b];
+    const d3 V = ld3(a.sh.V + 3 * (size_t)(a.sh.v_off[s] + local));
+    const double* xb = a.bd.x + 7 * b;
+    const d3 p = quat_rotate_row(xb + 3, V);
+    st3(a.ws.Vw + 3 * (size_t)g, d3{p.x + xb[0], p.y + xb[1], p.z + xb[2]});
+}
+
+// leaf boxes (kdop.py:53 make with K=3: min/max of the triangle's coordinates -/+ envelope) and the box of
+// every run of 32 consecutive triangles of a body; one warp per cluster
+__global__ void k_clusters(const StepArgs a, int n_clusters) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= n_clusters) return;
+    const int b = a.bd.clu_body[warp];
+    const int c = warp - a.bd.body_c0[b];
+    const int s = a.bd.shape[b];
+    const int nt = a.sh.t_off[s + 1] - a.sh.t_off[s];
+    const int t = 32 * c + lane;
+    const double env = a.pr.envelope;
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    if (t < nt) {
+        const int32_t* tri = a.sh.T + 3 * (size_t)(a.sh.t_off[s] + t);
+        const double* Vw = a.ws.Vw + 3 * (size_t)a.bd.body_v0[b];
+        for (int axis = 0; axis < 3; ++axis) {
+            double l = INFINITY, h = -INFINITY;
+            for (int k = 0; k < 3; ++k) {
+                const double pr = Vw[3 * tri[k] + axis];
+                if (pr < l) l = pr;
+                if (pr > h) h = pr;
+            }
+            lo[axis] = l - env;
+            hi[axis] = h + env;
+        }
+        double* L = a.ws.leaf + 6 * (size_t)(a.bd.body_t0[b] + t);
+        L[0] = lo[0]; L[1] = lo[1]; L[2] = lo[2]; L[3] = hi[0]; L[4] = hi[1]; L[5] = hi[2];
+    }
+    for (int axis = 0; axis < 3; ++axis) {
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[axis] = fmin(lo[axis], __shfl_xor_sync(0xffffffffu, lo[axis], o));
+            hi[axis] = fmax(hi[axis], __shfl_xor_sync(0xffffffffu, hi[axis], o));
+        }
+    }
+    if (lane == 0) {
+        double* C = a.ws.clu + 6 * (size_t)warp;
+        C[0] = lo[0]; C[1] = lo[1]; C[2] = lo[2]; C[3] = hi[0]; C[4] = hi[1]; C[5] = hi[2];
+    }
+}
+
+// body box = union of its cluster boxes (kdop_bvh.py:229-231); one warp per body
+__global__ void k_roots(const StepArgs a) {
+    const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (b >= a.bd.n_bodies) return;
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int c = a.bd.body_c0[b] + lane; c < a.bd.body_c0[b + 1]; c += 32) {
+        const double* C = a.ws.clu + 6 * (size_t)c;
+        for (int axis = 0; axis < 3; ++axis) { lo[axis] = fmin(lo[axis], C[axis]); hi[axis] = fmax(hi[axis], C[3 + axis]); }
+    }
+    for (int axis = 0; axis < 3; ++axis)
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[axis] = fmin(lo[axis], __shfl_xor_sync(0xffffffffu, lo[axis], o));
+            hi[axis] = fmax(hi[axis], __shfl_xor_sync(0xffffffffu, hi[axis], o));
+        }
+    if (lane == 0) {
+        double* R = a.ws.root + 6 * b;
+        R[0] = lo[0]; R[1] = lo[1]; R[2] = lo[2]; R[3] = hi[0]; R[4] = hi[1]; R[5] = hi[2];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// broad phase: body pairs (i < j, same scene) in combinations() order whose boxes overlap; warp per body
+// ---------------------------------------------------------------------------------------------------------
+template <bool WRITE>
+__global__ void k_pairs(const StepArgs a) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (i >= a.bd.n_bodies) return;
+    if (WRITE && a.ws.counters[kAbort]) return;
+    const int s = scene_of(a.bd.scene_start, a.bd.n_scenes, i);
+    const int end = a.bd.scene_start[s + 1];
+    double Ri[6];
+    for (int k = 0; k < 6; ++k) Ri[k] = a.ws.root[6 * i + k];
+    int count = 0;
+    const int base = WRITE ? a.ws.pair_cnt[i] : 0;
+    for (int j0 = i + 1; j0 < end; j0 += 32) {
+        const int j = j0 + lane;
+        const bool ov = j < end && overlap(Ri, a.ws.root + 6 * j);
+        const unsigned bal = __ballot_sync(0xffffffffu, ov);
+        if (WRITE && ov) {
+            const int pos = base + count + __popc(bal & lanemask_lt());
+            a.ws.pairs[2 * pos] = i;
+            a.ws.pairs[2 * pos + 1] = j;
+        }
+        count += __popc(bal);
+    }
+    if (!WRITE && lane == 0) a.ws.pair_cnt[i] = count;
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// mid phase: for body pair (A, B) the A-triangles whose leaf box overlaps some B leaf box and vice versa.
+// The reference's tandem traversal (kdop_bvh.py:127-178) reports exactly the overlapping leaf pairs because
+// each inner volume is the exact union of its children; np.unique of each column (collision_detection.py:234)
+// makes both sets ascending.  Clusters of 32 triangles with exact union boxes prune the same way.
+// ---------------------------------------------------------------------------------------------------------
+struct MidShared {
+    int16_t listA[kMaxClustersPerShape];
+    int16_t listB[kMaxClustersPerShape];
+    uint32_t maskA[kMaxClustersPerShape];
+    uint32_t maskB[kMaxClustersPerShape];
+};
+
+template <bool WRITE>
+__global__ void __launch_bounds__(kBlock) k_mid(const StepArgs a) {
+    __shared__ MidShared sm[kWarpsPerBlock];
+    MidShared& S = sm[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    if (a.ws.counters[kAbort]) return;
+    const int n_pairs = a.ws.counters[kNPairs];
+    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < n_pairs; p += (gridDim.x * blockDim.x) >> 5) {
+        const int A = a.ws.pairs[2 * p], B = a.ws.pairs[2 * p + 1];
+        const int cA0 = a.bd.body_c0[A], ncA = a.bd.body_c0[A + 1] - cA0;
+        const int cB0 = a.bd.body_c0[B], ncB = a.bd.body_c0[B + 1] - cB0;
+        const int tA0 = a.bd.body_t0[A], ntA = a.bd.body_t0[A + 1] - tA0;
+        const int tB0 = a.bd.body_t0[B], ntB = a.bd.body_t0[B + 1] - tB0;
+        const double* rootA = a.ws.root + 6 * A;
+        const double* rootB = a.ws.root + 6 * B;
+        if (ncA > kMaxClustersPerShape || ncB > kMaxClustersPerShape) {
+            if (lane == 0) { atomicOr(a.out.status, RB_STATUS_MESH_TOO_LARGE); atomicOr(a.ws.counters + kAbort, RB_STATUS_MESH_TOO_LARGE); }
+            if (!WRITE && lane == 0) { a.ws.pair_items[p] = 0; a.ws.pair_itemsA[p] = 0; a.ws.pair_ovl[p] = 0; }
+            continue;
+        }
+        int nA = 0, nB = 0;
+        for (int c0 = 0; c0 < ncA; c0 += 32) {
+            const int c = c0 + lane;
+            const bool ok = c < ncA && overlap(a.ws.clu + 6 * (size_t)(cA0 + c), rootB);
+            const unsigned bal = __ballot_sync(0xffffffffu, ok);
+            if (ok) S.listA[nA + __popc(bal & lanemask_lt())] = (int16_t)c;
+            nA += __popc(bal);
+        }
+        for (int c0 = 0; c0 < ncB; c0 += 32) {
+            const int c = c0 + lane;
+            const bool ok = c < ncB && overlap(a.ws.clu + 6 * (size_t)(cB0 + c), rootA);
+            const unsigned bal = __ballot_sync(0xffffffffu, ok);
+            if (ok) S.listB[nB + __popc(bal & lanemask_lt())] = (int16_t)c;
+            nB += __popc(bal);
+        }
+        for (int k = lane; k < nA; k += 32) S.maskA[k] = 0u;
+        for (int k = lane; k < nB; k += 32) S.maskB[k] = 0u;
+        __syncwarp();
+        int n_ovl = 0;
+        for (int ia = 0; ia < nA; ++ia) {
+            const int ca = S.listA[ia];
+            const double* CA = a.ws.clu + 6 * (size_t)(cA0 + ca);
+            const int ta = 32 * ca + lane;
+            const bool validA = ta < ntA;
+            double LA[6];
+            if (validA) for (int k = 0; k < 6; ++k) LA[k] = a.ws.leaf[6 * (size_t)(tA0 + ta) + k];
+            bool hitA = false;
+            for (int ib = 0; ib < nB; ++ib) {
+                const int cb = S.listB[ib];
+                if (!overlap(CA, a.ws.clu + 6 * (size_t)(cB0 + cb))) continue;
+                const int nbt = min(32, ntB - 32 * cb);
+                unsigned hitB = 0u;
+                for (int jb = 0; jb < nbt; ++jb) {
+                    const double* LB = a.ws.leaf + 6 * (size_t)(tB0 + 32 * cb + jb);
+                    if (validA && overlap(LA, LB)) { hitA = true; hitB |= 1u << jb; }
+                }
+                if (!WRITE) n_ovl += __popc(hitB);
+                hitB = __reduce_or_sync(0xffffffffu, hitB);
+                if (lane == 0) S.maskB[ib] |= hitB;
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, hitA);
+            if (lane == 0) S.maskA[ia] = bal;
+        }
+        __syncwarp();
+        int cntA = 0, cntB = 0;
+        for (int k = lane; k < nA; k += 32) cntA += __popc(S.maskA[k]);
+        for (int k = lane; k < nB; k += 32) cntB += __popc(S.maskB[k]);
+        cntA = __reduce_add_sync(0xffffffffu, cntA);
+        cntB = __reduce_add_sync(0xffffffffu, cntB);
+        if (!WRITE) {
+            n_ovl = __reduce_add_sync(0xffffffffu, n_ovl);
+            if (lane == 0) { a.ws.pair_items[p] = cntA + cntB; a.ws.pair_itemsA[p] = cntA; a.ws.pair_ovl[p] = n_ovl; }
+        } else {
+            int pos = a.ws.pair_items[p];
+            for (int side = 0; side < 2; ++side) {
+                const int n = side ? nB : nA;
+                const int16_t* list = side ? S.listB : S.listA;
+                const uint32_t* mask = side ? S.maskB : S.maskA;
+                for (int k = 0; k < n; ++k) {
+                    const uint32_t bits = mask[k];
+                    if (bits & (1u << lane)) {
+                        const int at = pos + __popc(bits & lanemask_lt());
+                        a.ws.item_pair[at] = p;
+                        a.ws.item_tri[at] = (side << 31) | (32 * list[k] + lane);
+                    }
+                    pos += __popc(bits);
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// narrow phase (collision_detection.py:87 _compute_contacts): one thread per candidate triangle
+// ---------------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_narrow(const StepArgs a) {
+    if (a.ws.counters[kAbort]) return;
+    const int n_items = a.ws.counters[kNItems];
+    const int max_it = a.pr.contact_optimization_max_iterations;
+    const double tol = a.pr.contact_optimization_tolerance;
+    const double envelope = a.pr.envelope;
+    for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < n_items; it += gridDim.x * blockDim.x) {
+        const int p = a.ws.item_pair[it];
+        const unsigned st = (unsigned)a.ws.item_tri[it];
+        const int side = st >> 31, tri = st & 0x7fffffff;
+        const int A = a.ws.pairs[2 * p], B = a.ws.pairs[2 * p + 1];
+        const int mesh = side ? B : A, sdf = side ? A : B;
+        const int sm = a.bd.shape[mesh], ss = a.bd.shape[sdf];
+        const int32_t* T = a.sh.T + 3 * (size_t)(a.sh.t_off[sm] + tri);
+        const double* Vw = a.ws.Vw + 3 * (size_t)a.bd.body_v0[mesh];
+        const double* xB = a.bd.x + 7 * sdf;
+        const double qB[4] = {xB[3], xB[4], xB[5], xB[6]};
+        const double cqB[4] = {qB[0], -qB[1], -qB[2], -qB[3]};
+        const d3 rB = d3{xB[0], xB[1], xB[2]};
+        d3 ps[3];
+        for (int c = 0; c < 3; ++c) {
+            const d3 pw = ld3(Vw + 3 * T[c]);
+            ps[c] = quat_rotate_row(cqB, sub(pw, rB));   // :120-121
+        }
+        const GridView g = load_grid(a.sh.grid_meta + 12 * ss, a.sh.grid + a.sh.g_off[ss]);
+        // seed: corner with the smallest gradient norm (:136-140); norm(list, axis=1) sums squares unfused
+        double gn[3];
+        for (int c = 0; c < 3; ++c) {
+            const d3 gr = grid_gradient(g, ps[c]);
+            gn[c] = sqrt((gr.x * gr.x + gr.y * gr.y) + gr.z * gr.z);
+        }
+        int best = 0;
+        if (gn[1] < gn[best]) best = 1;
+        if (gn[2] < gn[best]) best = 2;
+        d3 x = ps[best];
+        int n_fw = 0;
+        for (int i = 0; i < max_it; ++i) {   // Frank-Wolfe (:144-165)
+            ++n_fw;
+            // the reference evaluates the same gradient once per corner; one evaluation gives identical values
+            const d3 gr = grid_gradient(g, x);
+            const double o0 = dot3_np(ps[0], gr), o1 = dot3_np(ps[1], gr), o2 = dot3_np(ps[2], gr);
+            int v = 0;
+            double ov = o0;
+            if (o1 < ov) { v = 1; ov = o1; }
+            if (o2 < ov) { v = 2; ov = o2; }
+            const double alpha = 2.0 / (double)(i + 2);
+            const d3 s = ps[v];
+            x = d3{x.x + alpha * (s.x - x.x), x.y + alpha * (s.y - x.y), x.z + alpha * (s.z - x.z)};
+            if (ov > tol) break;
+        }
+        int flag = 0;
+        int lookups = 3 + n_fw;   // seed gradients + one gradient per Frank-Wolfe iteration
+        if (grid_is_inside(g, x, 0.5)) {   // :172 (is_inside default boundary 0.5)
+            lookups += 1;
+            const double phi = grid_value(g, x);
+            if (phi <= envelope) {
+                lookups += 1;
+                const d3 nb = grid_gradient(g, x);
+                const d3 nw = quat_rotate(qB, nb);
+                const double ln = norm3_np(nw);
+                if (ln > 0.0) {
+                    const d3 xr = quat_rotate(qB, x);
+                    st3(a.ws.item_p + 3 * (size_t)it, d3{xr.x + rB.x, xr.y + rB.y, xr.z + rB.z});
+                    st3(a.ws.item_n + 3 * (size_t)it, d3{nw.x / ln, nw.y / ln, nw.z / ln});
+                    a.ws.item_g[it] = phi;
+                    flag = 1;
+                    if (fabs(1.0 - norm3_np(d3{nw.x / ln, nw.y / ln, nw.z / ln})) > 0.1)   // types.py:293
+                        atomicOr(a.out.status, RB_STATUS_NONUNIT_NORMAL);
+                }
+            }
+        }
+        a.ws.item_flag[it] = flag;
+        if (a.pr.profiling) {   // statistic for the bandwidth accounting: lookups per scene
+            const int s = scene_of(a.bd.scene_start, a.bd.n_scenes, A);
+            atomicAdd(&a.out.stats[s].n_grid_lookups, lookups);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// contact reduction (collision_detection.py:255): a contact is dropped when an earlier contact of the same
+// unordered body pair has the identical position.  Contacts of one body pair are contiguous (one pair list
+// entry), so the test runs per pair.  Pass 1 counts survivors, pass 2 writes them in order.
+// ---------------------------------------------------------------------------------------------------------
+template <bool WRITE>
+__global__ void k_dedup(const StepArgs a) {
+    if (a.ws.counters[kAbort]) return;
+    const int lane = threadIdx.x & 31;
+    const int n_pairs = a.ws.counters[kNPairs];
+    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < n_pairs; p += (gridDim.x * blockDim.x) >> 5) {
+        const int i0 = a.ws.pair_items[p], i1 = a.ws.pair_items[p + 1];
+        int kept = 0;
+        int base = WRITE ? a.ws.pair_cont[p] : 0;
+        const int A = a.ws.pairs[2 * p], B = a.ws.pairs[2 * p + 1];
+        for (int c0 = i0; c0 < i1; c0 += 32) {
+            const int i = c0 + lane;
+            bool keep = false;
+            if (i < i1) {
+                if (!WRITE) {
+                    if (a.ws.item_flag[i]) {
+                        const double* pi = a.ws.item_p + 3 * (size_t)i;
+                        const double px = pi[0], py = pi[1], pz = pi[2];
+                        keep = true;
+                        for (int j = i0; j < i; ++j) {
+                            if (!a.ws.item_flag[j]) continue;
+                            const double* pj = a.ws.item_p + 3 * (size_t)j;
+                            if (px == pj[0] && py == pj[1] && pz == pj[2]) { keep = false; break; }
+                        }
+                    }
+                } else {
+                    keep = a.ws.item_flag[i] == 2;
+                }
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, keep);
+            if (!WRITE && i < i1 && keep) a.ws.item_flag[i] = 2;   // the write pass reads flag 2 = kept
+            if (WRITE && keep) {
+                const int k = base + kept + __popc(bal & lanemask_lt());
+                if (k < a.caps.contact_capacity) {
+                    const int side = ((unsigned)a.ws.item_tri[i]) >> 31;
+                    const int mesh = side ? B : A, sdf = side ? A : B;
+                    a.out.contact_ids[2 * k] = sdf;     // ContactPoint(bodyB_sdf_owner, bodyA_mesh_owner, ...)
+                    a.out.contact_ids[2 * k + 1] = mesh;
+                    for (int c = 0; c < 3; ++c) {
+                        a.out.contact_p[3 * k + c] = a.ws.item_p[3 * (size_t)i + c];
+                        a.out.contact_n[3 * k + c] = a.ws.item_n[3 * (size_t)i + c];
+                    }
+                    a.out.contact_g[k] = a.ws.item_g[i];
+                    a.ws.c_scene[k] = scene_of(a.bd.scene_start, a.bd.n_scenes, A);
+                }
+            }
+            kept += __popc(bal);
+        }
+        if (!WRITE && lane == 0) a.ws.pair_cont[p] = kept;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// contact problem (contacts.py:31 initialize): thread per contact
+// ---------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ double jrow_dot(const double* Jr, const double* wlo, const double* whi) {
+    double s = 0.0;
+    for (int c = 0; c < 6; ++c) s += Jr[c] * wlo[c];
+    for (int c = 0; c < 6; ++c) s += Jr[6 + c] * whi[c];
+    return s;
+}
+
+__global__ void k_contacts(const StepArgs a) {
+    if (a.ws.counters[kAbort]) return;
+    const int K = a.ws.counters[kNContacts];
+    const double dt = a.pr.dt;
+    const double r_scale = a.pr.scheme == RB_SCHEME_RIGID_GS ? 1.0 : 0.1;   // solver_interface.py:48
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
+        const int A = a.out.contact_ids[2 * k], B = a.out.contact_ids[2 * k + 1];
+        const d3 p = ld3(a.out.contact_p + 3 * k);
+        const d3 rA = sub(p, ld3(a.bd.x + 7 * A)), rB = sub(p, ld3(a.bd.x + 7 * B));
+        d3 vs, vt, vn;
+        make_orthonormal_vectors(ld3(a.out.contact_n + 3 * k), vs, vt, vn);   // (t, b, n)
+        const d3 dirs[3] = {vn, vs, vt};
+        const int lo = min(A, B), hi = max(A, B);
+        const int offA = (A == lo) ? 0 : 6, offB = (B == lo) ? 0 : 6;
+        double* J = a.ws.J + 48 * (size_t)k;
+        double* W = a.ws.WJT + 48 * (size_t)k;
+        for (int row = 0; row < 3; ++row) {   // contacts.py:140-147
+            const d3 d = dirs[row];
+            const d3 ca = cross_np(rA, d), cb = cross_np(rB, d);
+            double* JA = J + 12 * row + offA;
+            double* JB = J + 12 * row + offB;
+            JA[0] = -d.x; JA[1] = -d.y; JA[2] = -d.z; JA[3] = -ca.x; JA[4] = -ca.y; JA[5] = -ca.z;
+            JB[0] = d.x; JB[1] = d.y; JB[2] = d.z; JB[3] = cb.x; JB[4] = cb.y; JB[5] = cb.z;
+        }
+        {
+            double* JA = J + 36 + offA;
+            double* JB = J + 36 + offB;
+            JA[0] = -0.0; JA[1] = -0.0; JA[2] = -0.0; JA[3] = -vn.x; JA[4] = -vn.y; JA[5] = -vn.z;
+            JB[0] = 0.0; JB[1] = 0.0; JB[2] = 0.0; JB[3] = vn.x; JB[4] = vn.y; JB[5] = vn.z;
+        }
+        a.ws.lohi[2 * k] = lo;
+        a.ws.lohi[2 * k + 1] = hi;
+        bool hasw[2];
+        for (int side = 0; side < 2; ++side) {   // WJT = W J^T (bsr_matmat order)
+            const int bb = side ? hi : lo;
+            hasw[side] = !a.bd.fixed[bb];
+            const double m = hasw[side] ? 1.0 / a.bd.mass[bb] : 0.0;
+            const double* Wi = a.ws.Winv + 9 * bb;
+            for (int row = 0; row < 4; ++row) {
+                const double* Jr = J + 12 * row + 6 * side;
+                double* Wr = W + 12 * row + 6 * side;
+                for (int i = 0; i < 3; ++i) {
+                    double s = 0.0;
+                    s += (i == 0 ? m : 0.0) * Jr[0];
+                    s += (i == 1 ? m : 0.0) * Jr[1];
+                    s += (i == 2 ? m : 0.0) * Jr[2];
+                    double t = 0.0;
+                    t += Wi[3 * i + 0] * Jr[3];
+                    t += Wi[3 * i + 1] * Jr[4];
+                    t += Wi[3 * i + 2] * Jr[5];
+                    Wr[i] = hasw[side] ? s : 0.0;
+                    Wr[3 + i] = hasw[side] ? t : 0.0;
+                }
+            }
+        }
+        // b = (1 + e) v + J (dt W f_ext) + g   (contacts.py:46)
+        const int sc = scene_of(a.bd.scene_start, a.bd.n_scenes, A);
+        const int M = a.bd.scene_material_count[sc];
+        const int entry = a.bd.scene_material_offset[sc] + a.bd.material[A] * M + a.bd.material[B];
+        const double mu = a.bd.material_mu[3 * entry];
+        const double eps = a.pr.use_bounce ? a.bd.material_eps[entry] : 0.0;
+        const double* ulo = a.bd.u + 6 * lo;
+        const double* uhi = a.bd.u + 6 * hi;
+        const double* dlo = a.ws.du + 6 * lo;
+        const double* dhi = a.ws.du + 6 * hi;
+        const double gap = a.out.contact_g[k];
+        double vrow[4];
+        for (int row = 0; row < 4; ++row) vrow[row] = jrow_dot(J + 12 * row, ulo, uhi);
+        double gk0 = 0.0;
+        if (a.pr.use_pre_stabilization) {   // contacts.py:188 _compute_error_vector
+            const double rate = a.pr.gap_reduction / dt;
+            const double upper = -a.pr.max_gap_value / dt;
+            const double lower = -a.pr.min_gap_value;
+            if (gap < lower && vrow[0] <= 0.0) {
+                const double t = rate * gap;
+                gk0 = upper > t ? upper : t;
+            }
+        }
+        for (int row = 0; row < 4; ++row) {
+            const double jd = jrow_dot(J + 12 * row, dlo, dhi);
+            const double e = row == 0 ? eps : 0.0;
+            const double g = row == 0 ? gk0 : 0.0;
+            a.ws.b[4 * k + row] = ((1.0 + e) * vrow[row] + jd) + g;
+            // Delassus diagonal: reduceat over the nonzero products J .* WJT^T in column order (contacts.py:49)
+            double prods[12];
+            int m = 0;
+            for (int c = 0; c < 12; ++c) {
+                if (!hasw[c / 6]) continue;
+                const double pr = J[12 * row + c] * W[12 * row + c];
+                if (pr != 0.0) prods[m++] = pr;
+            }
+            double dg = np_reduce_sum(prods, m);
+            if (dg == 0.0) dg = 1.0;
+            a.ws.diag[4 * k + row] = dg;
+            a.ws.r[4 * k + row] = r_scale / dg;
+            a.ws.x[4 * k + row] = 0.0;
+            a.out.contact_sol[4 * k + row] = 0.0;
+        }
+        a.ws.mu[k] = mu;
+    }
+}
+
+// per-body contact lists, ascending contact index (the column order of the SciPy products)
+__global__ void k_body_contacts_count(const StepArgs a) {
+    if (a.ws.counters[kAbort]) return;
+    const int K = a.ws.counters[kNContacts];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x)
+        for (int side = 0; side < 2; ++side) {
+            const int b = a.ws.lohi[2 * k + side];
+            if (!a.bd.fixed[b]) atomicAdd(a.ws.bc_ptr + b, 1);
+        }
+}
+__global__ void k_body_contacts_fill(const StepArgs a) {
+    if (a.ws.counters[kAbort]) return;
+    const int K = a.ws.counters[kNContacts];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x)
+        for (int side = 0; side < 2; ++side) {
+            const int b = a.ws.lohi[2 * k + side];
+            if (a.bd.fixed[b]) continue;
+            const int at = a.ws.bc_ptr[b] + atomicAdd(a.ws.bc_fill + b, 1);
+            a.ws.bc_list[at] = (k << 1) | side;
+        }
+}
+__global__ void k_body_contacts_sort(const StepArgs a) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= a.bd.n_bodies || a.ws.counters[kAbort]) return;
+    int32_t* l = a.ws.bc_list + a.ws.bc_ptr[b];
+    const int n = a.ws.bc_ptr[b + 1] - a.ws.bc_ptr[b];
+    for (int i = 1; i < n; ++i) {
+        const int32_t v = l[i];
+        int j = i - 1;
+        while (j >= 0 && l[j] > v) { l[j + 1] = l[j]; --j; }
+        l[j + 1] = v;
+    }
+}
+
+// w[b] = (WJT x) rows of body b: sequential over its contacts (ascending) and their 4 columns
+__device__ __forceinline__ void body_wjt_dot(const Workspace& ws, int b, const double* x, double* out6) {
+    double s[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int e = ws.bc_ptr[b]; e < ws.bc_ptr[b + 1]; ++e) {
+        const int code = ws.bc_list[e];
+        const int k = code >> 1, side = code & 1;
+        const double* Wk = ws.WJT + 48 * (size_t)k + 6 * side;
+        const double x0 = x[4 * k], x1 = x[4 * k + 1], x2 = x[4 * k + 2], x3 = x[4 * k + 3];
+        for (int d = 0; d < 6; ++d) {
+            double t = s[d];
+            t += Wk[d] * x0;
+            t += Wk[12 + d] * x1;
+            t += Wk[24 + d] * x2;
+            t += Wk[36 + d] * x3;
+            s[d] = t;
+        }
+    }
+    for (int d = 0; d < 6; ++d) out6[d] = s[d];
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// solver: one block per scene
+// ---------------------------------------------------------------------------------------------------------
+struct SceneRange { int b0, b1, c0, c1; };
+__device__ __forceinline__ SceneRange scene_range(const StepArgs& a, int s) {
+    SceneRange R;
+    R.b0 = a.bd.scene_start[s];
+    R.b1 = a.bd.scene_start[s + 1];
+    // contacts follow the pair order, pairs follow the body order
+    const int p0 = a.ws.pair_cnt[R.b0], p1 = a.ws.pair_cnt[R.b1];
+    R.c0 = a.ws.pair_cont[p0];
+    R.c1 = a.ws.pair_cont[p1];
+    return R;
+}
+
+__device__ __forceinline__ double block_max(double v, double* red) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const double t = __shfl_xor_sync(0xffffffffu, v, o);
+        v = (t > v || t != t) ? t : v;
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = red[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = (red[w] > m || red[w] != red[w]) ? red[w] : m;
+        red[32] = m;
+    }
+    __syncthreads();
+    return red[32];
+}
+
+// serial Gauss-Seidel sweep over contacts c0..c1-1 by one warp (contacts.py:66-107)
+__device__ void gs_sweep_warp(const StepArgs& a, int c0, int c1, const double* b, const double* r, double* x,
+                              bool normal_only) {
+    const int lane = threadIdx.x & 31;
+    double* w = a.ws.w;
+    for (int k = c0; k < c1; ++k) {
+        const int lo = a.ws.lohi[2 * k], hi = a.ws.lohi[2 * k + 1];
+        const double* J = a.ws.J + 48 * (size_t)k;
+        double z = 0.0, xo = 0.0;
+        if (lane < 4) {
+            xo = x[4 * k + lane];
+            const double jw = jrow_dot(J + 12 * lane, w + 6 * lo, w + 6 * hi);
+            z = xo - r[4 * k + lane] * (jw + b[4 * k + lane]);
+        }
+        const double z0 = __shfl_sync(0xffffffffu, z, 0), z1 = __shfl_sync(0xffffffffu, z, 1);
+        const double z2 = __shfl_sync(0xffffffffu, z, 2), z3 = __shfl_sync(0xffffffffu, z, 3);
+        const double x0o = __shfl_sync(0xffffffffu, xo, 0), x1o = __shfl_sync(0xffffffffu, xo, 1);
+        const double x2o = __shfl_sync(0xffffffffu, xo, 2), x3o = __shfl_sync(0xffffffffu, xo, 3);
+        const double xn = z0 > 0.0 ? z0 : 0.0;
+        double f[3];
+        if (normal_only) { f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; }
+        else prox_sphere(z1, z2, z3, a.ws.mu[k], xn, f);
+        const double d0 = xn - x0o, d1 = f[0] - x1o, d2 = f[1] - x2o, d3v = f[2] - x3o;
+        if (lane == 0) { x[4 * k] = xn; x[4 * k + 1] = f[0]; x[4 * k + 2] = f[1]; x[4 * k + 3] = f[2]; }
+        if (lane < 12) {
+            const int side = lane / 6, d = lane - 6 * side;
+            const int bb = side ? hi : lo;
+            if (!a.bd.fixed[bb]) {
+                const double* Wk = a.ws.WJT + 48 * (size_t)k + 6 * side + d;
+                double s = 0.0;
+                s += Wk[0] * d0;
+                s += Wk[12] * d1;
+                s += Wk[24] * d2;
+                s += Wk[36] * d3v;
+                w[6 * bb + d] = w[6 * bb + d] + s;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// complementarity residual ||x - prox(x - (A x + b))||_inf / max(1, ||x||_inf) with unit r (the tolerance
+// the solver modes are compared at); A x = J W J^T x through w2 = WJT x.  All threads of the block call it.
+__device__ double scene_residual(const StepArgs& a, const SceneRange& R, const double* x, double* red) {
+    for (int bb = R.b0 + threadIdx.x; bb < R.b1; bb += blockDim.x) {
+        if (a.bd.fixed[bb]) { for (int d = 0; d < 6; ++d) a.ws.w2[6 * bb + d] = 0.0; continue; }
+        body_wjt_dot(a.ws, bb, x, a.ws.w2 + 6 * bb);
+    }
+    __syncthreads();
+    double m = 0.0, xm = 0.0;
+    for (int k = R.c0 + threadIdx.x; k < R.c1; k += blockDim.x) {
+        const int lo = a.ws.lohi[2 * k], hi = a.ws.lohi[2 * k + 1];
+        const double* J = a.ws.J + 48 * (size_t)k;
+        double z[4];
+        for (int row = 0; row < 4; ++row)
+            z[row] = x[4 * k + row] - (jrow_dot(J + 12 * row, a.ws.w2 + 6 * lo, a.ws.w2 + 6 * hi) + a.ws.b[4 * k + row]);
+        const double pn = z[0] > 0.0 ? z[0] : 0.0;
+        double f[3];
+        prox_sphere(z[1], z[2], z[3], a.ws.mu[k], pn, f);
+        const double d[4] = {x[4 * k] - pn, x[4 * k + 1] - f[0], x[4 * k + 2] - f[1], x[4 * k + 3] - f[2]};
+        for (int i = 0; i < 4; ++i) {
+            const double e = fabs(d[i]);
+            m = (e > m || e != e) ? e : m;
+            xm = fmax(xm, fabs(x[4 * k + i]));
+        }
+    }
+    const double mres = block_max(m, red);
+    const double mx = block_max(xm, red);
+    return mres / (mx > 1.0 ? mx : 1.0);
+}
+
+__global__ void __launch_bounds__(256) k_solve(const StepArgs a, int post) {
+    __shared__ double red[33];
+    __shared__ double ctl[4];     // last_merit, global_last, merit, decision
+    __shared__ int ictl[4];       // done, iterations, exitcode
+    if (a.ws.counters[kAbort]) return;
+    const int scheme = post ? RB_SCHEME_RIGID_GS : a.pr.scheme;
+    const bool rigid = scheme == RB_SCHEME_RIGID_GS;
+    const int max_it = a.pr.max_iterations;
+    double* x = a.ws.x;
+    double* sol = post ? a.ws.xold : a.out.contact_sol;
+    const double* b = a.ws.b;
+    double* r = a.ws.r;
+    for (int s = blockIdx.x; s < a.bd.n_scenes; s += gridDim.x) {
+        const SceneRange R = scene_range(a, s);
+        const int K = R.c1 - R.c0;
+        rb_scene_stats* st = a.out.stats + s;
+        if (threadIdx.x == 0) {
+            if (!post) {
+                st->n_contacts = K; st->contact_start = R.c0; st->iterations = -1; st->exitcode = -1;
+                st->merit = 0.0; st->residual = 0.0; st->post_iterations = -1; st->post_exitcode = -1;
+            }
+            else { st->post_iterations = -1; st->post_exitcode = -1; }
+        }
+        if (!post && a.out.residuals && a.pr.profiling)
+            for (int i = threadIdx.x; i < max_it; i += blockDim.x) a.out.residuals[(size_t)s * a.caps.max_iterations + i] = INFINITY;
+        if (K == 0) continue;
+        if (post) {   // steppers.py:32: no solve when no contact is deeper than min_gap
+            int any = 0;
+            for (int k = R.c0 + threadIdx.x; k < R.c1; k += blockDim.x) any |= (b[4 * k] != 0.0);
+            any = __syncthreads_or(any);
+            if (!any) continue;
+        }
+        if (threadIdx.x == 0) { ctl[0] = INFINITY; ctl[1] = INFINITY; ictl[0] = 0; ictl[1] = max_it; ictl[2] = 0; }
+        __syncthreads();
+        for (int it = 0; it < max_it; ++it) {
+            // w = WJT x for this scene's bodies
+            for (int bb = R.b0 + threadIdx.x; bb < R.b1; bb += blockDim.x) {
+                if (a.bd.fixed[bb]) { for (int d = 0; d < 6; ++d) a.ws.w[6 * bb + d] = 0.0; continue; }
+                body_wjt_dot(a.ws, bb, x, a.ws.w + 6 * bb);
+            }
+            __syncthreads();
+            if (scheme == RB_SCHEME_JACOBI || scheme == RB_SCHEME_JACOBI_HYBRID) {
+                const bool hybrid = scheme == RB_SCHEME_JACOBI_HYBRID;
+                for (int k = R.c0 + threadIdx.x; k < R.c1; k += blockDim.x) {
+                    const int lo = a.ws.lohi[2 * k], hi = a.ws.lohi[2 * k + 1];
+                    const double* J = a.ws.J + 48 * (size_t)k;
+                    double z[4];
+                    for (int row = 0; row < 4; ++row)
+                        z[row] = x[4 * k + row] - r[4 * k + row] * (jrow_dot(J + 12 * row, a.ws.w + 6 * lo, a.ws.w + 6 * hi) + b[4 * k + row]);
+                    const double xn = z[0] > 0.0 ? z[0] : 0.0;
+                    double f[3];
+                    prox_sphere(z[1], z[2], z[3], a.ws.mu[k], hybrid ? xn : x[4 * k], f);
+                    x[4 * k] = xn; x[4 * k + 1] = f[0]; x[4 * k + 2] = f[1]; x[4 * k + 3] = f[2];
+                }
+            } else {
+                if (threadIdx.x < 32) gs_sweep_warp(a, R.c0, R.c1, b, r, x, post != 0);
+            }
+            __syncthreads();
+            // merit = ||x - sol||_inf (problem.py:53)
+            double m = 0.0;
+            for (int i = 4 * R.c0 + threadIdx.x; i < 4 * R.c1; i += blockDim.x) {
+                const double e = fabs(x[i] - sol[i]);
+                m = (e > m || e != e) ? e : m;
+            }
+            const double merit = block_max(m, red);
+            const bool by_residual = !post && a.pr.termination == RB_TERMINATE_RESIDUAL;
+            double res = 0.0;
+            if (by_residual) res = scene_residual(a, R, x, red);
+            if (threadIdx.x == 0) {
+                const double last = ctl[0];
+                int decision = 0;  // 0 accept, 1 reject
+                int stop = 0;
+                if (rigid) {   // gauss_seidel_solver.py:439-482
+                    double gm;
+                    if (merit > last) { decision = 1; gm = last > 0.0 ? last : 0.0; }
+                    else {
+                        decision = 0;
+                        ctl[3] = (last - merit < a.pr.too_small_merit_change) ? 1.0 : 0.0;
+                        ctl[0] = merit;
+                        gm = merit > 0.0 ? merit : 0.0;
+                    }
+                    if (!post && a.out.residuals && a.pr.profiling) a.out.residuals[(size_t)s * a.caps.max_iterations + it] = gm;
+                    if (gm < a.pr.absolute_tolerance) { stop = 1; ictl[2] = 1; }
+                    else if (fabs(gm - ctl[1]) < a.pr.relative_tolerance * ctl[1]) { stop = 1; ictl[2] = 2; }
+                    ctl[1] = gm;
+                    ctl[2] = gm;
+                } else {       // solver_interface.py:88-113 then :50-69
+                    if (!post && a.out.residuals && a.pr.profiling) a.out.residuals[(size_t)s * a.caps.max_iterations + it] = merit;
+                    if (merit < a.pr.absolute_tolerance) { stop = 1; ictl[2] = 1; }
+                    else if (fabs(merit - last) < a.pr.relative_tolerance * last) { stop = 1; ictl[2] = 2; }
+                    if (!stop) {
+                        if (merit > last) decision = 1;
+                        else { decision = 0; ctl[3] = (last - merit < a.pr.too_small_merit_change) ? 1.0 : 0.0; ctl[0] = merit; }
+                    } else decision = 2;   // converged: keep sol as it is
+                    ctl[2] = merit;
+                }
+                if (by_residual) {
+                    // stop only on the complementarity residual; the merit logic still adapts r
+                    if (!post && a.out.residuals && a.pr.profiling) a.out.residuals[(size_t)s * a.caps.max_iterations + it] = res;
+                    ctl[2] = res;
+                    if (res <= a.pr.residual_tolerance) { stop = 1; ictl[2] = 3; decision = 3; }
+                    else {
+                        stop = 0;
+                        ictl[2] = 0;
+                        if (decision == 2) {   // a merit test would have stopped: apply the accept/reject rule
+                            if (merit > last) decision = 1;
+                            else { decision = 0; ctl[3] = (last - merit < a.pr.too_small_merit_change) ? 1.0 : 0.0; ctl[0] = merit; }
+                        }
+                    }
+                }
+                ictl[3] = decision;
+                if (stop) { ictl[0] = 1; ictl[1] = it; }
+            }
+            __syncthreads();
+            const int decision = ictl[3];
+            const double inc = ctl[3];
+            if (decision == 1) {
+                for (int i = 4 * R.c0 + threadIdx.x; i < 4 * R.c1; i += blockDim.x) {
+                    r[i] = a.pr.nu_reduce * r[i];
+                    x[i] = sol[i];
+                }
+            } else if (decision == 0) {
+                for (int i = 4 * R.c0 + threadIdx.x; i < 4 * R.c1; i += blockDim.x) {
+                    sol[i] = x[i];
+                    if (inc != 0.0) r[i] = a.pr.nu_increase * r[i];
+                }
+            } else if (decision == 3) {   // converged by residual: the current iterate is the solution
+                for (int i = 4 * R.c0 + threadIdx.x; i < 4 * R.c1; i += blockDim.x) sol[i] = x[i];
+            }
+            __syncthreads();
+            if (ictl[0]) break;
+        }
+        if (!post && a.pr.termination == RB_TERMINATE_RESIDUAL) {
+            if (ictl[2] != 3) {   // not converged: report the residual of the returned (last accepted) solution
+                const double rs = scene_residual(a, R, sol, red);
+                if (threadIdx.x == 0) ctl[2] = rs;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) st->residual = ctl[2];
+        }
+        if (threadIdx.x == 0) {
+            if (!post) { st->iterations = ictl[1]; st->exitcode = ictl[2]; st->merit = ctl[2]; }
+            else { st->post_iterations = ictl[1]; st->post_exitcode = ictl[2]; }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// integration (state_storage.py:239 velocity_update, :251 position_update): thread per body
+// ---------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void position_update(double* xb, const double* ub, double dt) {
+    for (int i = 0; i < 3; ++i) xb[i] = xb[i] + ub[i] * dt;
+    const double qw[4] = {0.0, ub[3], ub[4], ub[5]};
+    double q[4] = {xb[3], xb[4], xb[5], xb[6]}, dq[4], qn[4];
+    quat_prod(qw, q, dq);
+    for (int i = 0; i < 4; ++i) qn[i] = q[i] + (dq[i] * dt) * 0.5;
+    quat_unit(qn, xb + 3);
+}
+
+__global__ void k_integrate(const StepArgs a) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= a.bd.n_bodies || a.ws.counters[kAbort]) return;
+    double* ub = a.bd.u + 6 * b;
+    double du[6];
+    for (int d = 0; d < 6; ++d) du[d] = a.ws.du[6 * b + d];
+    if (!a.bd.fixed[b] && a.ws.bc_ptr[b + 1] > a.ws.bc_ptr[b]) {   // delta_u += WJT sol (steppers.py:84-85)
+        double dc[6];
+        body_wjt_dot(a.ws, b, a.out.contact_sol, dc);
+        for (int d = 0; d < 6; ++d) du[d] = du[d] + dc[d];
+    }
+    for (int d = 0; d < 6; ++d) ub[d] = ub[d] + du[d];
+    if (a.bd.fixed[b]) return;
+    position_update(a.bd.x + 7 * b, ub, a.pr.dt);
+    bool finite = true;
+    for (int d = 0; d < 7; ++d) finite &= isfinite(a.bd.x[7 * b + d]);
+    for (int d = 0; d < 6; ++d) finite &= isfinite(ub[d]);
+    if (!finite) atomicOr(a.out.status, RB_STATUS_NONFINITE);
+}
+
+// post-stabilisation problem (post_stabilization.py:30-104): b = gap on deep normal rows, r = 1/diag
+__global__ void k_post_setup(const StepArgs a) {
+    if (a.ws.counters[kAbort]) return;
+    const int K = a.ws.counters[kNContacts];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
+        const double g = a.out.contact_g[k];
+        for (int row = 0; row < 4; ++row) {
+            a.ws.b[4 * k + row] = (row == 0 && g < -a.pr.min_gap_value) ? g : 0.0;
+            a.ws.r[4 * k + row] = 1.0 / a.ws.diag[4 * k + row];
+            a.ws.x[4 * k + row] = 0.0;
+            a.ws.xold[4 * k + row] = 0.0;
+        }
+    }
+}
+__global__ void k_post_apply(const StepArgs a) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= a.bd.n_bodies || a.ws.counters[kAbort] || a.bd.fixed[b]) return;
+    // every non-fixed body of a corrected scene is updated (and its quaternion renormalised), contacts or not
+    const int s = scene_of(a.bd.scene_start, a.bd.n_scenes, b);
+    if (a.out.stats[s].post_iterations < 0) return;   // this scene had nothing to correct
+    double dr[6];
+    body_wjt_dot(a.ws, b, a.ws.xold, dr);
+    position_update(a.bd.x + 7 * b, dr, 1.0);
+}
+
+// energies and largest penetration (state_storage.py:188, contacts.py:222): thread per scene, body order
+__global__ void k_scene_summary(const StepArgs a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.bd.n_scenes || a.ws.counters[kAbort]) return;
+    rb_scene_stats* st = a.out.stats + s;
+    const SceneRange R = scene_range(a, s);
+    double gap = 0.0;
+    for (int k = R.c0; k < R.c1; ++k) gap = fmin(gap, a.out.contact_g[k]);
+    st->max_penetration = -gap;
+    {
+        const int p0 = a.ws.pair_cnt[R.b0], p1 = a.ws.pair_cnt[R.b1];
+        st->n_pairs = p1 - p0;
+        st->n_candidates = a.ws.pair_items[p1] - a.ws.pair_items[p0];
+        int ovl = 0;
+        if (a.pr.profiling) for (int p = p0; p < p1; ++p) ovl += a.ws.pair_ovl[p];
+        st->n_leaf_overlaps = ovl;
+    }
+    if (!a.pr.profiling) return;
+    double G[3] = {0.0, 0.0, 0.0};
+    int has_gravity = 0;
+    for (int f = a.bd.scene_force_start[s]; f < a.bd.scene_force_start[s + 1]; ++f)
+        if (a.bd.force_kind[f] == 0) {
+            const double* fp = a.bd.force_params + 4 * f;
+            for (int i = 0; i < 3; ++i) G[i] = G[i] + fp[1 + i] * fp[0];
+            has_gravity = 1;
+        }
+    double kinetic = 0.0, potential = 0.0;
+    for (int b = R.b0; b < R.b1; ++b) {
+        if (a.bd.fixed[b]) continue;
+        const double* xb = a.bd.x + 7 * b;
+        double Rm[9], Iw[9], Ib[3] = {a.bd.inertia[3 * b], a.bd.inertia[3 * b + 1], a.bd.inertia[3 * b + 2]};
+        quat_to_matrix(xb + 3, Rm);
+        update_inertia_tensor(Rm, Ib, Iw);
+        const double m = a.bd.mass[b];
+        if (has_gravity) {
+            const d3 Gv = d3{G[0], G[1], G[2]};
+            const double ln = norm3_np(Gv);
+            const d3 up = d3{G[0] / ln, G[1] / ln, G[2] / ln};
+            const double g = norm3_np(Gv);
+            const double h = dot3_np(up, ld3(xb));
+            potential += m * g * h;
+        }
+        const d3 v = ld3(a.bd.u + 6 * b), w = ld3(a.bd.u + 6 * b + 3);
+        const double wIw = dot3_np(w, gemv3_np(Iw, w));
+        kinetic += 0.5 * (m * dot3_np(v, v) + wIw);
+    }
+    st->kinetic_energy = kinetic;
+    st->potential_energy = potential;
+}
+
+__global__ void k_finish(const StepArgs a) {
+    if (a.out.n_contacts_total) *a.out.n_contacts_total = a.ws.counters[kNContacts];
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------------------------
+thread_local std::string g_error;
+
+// phase events of the last profiled step (host-side CUDA events; no device memory)
+struct ProfileEvents {
+    cudaEvent_t ev[8];
+    bool created = false;
+    bool recorded = false;
+};
+thread_local ProfileEvents g_prof;
+
+static void prof_mark(bool on, int i, cudaStream_t st) {
+    if (!on) return;
+    if (!g_prof.created) {
+        for (int k = 0; k < 8; ++k) cudaEventCreate(&g_prof.ev[k]);
+        g_prof.created = true;
+    }
+    cudaEventRecord(g_prof.ev[i], st);
+    if (i == 6) g_prof.recorded = true;
+}
+
+static int fail(int code, const std::string& msg) {
+    g_error = msg;
+    return code;
+}
+
+static inline int blocks_for(int64_t n, int block) { return (int)((n + block - 1) / block > 0 ? (n + block - 1) / block : 1); }
+
+}  // namespace rb
+
+using namespace rb;
+
+extern "C" {
+
+int rb_abi_version(void) { return RB_ABI_VERSION; }
+
+const char* rb_last_error(void) { return rb::g_error.c_str(); }
+
+int rb_topology_sizes(int32_t n_bodies, const int32_t* body_shape, int32_t n_shapes, const int32_t* v_off,
+                      const int32_t* t_off, int64_t* out) {
+    if (n_bodies < 0 || n_shapes <= 0 || !body_shape || !v_off || !t_off || !out)
+        return fail(RB_ERR_ARG, "rb_topology_sizes: bad argument");
+    int64_t nv = 0, nt = 0, nc = 0;
+    for (int b = 0; b < n_bodies; ++b) {
+        const int s = body_shape[b];
+        if (s < 0 || s >= n_shapes) return fail(RB_ERR_ARG, "rb_topology_sizes: shape index out of range");
+        nv += v_off[s + 1] - v_off[s];
+        const int t = t_off[s + 1] - t_off[s];
+        nt += t;
+        nc += (t + 31) / 32;
+    }
+    out[0] = nv; out[1] = nt; out[2] = nc;
+    return RB_OK;
+}
+
+int rb_workspace_bytes(const rb_bodies* bd, const rb_caps* caps, size_t* bytes) {
+    if (!bd || !caps || !bytes) return fail(RB_ERR_ARG, "rb_workspace_bytes: null argument");
+    if (bd->n_bodies < 0 || bd->n_body_vertices < 0 || bd->n_body_triangles < 0 || bd->n_clusters < 0 ||
+        caps->pair_capacity < 0 || caps->item_capacity < 0 || caps->contact_capacity < 0)
+        return fail(RB_ERR_ARG, "rb_workspace_bytes: negative size");
+    *bytes = rb::layout(nullptr, nullptr, bd->n_bodies, bd->n_body_vertices, bd->n_body_triangles, bd->n_clusters,
+                        caps->pair_capacity, caps->item_capacity, caps->contact_capacity);
+    return RB_OK;
+}
+
+int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const rb_params* pr,
+            const rb_outputs* out, void* workspace, size_t workspace_bytes, void* stream_ptr) {
+    if (!sh || !bd || !caps || !pr || !out || !workspace) return fail(RB_ERR_ARG, "rb_step: null argument");
+    if (bd->n_bodies <= 0 || bd->n_scenes <= 0) return fail(RB_ERR_ARG, "rb_step: empty scene batch");
+    if (!bd->x || !bd->u || !out->contact_ids || !out->stats || !out->status)
+        return fail(RB_ERR_ARG, "rb_step: null state or output buffer");
+    if (pr->scheme < 0 || pr->scheme > RB_SCHEME_JACOBI_HYBRID)
+        return fail(RB_ERR_UNSUPPORTED, "rb_step: solver scheme not available in this build");
+    if (pr->max_iterations < 0 || pr->max_iterations > caps->max_iterations)
+        return fail(RB_ERR_ARG, "rb_step: max_iterations exceeds rb_caps.max_iterations");
+    if (!(pr->dt > 0.0)) return fail(RB_ERR_ARG, "rb_step: dt must be positive");
+    size_t need = 0;
+    int rc = rb_workspace_bytes(bd, caps, &need);
+    if (rc != RB_OK) return rc;
+    if (workspace_bytes < need) return fail(RB_ERR_WORKSPACE, "rb_step: workspace too small");
+    const int64_t n_body_vertices = bd->n_body_vertices, n_body_triangles = bd->n_body_triangles,
+                  n_clusters = bd->n_clusters;
+    cudaStream_t st = (cudaStream_t)stream_ptr;
+    StepArgs a;
+    a.sh = *sh; a.bd = *bd; a.caps = *caps; a.pr = *pr; a.out = *out;
+    rb::layout(&a.ws, (char*)workspace, bd->n_bodies, n_body_vertices, n_body_triangles, n_clusters,
+               caps->pair_capacity, caps->item_capacity, caps->contact_capacity);
+    if (n_body_vertices <= 0 || n_body_triangles <= 0 || n_clusters <= 0)
+        return fail(RB_ERR_ARG, "rb_step: bodies without geometry");
+    const int N = bd->n_bodies;
+    const int G = 148 * 8;
+    const bool prof = pr->profiling != 0;
+    prof_mark(prof, 0, st);
+    k_zero_i32<<<1, 32, 0, st>>>(a.ws.counters, 16);
+    k_zero_stats<<<blocks_for(bd->n_scenes, 128), 128, 0, st>>>(a);
+    k_zero_i32<<<blocks_for(N + 1, 256), 256, 0, st>>>(a.ws.bc_ptr, N + 1);
+    k_zero_i32<<<blocks_for(N, 256), 256, 0, st>>>(a.ws.bc_fill, N);
+    k_bodies<<<blocks_for(N, 128), 128, 0, st>>>(a);
+    k_world_vertices<<<blocks_for(n_body_vertices, 256), 256, 0, st>>>(a, (int)n_body_vertices);
+    k_clusters<<<blocks_for(32 * n_clusters, kBlock), kBlock, 0, st>>>(a, (int)n_clusters);
+    k_roots<<<blocks_for(32 * (int64_t)N, kBlock), kBlock, 0, st>>>(a);
+    prof_mark(prof, 1, st);
+    // broad phase
+    k_pairs<false><<<blocks_for(32 * (int64_t)N, kBlock), kBlock, 0, st>>>(a);
+    scan(a.ws.pair_cnt, nullptr, N, a.ws.scan_tmp, a.ws.counters + kNPairs, st);
+    k_check<<<1, 1, 0, st>>>(a.ws.counters, kNPairs, caps->pair_capacity, RB_STATUS_PAIR_OVERFLOW, out->status);
+    k_pairs<true><<<blocks_for(32 * (int64_t)N, kBlock), kBlock, 0, st>>>(a);
+    // mid phase
+    k_mid<false><<<G, kBlock, 0, st>>>(a);
+    scan(a.ws.pair_items, a.ws.counters + kNPairs, caps->pair_capacity, a.ws.scan_tmp, a.ws.counters + kNItems, st);
+    k_check<<<1, 1, 0, st>>>(a.ws.counters, kNItems, caps->item_capacity, RB_STATUS_ITEM_OVERFLOW, out->status);
+    k_mid<true><<<G, kBlock, 0, st>>>(a);
+    prof_mark(prof, 2, st);
+    // narrow phase
+    k_narrow<<<G, 256, 0, st>>>(a);
+    prof_mark(prof, 3, st);
+    // reduction and compaction
+    k_dedup<false><<<G, kBlock, 0, st>>>(a);
+    scan(a.ws.pair_cont, a.ws.counters + kNPairs, caps->pair_capacity, a.ws.scan_tmp, a.ws.counters + kNContacts, st);
+    k_check<<<1, 1, 0, st>>>(a.ws.counters, kNContacts, caps->contact_capacity, RB_STATUS_CONTACT_OVERFLOW, out->status);
+    k_dedup<true><<<G, kBlock, 0, st>>>(a);
+    prof_mark(prof, 4, st);
+    // contact problem
+    k_contacts<<<G, 128, 0, st>>>(a);
+    k_body_contacts_count<<<G, 256, 0, st>>>(a);
+    scan(a.ws.bc_ptr, nullptr, N, a.ws.scan_tmp, nullptr, st);
+    k_body_contacts_fill<<<G, 256, 0, st>>>(a);
+    k_body_contacts_sort<<<blocks_for(N, 128), 128, 0, st>>>(a);
+    // solve, integrate, post-stabilise
+    const int sg = bd->n_scenes < 148 * 16 ? bd->n_scenes : 148 * 16;
+    k_solve<<<sg, 256, 0, st>>>(a, 0);
+    prof_mark(prof, 5, st);
+    k_integrate<<<blocks_for(N, 128), 128, 0, st>>>(a);
+    if (pr->use_post_stabilization) {
+        k_post_setup<<<G, 128, 0, st>>>(a);
+        k_solve<<<sg, 256, 0, st>>>(a, 1);
+        k_post_apply<<<blocks_for(N, 128), 128, 0, st>>>(a);
+    }
+    k_scene_summary<<<blocks_for(bd->n_scenes, 64), 64, 0, st>>>(a);
+    k_finish<<<1, 1, 0, st>>>(a);
+    prof_mark(prof, 6, st);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(RB_ERR_CUDA, std::string("rb_step: ") + cudaGetErrorString(e));
+    return RB_OK;
+}
+
+int rb_profile_times(float* out, int32_t n) {
+    if (!out || n < 7) return fail(RB_ERR_ARG, "rb_profile_times: need room for 7 values");
+    if (!g_prof.recorded) return fail(RB_ERR_ARG, "rb_profile_times: no profiled step on this thread");
+    cudaError_t e = cudaEventSynchronize(g_prof.ev[6]);
+    if (e != cudaSuccess) return fail(RB_ERR_CUDA, std::string("rb_profile_times: ") + cudaGetErrorString(e));
+    for (int i = 0; i < 6; ++i) cudaEventElapsedTime(out + i, g_prof.ev[i], g_prof.ev[i + 1]);
+    cudaEventElapsedTime(out + 6, g_prof.ev[0], g_prof.ev[6]);
+    return RB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,145 @@
+"""GPU step (through the C ABI) against the reference's recorded steps and against the oracle.
+
+FP64 parity target: bit-identical contact sets (body indices, positions, normals, gaps), solver impulses,
+iteration counts and body states.  The north-star bound is 1e-9 relative; the kernels reproduce NumPy's
+rounding sequence, so the tests demand exact equality."""
+import numpy as np
+import pytest
+
+from conftest import FIXTURES, load_fixture, step_slice
+
+pytestmark = pytest.mark.gpu
+
+
+def _world(d, **kw):
+    from rainbow_b200 import world as W
+    return W.DeviceWorld(d, **kw)
+
+
+def _params(d, dt=None, scheme="rigid_gauss_seidel", profiling=True):
+    from rainbow_b200 import world as W
+    return W.make_rb_params(W.params_from_vector(d["params"]), dt=dt, scheme=scheme, profiling=profiling)
+
+
+def _assert_step(world, d, s, scene=0):
+    st = world.stats()[scene]
+    c = world.contacts()
+    k0, K = st.contact_start, st.n_contacts
+    ids = c["ids"][k0:k0 + K] - world.scene_start[scene]
+    np.testing.assert_array_equal(ids, step_slice(d, "contacts_ids", s), err_msg="step %d contact ids" % s)
+    for key, ref in (("p", "contacts_p"), ("n", "contacts_n"), ("g", "contacts_g")):
+        np.testing.assert_array_equal(c[key][k0:k0 + K], step_slice(d, ref, s), err_msg="step %d %s" % (s, key))
+    np.testing.assert_array_equal(c["sol"][4 * k0:4 * (k0 + K)], step_slice(d, "sol", s), err_msg="step %d sol" % s)
+    assert st.iterations == d["step_iterations"][s]
+    assert st.exitcode == d["step_exitcode"][s]
+    assert st.post_iterations == d["step_post_iterations"][s]
+    x, u = world.state()
+    b0, b1 = world.scene_start[scene], world.scene_start[scene + 1]
+    np.testing.assert_array_equal(x[b0:b1].ravel(), d["step_x"][s], err_msg="step %d x" % s)
+    np.testing.assert_array_equal(u[b0:b1].ravel(), d["step_u"][s], err_msg="step %d u" % s)
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_gpu_matches_reference_step_by_step(name):
+    d = load_fixture(name)
+    world = _world(d)
+    N = world.n_bodies
+    for s in range(int(d["steps"])):
+        if s > 0:
+            world.set_state(d["step_x"][s - 1].reshape(N, 7), d["step_u"][s - 1].reshape(N, 6))
+        status = world.step(_params(d, dt=float(d["step_dt"][s])))
+        assert status == 0
+        _assert_step(world, d, s)
+
+
+def test_gpu_free_run_matches_reference():
+    d = load_fixture("boxes8")
+    world = _world(d)
+    for s in range(int(d["steps"])):
+        world.step(_params(d, dt=float(d["step_dt"][s])))
+    _assert_step(world, d, int(d["steps"]) - 1)
+
+
+@pytest.mark.parametrize("scheme", ["gauss_seidel", "parallel_jacobi", "parallel_jacobi_hybrid"])
+def test_gpu_proximal_contact_schemes_match_reference(scheme):
+    d = load_fixture("solvers")
+    world = _world(d)
+    world.step(_params(d, scheme=scheme))
+    st = world.stats()[0]
+    c = world.contacts()
+    np.testing.assert_array_equal(c["ids"], d["contacts_ids"])
+    np.testing.assert_array_equal(c["sol"], d["sol_" + scheme])
+    assert st.iterations == d["iterations_" + scheme]
+    assert st.exitcode == d["exitcode_" + scheme]
+
+
+@pytest.mark.parametrize("scheme", ["parallel_jacobi", "gauss_seidel"])
+def test_gpu_schemes_match_oracle_over_steps(oracle_lib, scheme):
+    """Several chained steps with a proximal_contact scheme: GPU and oracle stay bit-identical."""
+    d = load_fixture("spheres")
+    world = _world(d)
+    sc = oracle_lib.OracleScene(d)
+    for s in range(4):
+        world.step(_params(d, scheme=scheme))
+        o = sc.step(scheme=scheme)
+        c = world.contacts()
+        np.testing.assert_array_equal(c["ids"], o["ids"])
+        np.testing.assert_array_equal(c["sol"], o["sol"])
+        x, u = world.state()
+        np.testing.assert_array_equal(x.ravel(), o["x"])
+        np.testing.assert_array_equal(u.ravel(), o["u"])
+
+
+def test_batched_scenes_equal_alone():
+    """Every scene gives the same bits alone and packed with the other fixtures into one launch."""
+    from rainbow_b200 import world as W
+    ds = [load_fixture(n) for n in ("boxes8", "spheres", "tower6", "c1_boxes64")]
+    # one parameter set for the whole batch: the tower's dt and tolerances
+    params = W.params_from_vector(ds[2]["params"])
+    alone = []
+    for d in ds:
+        w = _world(d, max_iterations=100)
+        for _ in range(3):
+            w.step(W.make_rb_params(params))
+        alone.append((w.state(), w.contacts(), w.stats()[0]))
+    batch = W.DeviceWorld(ds, max_iterations=100)
+    for _ in range(3):
+        batch.step(W.make_rb_params(params))
+    x, u = batch.state()
+    c = batch.contacts()
+    for i, ((xa, ua), ca, sa) in enumerate(alone):
+        b0, b1 = batch.scene_start[i], batch.scene_start[i + 1]
+        np.testing.assert_array_equal(x[b0:b1], xa)
+        np.testing.assert_array_equal(u[b0:b1], ua)
+        st = batch.stats()[i]
+        assert (st.n_contacts, st.iterations, st.exitcode) == (sa.n_contacts, sa.iterations, sa.exitcode)
+        k0 = st.contact_start
+        np.testing.assert_array_equal(c["ids"][k0:k0 + st.n_contacts] - b0, ca["ids"])
+        np.testing.assert_array_equal(c["sol"][4 * k0:4 * (k0 + st.n_contacts)], ca["sol"])
+
+
+def test_capacity_growth_repeats_step():
+    """Work lists far too small: the step reports the overflow, leaves the state alone, grows and repeats."""
+    d = load_fixture("spheres")
+    ref = _world(d)
+    ref.step(_params(d))
+    small = _world(d, caps={"pairs": 2, "items": 8, "contacts": 4})
+    small.step(_params(d))
+    assert small.caps.pair_capacity > 2 and small.caps.contact_capacity > 4
+    np.testing.assert_array_equal(small.state()[0], ref.state()[0])
+    np.testing.assert_array_equal(small.contacts()["sol"], ref.contacts()["sol"])
+
+
+def test_profile_counts_match_oracle(oracle_lib):
+    d = load_fixture("c1_boxes64")
+    world = _world(d)
+    world.step(_params(d, profiling=True))
+    st = world.stats()[0]
+    o = oracle_lib.OracleScene(d).step()
+    assert st.n_leaf_overlaps == o["n_leaf_overlaps"]
+    assert st.n_candidates == o["n_candidates"]
+    assert abs(st.kinetic_energy - o["kinetic"]) <= 1e-12 * max(1.0, abs(o["kinetic"]))
+    assert st.potential_energy == o["potential"]
+    assert st.max_penetration == o["max_penetration"]
+    times = world.profile_times()
+    assert len(times) == 7 and times[6] > 0.0
