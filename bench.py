@@ -33,7 +33,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-LAUNCHES_PER_STEP = 38          # kernels issued by one rb_step without post-stabilisation (rb_step.cu)
+LAUNCHES_PER_STEP = 36          # kernels issued by one rb_step without post-stabilisation, batches below 4736 scenes
 
 
 def parse():
@@ -44,10 +44,12 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batch1024", choices=["batch1024", "mixed4096", "boxes64"])
     ap.add_argument("--scheme", default="rigid_gauss_seidel")
-    ap.add_argument("--termination", default="residual", choices=["residual", "merit"])
+    ap.add_argument("--termination", default="residual_fixed_r", choices=["residual_fixed_r", "residual", "merit"])
+    ap.add_argument("--scenes", type=int, default=1024, help="scenes of the batch1024 workload")
     ap.add_argument("--tolerance", type=float, default=1e-6)
     ap.add_argument("--pre-roll", type=int, default=60)
     ap.add_argument("--plain-scenes", type=int, default=32, help="scenes of the one-scene-per-launch baseline")
+    ap.add_argument("--no-warm-start", action="store_true", help="start every solve from zero impulses")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     ap.add_argument("--cpu-scenes", type=int, default=16, help="scenes in the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
@@ -57,12 +59,13 @@ def parse():
 # --------------------------------------------------------------------------------------------------------------
 # workloads
 # --------------------------------------------------------------------------------------------------------------
-def build_workload(name, device):
+def build_workload(name, device, n_scenes=1024):
     from rainbow_b200 import engine_io, scenes
     if name == "batch1024":
-        arrays, params = scenes.batch_arrays(n_scenes=1024, seed=0, pool=64, resolution=32, device=device)
+        arrays, params = scenes.batch_arrays(n_scenes=n_scenes, seed=0, pool=64, resolution=32, device=device)
         bodies = sum(len(a["body_mass"]) for a in arrays)
-        cfg = {"workload": "batch_1024_scenes", "scenes": 1024, "bodies": int(bodies), "bodies_per_scene": "8..256",
+        cfg = {"workload": "batch_%d_scenes" % n_scenes, "scenes": n_scenes, "bodies": int(bodies),
+               "bodies_per_scene": "8..256",
                "shapes": "boxes side U(0.5,2), spheres r U(0.25,1) 16x16, pool 64+64", "sdf_resolution": 32,
                "dt": 0.01}
         return arrays, params, cfg, None
@@ -147,7 +150,7 @@ def cpu_baseline(arrays, args, workers):
     import multiprocessing as mp
     from oracle import oracle as O
     O.build()
-    tol_mode = 1 if args.termination == "residual" else 0
+    tol_mode = {"merit": 0, "residual": 1, "residual_fixed_r": 2}[args.termination]
     sample = arrays[:max(1, min(len(arrays), args.cpu_scenes))]
     workers = max(1, min(workers, len(sample)))
     jobs = [(sample[w::workers], args.scheme, tol_mode, args.tolerance, args.pre_roll, args.cpu_seconds)
@@ -171,7 +174,7 @@ def run_reference(args):
     workers = os.cpu_count() or 1
     import torch
     dev = "cuda:0" if torch.cuda.is_available() else "cpu"
-    arrays, params, cfg, _ = build_workload(args.workload, dev)
+    arrays, params, cfg, _ = build_workload(args.workload, dev, args.scenes)
     value, info = cpu_baseline(arrays, args, workers if len(arrays) > 1 else 1)
     cfg.update({"scheme": args.scheme, "termination": args.termination, "tolerance": args.tolerance})
     line = {
@@ -215,21 +218,24 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device(dev))
     from rainbow_b200 import engine_io, world as W
     from rainbow_b200.stepper import GpuStepper
-    arrays, params, cfg, engine = build_workload(args.workload, dev)
+    arrays, params, cfg, engine = build_workload(args.workload, dev, args.scenes)
     max_it = int(params.max_iterations)
     world = W.DeviceWorld(arrays, device=dev, max_iterations=max_it)
     kw = dict(scheme=args.scheme, termination=args.termination, residual_tolerance=args.tolerance)
-    rp = W.make_rb_params(params, **kw)
-    rp_prof = W.make_rb_params(params, profiling=True, **kw)
+    warm = not args.no_warm_start
+    rp = W.make_rb_params(params, warm_start=warm, **kw)
+    rp_prof = W.make_rb_params(params, profiling=True, warm_start=warm, **kw)
+    rp_plain = W.make_rb_params(params, **kw)          # reference semantics: every solve starts from zero
     stream = torch.cuda.current_stream()
     for _ in range(args.pre_roll):
         world.step(rp)
     x0, u0 = world.state()                 # state the timed region (and every baseline) starts from
-    for _ in range(max(3, args.warmup)):
-        world.step(rp)
     world.step(rp_prof)                    # phase split and byte accounting (outside the timed region)
     phases = world.profile_times()
     stats = world.stats()
+    world.set_state(x0, u0)
+    for _ in range(max(3, args.warmup)):
+        world.step(rp)
     world.set_state(x0, u0)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     if world_size > 1:
@@ -250,26 +256,28 @@ def run_ours(args):
     n_scenes = world.n_scenes
     value = world_size * n_scenes * args.steps / (total_ms / 1000.0)
     residuals = np.array([s.residual for s in after if s.n_contacts > 0])
+    iters = np.array([s.iterations + 1 if s.exitcode == 3 else max_it for s in after if s.n_contacts > 0])
+    ncont = np.array([s.n_contacts for s in after])
     unconverged = int(sum(1 for s in after if s.n_contacts > 0 and s.exitcode != 3)) \
-        if args.termination == "residual" else None
+        if args.termination != "merit" else None
 
     # plain one-scene-per-launch FP64 baseline (same scheme, same tolerance, same starting states)
     plain = None
-    if n_scenes > 1:
+    if n_scenes > 1 and args.plain_scenes > 0:
         x0r, u0r = x0.reshape(-1, 7), u0.reshape(-1, 6)
         pts = []
         for s in range(min(args.plain_scenes, n_scenes)):
             b0, b1 = world.scene_start[s], world.scene_start[s + 1]
             w1 = W.DeviceWorld(arrays[s], device=dev, max_iterations=max_it)
             w1.set_state(x0r[b0:b1], u0r[b0:b1])
-            w1.step(rp)                    # sizes its work lists
+            w1.step(rp_plain)              # sizes its work lists
             w1.set_state(x0r[b0:b1], u0r[b0:b1])
             torch.cuda.synchronize()
-            pts.append(timed_steps(w1, rp, args.steps, stream, flush))
+            pts.append(timed_steps(w1, rp_plain, args.steps, stream, flush))
         pt = np.concatenate(pts)
         plain = {"value": len(pt) / (pt.sum() / 1000.0), "unit": "scene-steps/s", "scenes_sampled": len(pts),
                  "p50_ms": float(np.percentile(pt, 50)), "p99_ms": float(np.percentile(pt, 99)),
-                 "method": "each scene alone: one rb_step launch sequence per scene-step, FP64"}
+                 "method": "each scene alone: one rb_step launch sequence per scene-step, FP64, no warm start"}
 
     # end to end through the public API, host buffers in and out every step
     e2e = None
@@ -279,6 +287,7 @@ def run_ours(args):
             engine.stepper = GpuStepper(device=dev, termination=args.termination,
                                         residual_tolerance=args.tolerance)
             engine.params.proximal_solver = None if args.scheme == "rigid_gauss_seidel" else args.scheme
+            engine.params.warm_start = warm
             engine.stepper.step(engine.params.time_step, engine, False)
             engine_io.write_back(engine, x0.reshape(-1, 7), u0.reshape(-1, 6))
             torch.cuda.synchronize()
@@ -336,12 +345,12 @@ def run_ours(args):
     achieved = nbytes / dt_s / 1e9 if dt_s > 0 else 0.0
 
     cpu = None
-    if rank == 0:
+    if rank == 0 and args.cpu_seconds > 0:
         cv, info = cpu_baseline(arrays, args, cpu_pool_workers if n_scenes > 1 else 1)
         cpu = dict(value=cv, unit="scene-steps/s", **info)
 
     cfg.update({"scheme": args.scheme, "termination": args.termination, "tolerance": args.tolerance,
-                "precision": "fp64", "pre_roll_steps": args.pre_roll, "contacts_per_step": int(K),
+                "precision": "fp64", "warm_start": warm, "pre_roll_steps": args.pre_roll, "contacts_per_step": int(K),
                 "sweeps_per_step_contacts": int(sweeps), "l2": "256 MB buffer written between timed steps",
                 "parallelism": "replicas" if world_size > 1 else "single"})
     line = {
@@ -354,7 +363,10 @@ def run_ours(args):
         "speedup_vs_plain": (value / world_size) / plain["value"] if plain else None,
         "residual": {"max": float(residuals.max()) if len(residuals) else 0.0,
                      "median": float(np.median(residuals)) if len(residuals) else 0.0,
-                     "unconverged_scenes": unconverged},
+                     "unconverged_scenes": unconverged,
+                     "sweeps_p50_p90_max": [float(np.percentile(iters, 50)), float(np.percentile(iters, 90)),
+                                            int(iters.max())] if len(iters) else None,
+                     "contacts_per_scene_p50_max": [float(np.percentile(ncont, 50)), int(ncont.max())]},
         "roofline": {"bound": "hbm", "kernel_phase": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None, "algorithmic_bytes": int(nbytes),
                      "bytes_model": model, "phase_ms": dt_s * 1000.0,

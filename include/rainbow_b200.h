@@ -50,7 +50,10 @@ extern "C" {
 
 /* termination rules */
 #define RB_TERMINATE_MERIT 0          /* the reference's iterate-change merit (problem.py:53) */
-#define RB_TERMINATE_RESIDUAL 1       /* complementarity residual <= residual_tolerance */
+#define RB_TERMINATE_RESIDUAL 1       /* complementarity residual <= residual_tolerance; the reference's merit
+                                         rule still rejects iterates and adapts r */
+#define RB_TERMINATE_RESIDUAL_FIXED_R 2 /* complementarity residual <= residual_tolerance; every sweep is
+                                         accepted and r stays at its initial value */
 
 /* Shapes (rainbow/simulators/prox_rigid_bodies/types.py:82 Shape): body-frame mesh and signed distance grid. */
 typedef struct rb_shapes {
@@ -91,6 +94,7 @@ typedef struct rb_bodies {
     int32_t n_body_vertices;      /* sum over bodies of their shape's vertex count */
     int32_t n_body_triangles;     /* sum over bodies of their shape's triangle count */
     int32_t n_clusters;           /* sum over bodies of ceil(triangles / 32) */
+    int32_t max_scene_bodies;     /* bodies of the largest scene (sizes the solver's on-chip body arrays) */
     const int32_t* body_v0;       /* n_bodies+1 prefix sums of per-body vertex counts */
     const int32_t* body_t0;       /* n_bodies+1 prefix sums of per-body triangle counts */
     const int32_t* body_c0;       /* n_bodies+1 prefix sums of per-body 32-triangle cluster counts */
@@ -133,6 +137,10 @@ typedef struct rb_params {
     int32_t termination;          /* RB_TERMINATE_* */
     double residual_tolerance;    /* used by RB_TERMINATE_RESIDUAL */
     int32_t profiling;            /* nonzero: fill energies and residual histories */
+    int32_t warm_start;           /* nonzero: start each contact's impulse from the previous step's solution for
+                                     the same (body pair, side, triangle) found in rb_outputs.cache_*; the
+                                     reference always starts from zero (contacts.py:53), so this is off for
+                                     parity runs */
 } rb_params;
 
 /* Per-scene results of one step. */
@@ -144,8 +152,8 @@ typedef struct rb_scene_stats {
     int32_t post_iterations;
     int32_t post_exitcode;
     int32_t n_pairs;              /* body pairs with overlapping bounding boxes */
-    int32_t n_candidates;         /* triangles searched */
-    int32_t n_leaf_overlaps;      /* overlapping leaf (triangle) pairs: the profile key number_of_overlaps */
+    int32_t n_candidates;         /* triangles searched (profiling only) */
+    int32_t n_leaf_overlaps;      /* overlapping leaf (triangle) pairs: profile key number_of_overlaps (profiling only) */
     int32_t n_grid_lookups;       /* signed distance lookups of the contact search (profiling only) */
     double merit;                 /* last global merit */
     double residual;              /* complementarity residual of the returned solution (when computed) */
@@ -165,6 +173,15 @@ typedef struct rb_outputs {
     double* residuals;            /* n_scenes * max_iterations (profiling), may be NULL */
     int32_t* status;              /* 1 int32: RB_STATUS_* bits, OR-ed by the step (caller zeroes it) */
     int32_t* n_contacts_total;    /* 1 int32 */
+    int32_t* needed;              /* 3 int32: body pairs, candidates and contacts the step produced (a stage
+                                     after an overflow reports 0); used to size the capacities */
+    /* contact cache carried from step to step for warm starting (capacity rb_caps.contact_capacity): keys
+       (lower body index << 31 | higher body index, side << 30 | triangle) in ascending order and the 4
+       impulses per contact.  Read when params->warm_start is set, always rewritten at the end of a step.
+       Set *cache_count = 0 when the scene batch changes. */
+    int64_t* cache_key;           /* 2 per contact */
+    double* cache_sol;            /* 4 per contact */
+    int32_t* cache_count;         /* 1 int32 */
 } rb_outputs;
 
 /* Library ABI version (RB_ABI_VERSION). */

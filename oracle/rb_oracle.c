@@ -863,10 +863,14 @@ static void solve_rigid(const Problem* P, const double* params, double* r, const
         double global_merit = 0.0;
         sweep_gs(P, r, b, mu, x, w, normal_only);
         double merit = merit_inf(x, sol, n);
-        if (tol_mode == 1) {   /* stop on the complementarity residual only; merit still adapts r */
+        if (tol_mode >= 1) {   /* stop on the complementarity residual only; merit still adapts r (mode 1) */
             double res = complementarity_residual(P, b, mu, x, w);
             if (residuals) residuals[it] = res;
             if (res <= tol) { memcpy(sol, x, sizeof(double) * n); *iterations = it; *exitcode = 3; break; }
+            if (tol_mode == 2) {   /* fixed r, every sweep accepted */
+                memcpy(sol, x, sizeof(double) * n);
+                continue;
+            }
             if (merit > last_merit) {
                 for (int i = 0; i < n; ++i) r[i] = params[P_NU_REDUCE] * r[i];
                 memcpy(x, sol, sizeof(double) * n);
@@ -924,6 +928,7 @@ static void solve_interface(const Problem* P, const double* params, int scheme, 
             double res = complementarity_residual(P, b, mu, x, w);
             if (residuals) residuals[it] = res;
             if (res <= tol) { memcpy(sol, x, sizeof(double) * n); *iterations = it; *exitcode = 3; break; }
+            if (tol_mode == 2) { memcpy(sol, x, sizeof(double) * n); continue; }   /* fixed r, always accept */
         }
         if (merit > last_merit) {
             for (int i = 0; i < n; ++i) r[i] = params[P_NU_REDUCE] * r[i];

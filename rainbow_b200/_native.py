@@ -20,7 +20,7 @@ STATUS_NONUNIT_NORMAL = 16
 STATUS_MESH_TOO_LARGE = 32
 
 SCHEME_RIGID_GS, SCHEME_GS, SCHEME_JACOBI, SCHEME_JACOBI_HYBRID, SCHEME_COLOURED_GS = 0, 1, 2, 3, 4
-TERMINATE_MERIT, TERMINATE_RESIDUAL = 0, 1
+TERMINATE_MERIT, TERMINATE_RESIDUAL, TERMINATE_RESIDUAL_FIXED_R = 0, 1, 2
 
 _vp = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -38,7 +38,7 @@ class RbBodies(ctypes.Structure):
         ("n_forces", _i32), ("scene_force_start", _vp), ("force_kind", _vp), ("force_params", _vp),
         ("scene_material_offset", _vp), ("scene_material_count", _vp), ("material_mu", _vp),
         ("material_eps", _vp),
-        ("n_body_vertices", _i32), ("n_body_triangles", _i32), ("n_clusters", _i32),
+        ("n_body_vertices", _i32), ("n_body_triangles", _i32), ("n_clusters", _i32), ("max_scene_bodies", _i32),
         ("body_v0", _vp), ("body_t0", _vp), ("body_c0", _vp), ("vert_body", _vp), ("tri_body", _vp),
         ("clu_body", _vp), ("x", _vp), ("u", _vp),
     ]
@@ -58,6 +58,7 @@ class RbParams(ctypes.Structure):
         ("too_small_merit_change", ctypes.c_double), ("contact_optimization_max_iterations", _i32),
         ("contact_optimization_tolerance", ctypes.c_double), ("envelope", ctypes.c_double), ("scheme", _i32),
         ("termination", _i32), ("residual_tolerance", ctypes.c_double), ("profiling", _i32),
+        ("warm_start", _i32),
     ]
 
 
@@ -73,7 +74,8 @@ class RbSceneStats(ctypes.Structure):
 class RbOutputs(ctypes.Structure):
     _fields_ = [("contact_ids", _vp), ("contact_p", _vp), ("contact_n", _vp), ("contact_g", _vp),
                 ("contact_sol", _vp), ("stats", _vp), ("residuals", _vp), ("status", _vp),
-                ("n_contacts_total", _vp)]
+                ("n_contacts_total", _vp), ("needed", _vp), ("cache_key", _vp), ("cache_sol", _vp),
+                ("cache_count", _vp)]
 
 
 # exported symbols and their ctypes signatures: every function declared in include/rainbow_b200.h

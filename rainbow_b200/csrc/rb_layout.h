@@ -51,6 +51,12 @@ struct Workspace {
     double* x;           // 4K
     double* xold;        // 4K
     double* mu;          // K
+    int64_t* ckey;       // 2K  contact keys (pair, side << 30 | triangle)
+    int32_t* lev_of;     // K   Gauss-Seidel level of each contact
+    int32_t* lev_order;  // K   contacts sorted by level (per scene)
+    int32_t* lev_ptr;    // K + S + 1 level boundaries (per scene)
+    int32_t* lev_cur;    // K + S + 1 scatter cursors
+    int32_t* cpred;      // 2K  previous contact on the same (non-fixed) body, per side, or -1
     // scans and counters
     int32_t* scan_tmp;   // kScanBlocks + 1
     int32_t* counters;   // 16
@@ -62,7 +68,7 @@ inline size_t align_up(size_t v) { return (v + 255) & ~size_t(255); }
 
 // Computes (and, when base != nullptr, assigns) every array; returns the total bytes.
 inline size_t layout(Workspace* ws, char* base, int64_t N, int64_t NV, int64_t NT, int64_t NC, int64_t P,
-                     int64_t C, int64_t K) {
+                     int64_t C, int64_t K, int64_t S) {
     size_t off = 0;
     auto take = [&](auto*& ptr, int64_t count) {
         using T = std::remove_reference_t<decltype(*ptr)>;
@@ -83,6 +89,9 @@ inline size_t layout(Workspace* ws, char* base, int64_t N, int64_t NV, int64_t N
     take(w->J, 48 * K); take(w->WJT, 48 * K);
     take(w->b, 4 * K); take(w->diag, 4 * K); take(w->r, 4 * K); take(w->x, 4 * K); take(w->xold, 4 * K);
     take(w->mu, K);
+    take(w->ckey, 2 * K);
+    take(w->lev_of, K); take(w->lev_order, K); take(w->lev_ptr, K + S + 1); take(w->lev_cur, K + S + 1);
+    take(w->cpred, 2 * K);
     take(w->scan_tmp, kScanBlocks + 1); take(w->counters, 16);
     return off;
 }

@@ -36,6 +36,7 @@ namespace rb {
 constexpr int kWarpsPerBlock = 4;
 constexpr int kBlock = 32 * kWarpsPerBlock;
 constexpr int kAbort = 15;   // counters[kAbort]: nonzero once a capacity was exceeded
+constexpr int kSolveSmemBodies = 4608;   // 216 KB of body accumulators per solver block
 
 // ---------------------------------------------------------------------------------------------------------
 // small helpers
@@ -146,6 +147,7 @@ __global__ void k_zero_i32(int32_t* p, int n) {
 struct StepArgs;
 // capacity check after a scan: a total above the capacity aborts the rest of the step
 __global__ void k_check(int32_t* counters, int which, int cap, int bit, int32_t* status) {
+    if (counters[kAbort]) return;   // an earlier stage overflowed: this stage's total is not meaningful
     if (counters[which] > cap) {
         atomicOr(counters + kAbort, bit);
         atomicOr(status, bit);
@@ -335,7 +337,8 @@ struct MidShared {
     uint32_t maskB[kMaxClustersPerShape];
 };
 
-template <bool WRITE>
+// single pass: each pair reserves room for its candidates with one atomic and writes them in ascending
+// (side, triangle) order; pair_items[p] = first candidate of the pair, pair_itemsA[p] = number of candidates
 __global__ void __launch_bounds__(kBlock) k_mid(const StepArgs a) {
     __shared__ MidShared sm[kWarpsPerBlock];
     MidShared& S = sm[threadIdx.x >> 5];
@@ -352,7 +355,7 @@ __global__ void __launch_bounds__(kBlock) k_mid(const StepArgs a) {
         const double* rootB = a.ws.root + 6 * B;
         if (ncA > kMaxClustersPerShape || ncB > kMaxClustersPerShape) {
             if (lane == 0) { atomicOr(a.out.status, RB_STATUS_MESH_TOO_LARGE); atomicOr(a.ws.counters + kAbort, RB_STATUS_MESH_TOO_LARGE); }
-            if (!WRITE && lane == 0) { a.ws.pair_items[p] = 0; a.ws.pair_itemsA[p] = 0; a.ws.pair_ovl[p] = 0; }
+            if (lane == 0) { a.ws.pair_items[p] = 0; a.ws.pair_itemsA[p] = 0; a.ws.pair_ovl[p] = 0; }
             continue;
         }
         int nA = 0, nB = 0;
@@ -391,7 +394,7 @@ __global__ void __launch_bounds__(kBlock) k_mid(const StepArgs a) {
                     const double* LB = a.ws.leaf + 6 * (size_t)(tB0 + 32 * cb + jb);
                     if (validA && overlap(LA, LB)) { hitA = true; hitB |= 1u << jb; }
                 }
-                if (!WRITE) n_ovl += __popc(hitB);
+                n_ovl += __popc(hitB);
                 hitB = __reduce_or_sync(0xffffffffu, hitB);
                 if (lane == 0) S.maskB[ib] |= hitB;
             }
@@ -404,11 +407,12 @@ __global__ void __launch_bounds__(kBlock) k_mid(const StepArgs a) {
         for (int k = lane; k < nB; k += 32) cntB += __popc(S.maskB[k]);
         cntA = __reduce_add_sync(0xffffffffu, cntA);
         cntB = __reduce_add_sync(0xffffffffu, cntB);
-        if (!WRITE) {
-            n_ovl = __reduce_add_sync(0xffffffffu, n_ovl);
-            if (lane == 0) { a.ws.pair_items[p] = cntA + cntB; a.ws.pair_itemsA[p] = cntA; a.ws.pair_ovl[p] = n_ovl; }
-        } else {
-            int pos = a.ws.pair_items[p];
+        n_ovl = __reduce_add_sync(0xffffffffu, n_ovl);
+        int pos = 0;
+        if (lane == 0) pos = atomicAdd(a.ws.counters + kNItems, cntA + cntB);
+        pos = __shfl_sync(0xffffffffu, pos, 0);
+        if (lane == 0) { a.ws.pair_items[p] = pos; a.ws.pair_itemsA[p] = cntA + cntB; a.ws.pair_ovl[p] = n_ovl; }
+        if (pos + cntA + cntB <= a.caps.item_capacity) {   // otherwise k_check aborts the step
             for (int side = 0; side < 2; ++side) {
                 const int n = side ? nB : nA;
                 const int16_t* list = side ? S.listB : S.listA;
@@ -521,7 +525,7 @@ __global__ void k_dedup(const StepArgs a) {
     const int lane = threadIdx.x & 31;
     const int n_pairs = a.ws.counters[kNPairs];
     for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < n_pairs; p += (gridDim.x * blockDim.x) >> 5) {
-        const int i0 = a.ws.pair_items[p], i1 = a.ws.pair_items[p + 1];
+        const int i0 = a.ws.pair_items[p], i1 = i0 + a.ws.pair_itemsA[p];
         int kept = 0;
         int base = WRITE ? a.ws.pair_cont[p] : 0;
         const int A = a.ws.pairs[2 * p], B = a.ws.pairs[2 * p + 1];
@@ -559,6 +563,10 @@ __global__ void k_dedup(const StepArgs a) {
                     }
                     a.out.contact_g[k] = a.ws.item_g[i];
                     a.ws.c_scene[k] = scene_of(a.bd.scene_start, a.bd.n_scenes, A);
+                    // key of the contact for warm starting: contacts come out in ascending key order
+                    a.ws.ckey[2 * k] = ((int64_t)A << 31) | (int64_t)B;
+                    a.ws.ckey[2 * k + 1] = (int64_t)(((unsigned)a.ws.item_tri[i] >> 31) << 30) |
+                                           (int64_t)(a.ws.item_tri[i] & 0x7fffffff);
                 }
             }
             kept += __popc(bal);
@@ -676,6 +684,21 @@ __global__ void k_contacts(const StepArgs a) {
             a.out.contact_sol[4 * k + row] = 0.0;
         }
         a.ws.mu[k] = mu;
+        if (a.pr.warm_start && a.out.cache_count) {   // previous impulses of the same contact (binary search)
+            const int64_t k1 = a.ws.ckey[2 * k], k2 = a.ws.ckey[2 * k + 1];
+            int lo_i = 0, hi_i = min(*a.out.cache_count, a.caps.contact_capacity);
+            while (lo_i < hi_i) {
+                const int mid = (lo_i + hi_i) >> 1;
+                const int64_t m1 = a.out.cache_key[2 * mid], m2 = a.out.cache_key[2 * mid + 1];
+                if (m1 < k1 || (m1 == k1 && m2 < k2)) lo_i = mid + 1; else hi_i = mid;
+            }
+            if (lo_i < *a.out.cache_count && a.out.cache_key[2 * lo_i] == k1 && a.out.cache_key[2 * lo_i + 1] == k2)
+                for (int row = 0; row < 4; ++row) {
+                    const double v = a.out.cache_sol[4 * lo_i + row];
+                    a.ws.x[4 * k + row] = v;
+                    a.out.contact_sol[4 * k + row] = v;
+                }
+        }
     }
 }
 
@@ -711,12 +734,48 @@ __global__ void k_body_contacts_sort(const StepArgs a) {
         while (j >= 0 && l[j] > v) { l[j + 1] = l[j]; --j; }
         l[j + 1] = v;
     }
+    // predecessor of each contact along this body: the chain the Gauss-Seidel levels follow
+    int prev = -1;
+    for (int i = 0; i < n; ++i) {
+        const int code = l[i];
+        a.ws.cpred[code] = prev;   // code = (k << 1) | side
+        prev = code >> 1;
+    }
+}
+__global__ void k_preds_init(const StepArgs a) {
+    if (a.ws.counters[kAbort]) return;
+    const int K = a.ws.counters[kNContacts];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 2 * K; i += gridDim.x * blockDim.x) a.ws.cpred[i] = -1;
 }
 
-// w[b] = (WJT x) rows of body b: sequential over its contacts (ascending) and their 4 columns
+// w[b] = (WJT x) rows of body b: sequential over its contacts (ascending) and their 4 columns.  The loads of
+// four contacts are issued before their products are accumulated (in order) to overlap their latency.
 __device__ __forceinline__ void body_wjt_dot(const Workspace& ws, int b, const double* x, double* out6) {
     double s[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    for (int e = ws.bc_ptr[b]; e < ws.bc_ptr[b + 1]; ++e) {
+    const int e0 = ws.bc_ptr[b], e1 = ws.bc_ptr[b + 1];
+    int e = e0;
+    for (; e + 4 <= e1; e += 4) {
+        int code[4];
+        for (int j = 0; j < 4; ++j) code[j] = ws.bc_list[e + j];
+        double xv[4][4];
+        const double* Wk[4];
+        for (int j = 0; j < 4; ++j) {
+            const int k = code[j] >> 1;
+            Wk[j] = ws.WJT + 48 * (size_t)k + 6 * (code[j] & 1);
+            for (int i = 0; i < 4; ++i) xv[j][i] = x[4 * k + i];
+        }
+        for (int d = 0; d < 6; ++d) {
+            double t = s[d];
+            for (int j = 0; j < 4; ++j) {
+                t += Wk[j][d] * xv[j][0];
+                t += Wk[j][12 + d] * xv[j][1];
+                t += Wk[j][24 + d] * xv[j][2];
+                t += Wk[j][36 + d] * xv[j][3];
+            }
+            s[d] = t;
+        }
+    }
+    for (; e < e1; ++e) {
         const int code = ws.bc_list[e];
         const int k = code >> 1, side = code & 1;
         const double* Wk = ws.WJT + 48 * (size_t)k + 6 * side;
@@ -734,7 +793,9 @@ __device__ __forceinline__ void body_wjt_dot(const Workspace& ws, int b, const d
 }
 
 // ---------------------------------------------------------------------------------------------------------
-// solver: one block per scene
+// solver: one thread group per scene -- a warp for small scenes (warp-synchronous, many scenes per SM), a
+// block for large ones.  Every member of the group evaluates the solver's control logic redundantly from the
+// same reduced values, so no broadcast through shared memory is needed.
 // ---------------------------------------------------------------------------------------------------------
 struct SceneRange { int b0, b1, c0, c1; };
 __device__ __forceinline__ SceneRange scene_range(const StepArgs& a, int s) {
@@ -748,240 +809,355 @@ __device__ __forceinline__ SceneRange scene_range(const StepArgs& a, int s) {
     return R;
 }
 
-__device__ __forceinline__ double block_max(double v, double* red) {
-    for (int o = 16; o > 0; o >>= 1) {
-        const double t = __shfl_xor_sync(0xffffffffu, v, o);
-        v = (t > v || t != t) ? t : v;
+__device__ __forceinline__ double nanmax(double v, double t) { return (t > v || t != t) ? t : v; }
+
+struct WarpGroup {
+    __device__ __forceinline__ int rank() const { return threadIdx.x & 31; }
+    __device__ __forceinline__ int size() const { return 32; }
+    __device__ __forceinline__ void sync() const { __syncwarp(); }
+    __device__ __forceinline__ bool any(bool p) const { __syncwarp(); return __any_sync(0xffffffffu, p); }
+    __device__ __forceinline__ double max(double v) const {
+        for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        return v;
     }
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    __syncthreads();
-    if (lane == 0) red[wid] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    __device__ __forceinline__ int imax(int v) const {
+        for (int o = 16; o > 0; o >>= 1) v = ::max(v, __shfl_xor_sync(0xffffffffu, v, o));
+        return v;
+    }
+};
+
+struct BlockGroup {
+    double* red;   // 33 doubles of shared memory
+    int* ired;     // 33 ints of shared memory
+    __device__ __forceinline__ int rank() const { return threadIdx.x; }
+    __device__ __forceinline__ int size() const { return blockDim.x; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+    __device__ __forceinline__ bool any(bool p) const { return __syncthreads_or(p); }
+    __device__ double max(double v) const {
+        for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        __syncthreads();
+        if (lane == 0) red[wid] = v;
+        __syncthreads();
         double m = red[0];
-        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = (red[w] > m || red[w] != red[w]) ? red[w] : m;
-        red[32] = m;
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) m = nanmax(m, red[k]);
+        __syncthreads();
+        return m;
     }
-    __syncthreads();
-    return red[32];
+    __device__ int imax(int v) const {
+        for (int o = 16; o > 0; o >>= 1) v = ::max(v, __shfl_xor_sync(0xffffffffu, v, o));
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        __syncthreads();
+        if (lane == 0) ired[wid] = v;
+        __syncthreads();
+        int m = ired[0];
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) m = ::max(m, ired[k]);
+        __syncthreads();
+        return m;
+    }
+};
+
+// Body accumulators w = WJT x of one scene: in shared memory when the scene fits, else in global memory.
+struct WView {
+    double* base;
+    int b0;
+    __device__ __forceinline__ double* at(int b) const { return base + 6 * (b - b0); }
+};
+
+// w for every body of the scene from x (sequential over the body's contacts: the order of WJT.dot(x))
+template <class G>
+__device__ __forceinline__ void scene_wjt(const StepArgs& a, const G& g, const SceneRange& R, const double* x, WView w) {
+    for (int bb = R.b0 + g.rank(); bb < R.b1; bb += g.size()) {
+        double* o = w.at(bb);
+        if (a.bd.fixed[bb]) { for (int d = 0; d < 6; ++d) o[d] = 0.0; continue; }
+        body_wjt_dot(a.ws, bb, x, o);
+    }
+    g.sync();
 }
 
-// serial Gauss-Seidel sweep over contacts c0..c1-1 by one warp (contacts.py:66-107)
-__device__ void gs_sweep_warp(const StepArgs& a, int c0, int c1, const double* b, const double* r, double* x,
-                              bool normal_only) {
-    const int lane = threadIdx.x & 31;
-    double* w = a.ws.w;
-    for (int k = c0; k < c1; ++k) {
-        const int lo = a.ws.lohi[2 * k], hi = a.ws.lohi[2 * k + 1];
-        const double* J = a.ws.J + 48 * (size_t)k;
-        double z = 0.0, xo = 0.0;
-        if (lane < 4) {
-            xo = x[4 * k + lane];
-            const double jw = jrow_dot(J + 12 * lane, w + 6 * lo, w + 6 * hi);
-            z = xo - r[4 * k + lane] * (jw + b[4 * k + lane]);
+// One projected Gauss-Seidel update of contact k (contacts.py:78-107): z from the current w, normal impulse
+// clamped at zero, friction projected on the ball of radius mu x_n (or zeroed for post-stabilisation),
+// then w += WJT[:, block] delta with the reference's term order.
+__device__ __forceinline__ void gs_contact(const StepArgs& a, int k, const double* b, const double* r, double* x,
+                                           WView w, bool normal_only) {
+    const int lo = a.ws.lohi[2 * k], hi = a.ws.lohi[2 * k + 1];
+    const double* J = a.ws.J + 48 * (size_t)k;
+    const double* Wk = a.ws.WJT + 48 * (size_t)k;
+    const double* wlo = w.at(lo);
+    const double* whi = w.at(hi);
+    double xo[4], z[4];
+    for (int row = 0; row < 4; ++row) {
+        xo[row] = x[4 * k + row];
+        z[row] = xo[row] - r[4 * k + row] * (jrow_dot(J + 12 * row, wlo, whi) + b[4 * k + row]);
+    }
+    const double xn = z[0] > 0.0 ? z[0] : 0.0;
+    double f[3];
+    if (normal_only) { f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; }
+    else prox_sphere(z[1], z[2], z[3], a.ws.mu[k], xn, f);
+    const double d0 = xn - xo[0], d1 = f[0] - xo[1], d2 = f[1] - xo[2], d3v = f[2] - xo[3];
+    x[4 * k] = xn; x[4 * k + 1] = f[0]; x[4 * k + 2] = f[1]; x[4 * k + 3] = f[2];
+    for (int side = 0; side < 2; ++side) {
+        const int bb = side ? hi : lo;
+        if (a.bd.fixed[bb]) continue;
+        double* wb = w.at(bb);
+        const double* Ws = Wk + 6 * side;
+        for (int d = 0; d < 6; ++d) {
+            double t = 0.0;
+            t += Ws[d] * d0;
+            t += Ws[12 + d] * d1;
+            t += Ws[24 + d] * d2;
+            t += Ws[36 + d] * d3v;
+            wb[d] = wb[d] + t;
         }
-        const double z0 = __shfl_sync(0xffffffffu, z, 0), z1 = __shfl_sync(0xffffffffu, z, 1);
-        const double z2 = __shfl_sync(0xffffffffu, z, 2), z3 = __shfl_sync(0xffffffffu, z, 3);
-        const double x0o = __shfl_sync(0xffffffffu, xo, 0), x1o = __shfl_sync(0xffffffffu, xo, 1);
-        const double x2o = __shfl_sync(0xffffffffu, xo, 2), x3o = __shfl_sync(0xffffffffu, xo, 3);
-        const double xn = z0 > 0.0 ? z0 : 0.0;
-        double f[3];
-        if (normal_only) { f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; }
-        else prox_sphere(z1, z2, z3, a.ws.mu[k], xn, f);
-        const double d0 = xn - x0o, d1 = f[0] - x1o, d2 = f[1] - x2o, d3v = f[2] - x3o;
-        if (lane == 0) { x[4 * k] = xn; x[4 * k + 1] = f[0]; x[4 * k + 2] = f[1]; x[4 * k + 3] = f[2]; }
-        if (lane < 12) {
-            const int side = lane / 6, d = lane - 6 * side;
-            const int bb = side ? hi : lo;
-            if (!a.bd.fixed[bb]) {
-                const double* Wk = a.ws.WJT + 48 * (size_t)k + 6 * side + d;
-                double s = 0.0;
-                s += Wk[0] * d0;
-                s += Wk[12] * d1;
-                s += Wk[24] * d2;
-                s += Wk[36] * d3v;
-                w[6 * bb + d] = w[6 * bb + d] + s;
-            }
+    }
+}
+
+// Wavefront levels of the serial Gauss-Seidel order: level(k) = 1 + max level of the earlier contacts on
+// k's non-fixed bodies.  Contacts of one level share no non-fixed body and every body sees its contacts in
+// ascending order, so sweeping level by level (each level in parallel, any order inside a level) reproduces
+// the serial sweep exactly.  The levels are the longest-path depths along the per-body predecessor chains,
+// found by parallel relaxation; contacts are then bucketed by level.  Returns the number of levels.
+template <class G>
+__device__ int scene_levels(const StepArgs& a, const G& g, const SceneRange& R, int s) {
+    for (int k = R.c0 + g.rank(); k < R.c1; k += g.size()) a.ws.lev_of[k] = 1;
+    g.sync();
+    for (;;) {
+        bool changed = false;
+        for (int k = R.c0 + g.rank(); k < R.c1; k += g.size()) {
+            const int p0 = a.ws.cpred[2 * k], p1 = a.ws.cpred[2 * k + 1];
+            const int l0 = p0 >= 0 ? *(volatile int*)(a.ws.lev_of + p0) : 0;
+            const int l1 = p1 >= 0 ? *(volatile int*)(a.ws.lev_of + p1) : 0;
+            const int l = 1 + max(l0, l1);
+            if (l != a.ws.lev_of[k]) { a.ws.lev_of[k] = l; changed = true; }
         }
-        __syncwarp();
+        if (!g.any(changed)) break;
+    }
+    int L = 0;
+    for (int k = R.c0 + g.rank(); k < R.c1; k += g.size()) L = max(L, a.ws.lev_of[k]);
+    L = g.imax(L);
+    int* ptr = a.ws.lev_ptr + R.c0 + s;   // ptr[l-1] .. ptr[l]: contacts of level l (1-based), ptr[L] = K
+    int* cur = a.ws.lev_cur + R.c0 + s;
+    for (int l = g.rank(); l <= L; l += g.size()) cur[l] = 0;
+    g.sync();
+    for (int k = R.c0 + g.rank(); k < R.c1; k += g.size()) atomicAdd(cur + a.ws.lev_of[k] - 1, 1);
+    g.sync();
+    if (g.rank() == 0) {
+        int acc = 0;
+        for (int l = 0; l < L; ++l) { const int c = cur[l]; ptr[l] = acc; cur[l] = acc; acc += c; }
+        ptr[L] = acc;
+    }
+    g.sync();
+    for (int k = R.c0 + g.rank(); k < R.c1; k += g.size())
+        a.ws.lev_order[R.c0 + atomicAdd(cur + a.ws.lev_of[k] - 1, 1)] = k;
+    g.sync();
+    return L;
+}
+
+template <class G>
+__device__ __forceinline__ void gs_sweep_levels(const StepArgs& a, const G& g, const SceneRange& R, int s, int L,
+                                                const double* b, const double* r, double* x, WView w,
+                                                bool normal_only) {
+    const int* ptr = a.ws.lev_ptr + R.c0 + s;
+    for (int l = 1; l <= L; ++l) {
+        const int start = ptr[l - 1], end = ptr[l];
+        for (int i = start + g.rank(); i < end; i += g.size())
+            gs_contact(a, a.ws.lev_order[R.c0 + i], b, r, x, w, normal_only);
+        g.sync();
     }
 }
 
 // complementarity residual ||x - prox(x - (A x + b))||_inf / max(1, ||x||_inf) with unit r (the tolerance
-// the solver modes are compared at); A x = J W J^T x through w2 = WJT x.  All threads of the block call it.
-__device__ double scene_residual(const StepArgs& a, const SceneRange& R, const double* x, double* red) {
-    for (int bb = R.b0 + threadIdx.x; bb < R.b1; bb += blockDim.x) {
-        if (a.bd.fixed[bb]) { for (int d = 0; d < 6; ++d) a.ws.w2[6 * bb + d] = 0.0; continue; }
-        body_wjt_dot(a.ws, bb, x, a.ws.w2 + 6 * bb);
-    }
-    __syncthreads();
+// the solver modes are compared at); A x = J W J^T x through w = WJT x (the accumulators are rebuilt from x
+// at the start of every sweep, so they are free to hold this product here).
+template <class G>
+__device__ double scene_residual(const StepArgs& a, const G& g, const SceneRange& R, const double* x, WView w) {
+    scene_wjt(a, g, R, x, w);
     double m = 0.0, xm = 0.0;
-    for (int k = R.c0 + threadIdx.x; k < R.c1; k += blockDim.x) {
+    for (int k = R.c0 + g.rank(); k < R.c1; k += g.size()) {
         const int lo = a.ws.lohi[2 * k], hi = a.ws.lohi[2 * k + 1];
         const double* J = a.ws.J + 48 * (size_t)k;
         double z[4];
         for (int row = 0; row < 4; ++row)
-            z[row] = x[4 * k + row] - (jrow_dot(J + 12 * row, a.ws.w2 + 6 * lo, a.ws.w2 + 6 * hi) + a.ws.b[4 * k + row]);
+            z[row] = x[4 * k + row] - (jrow_dot(J + 12 * row, w.at(lo), w.at(hi)) + a.ws.b[4 * k + row]);
         const double pn = z[0] > 0.0 ? z[0] : 0.0;
         double f[3];
         prox_sphere(z[1], z[2], z[3], a.ws.mu[k], pn, f);
         const double d[4] = {x[4 * k] - pn, x[4 * k + 1] - f[0], x[4 * k + 2] - f[1], x[4 * k + 3] - f[2]};
         for (int i = 0; i < 4; ++i) {
-            const double e = fabs(d[i]);
-            m = (e > m || e != e) ? e : m;
+            m = nanmax(m, fabs(d[i]));
             xm = fmax(xm, fabs(x[4 * k + i]));
         }
     }
-    const double mres = block_max(m, red);
-    const double mx = block_max(xm, red);
+    const double mres = g.max(m);
+    const double mx = g.max(xm);
     return mres / (mx > 1.0 ? mx : 1.0);
 }
 
-__global__ void __launch_bounds__(256) k_solve(const StepArgs a, int post) {
-    __shared__ double red[33];
-    __shared__ double ctl[4];     // last_merit, global_last, merit, decision
-    __shared__ int ictl[4];       // done, iterations, exitcode
-    if (a.ws.counters[kAbort]) return;
+// The proximal solve of one scene (gauss_seidel_solver.py:14 / solver_interface.py:123).
+template <class G>
+__device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, double* w_smem, int smem_bodies) {
     const int scheme = post ? RB_SCHEME_RIGID_GS : a.pr.scheme;
     const bool rigid = scheme == RB_SCHEME_RIGID_GS;
+    const bool jacobi = scheme == RB_SCHEME_JACOBI || scheme == RB_SCHEME_JACOBI_HYBRID;
     const int max_it = a.pr.max_iterations;
     double* x = a.ws.x;
     double* sol = post ? a.ws.xold : a.out.contact_sol;
     const double* b = a.ws.b;
     double* r = a.ws.r;
+    const SceneRange R = scene_range(a, s);
+    const int K = R.c1 - R.c0;
+    const int nb = R.b1 - R.b0;
+    rb_scene_stats* st = a.out.stats + s;
+    double* hist = (!post && a.out.residuals && a.pr.profiling) ? a.out.residuals + (size_t)s * a.caps.max_iterations
+                                                                : nullptr;
+    if (g.rank() == 0) {
+        if (!post) {
+            st->n_contacts = K; st->contact_start = R.c0; st->iterations = -1; st->exitcode = -1;
+            st->merit = 0.0; st->residual = 0.0; st->post_iterations = -1; st->post_exitcode = -1;
+        } else {
+            st->post_iterations = -1; st->post_exitcode = -1;
+        }
+    }
+    if (hist) for (int i = g.rank(); i < max_it; i += g.size()) hist[i] = INFINITY;
+    if (K == 0) { g.sync(); return; }
+    if (post) {   // steppers.py:32: no solve when no contact is deeper than min_gap
+        bool any = false;
+        for (int k = R.c0 + g.rank(); k < R.c1; k += g.size()) any |= (b[4 * k] != 0.0);
+        if (!g.any(any)) return;
+    }
+    const bool on_chip = w_smem != nullptr && nb <= smem_bodies;
+    const WView w = {on_chip ? w_smem : a.ws.w + 6 * R.b0, R.b0};
+    const int L = jacobi ? 0 : scene_levels(a, g, R, s);
+    const bool by_residual = !post && a.pr.termination != RB_TERMINATE_MERIT;
+    const bool fixed_r = !post && a.pr.termination == RB_TERMINATE_RESIDUAL_FIXED_R;
+    double last = INFINITY, global_last = INFINITY, shown = 0.0;
+    int iterations = max_it, exitcode = 0;
+    bool w_is_wjt_x = false;   // w already holds WJT x for the current x (left by the residual pass)
+    for (int it = 0; it < max_it; ++it) {
+        if (!w_is_wjt_x) scene_wjt(a, g, R, x, w);   // every sweep starts from w = WJT x (contacts.py:72)
+        if (jacobi) {               // proximal_contact/jacobi_solver.py:41-79
+            const bool hybrid = scheme == RB_SCHEME_JACOBI_HYBRID;
+            for (int k = R.c0 + g.rank(); k < R.c1; k += g.size()) {
+                const int lo = a.ws.lohi[2 * k], hi = a.ws.lohi[2 * k + 1];
+                const double* J = a.ws.J + 48 * (size_t)k;
+                double z[4];
+                for (int row = 0; row < 4; ++row)
+                    z[row] = x[4 * k + row] - r[4 * k + row] * (jrow_dot(J + 12 * row, w.at(lo), w.at(hi)) + b[4 * k + row]);
+                const double xn = z[0] > 0.0 ? z[0] : 0.0;
+                double f[3];
+                prox_sphere(z[1], z[2], z[3], a.ws.mu[k], hybrid ? xn : x[4 * k], f);
+                x[4 * k] = xn; x[4 * k + 1] = f[0]; x[4 * k + 2] = f[1]; x[4 * k + 3] = f[2];
+            }
+            g.sync();
+        } else {
+            gs_sweep_levels(a, g, R, s, L, b, r, x, w, post != 0);
+        }
+        // merit = ||x - sol||_inf (problem.py:53)
+        double m = 0.0;
+        for (int i = 4 * R.c0 + g.rank(); i < 4 * R.c1; i += g.size()) m = nanmax(m, fabs(x[i] - sol[i]));
+        const double merit = g.max(m);
+        const double res = by_residual ? scene_residual(a, g, R, x, w) : 0.0;
+        int decision = 0;   // 0 accept, 1 reject, 2 keep sol, 3 take x
+        bool stop = false, inc = false;
+        if (rigid) {        // gauss_seidel_solver.py:439-482
+            double gm;
+            if (merit > last) { decision = 1; gm = last > 0.0 ? last : 0.0; }
+            else {
+                inc = last - merit < a.pr.too_small_merit_change;
+                last = merit;
+                gm = merit > 0.0 ? merit : 0.0;
+            }
+            if (gm < a.pr.absolute_tolerance) { stop = true; exitcode = 1; }
+            else if (fabs(gm - global_last) < a.pr.relative_tolerance * global_last) { stop = true; exitcode = 2; }
+            global_last = gm;
+            shown = gm;
+        } else {            // solver_interface.py:88-113 then :50-69
+            if (merit < a.pr.absolute_tolerance) { stop = true; exitcode = 1; }
+            else if (fabs(merit - last) < a.pr.relative_tolerance * last) { stop = true; exitcode = 2; }
+            if (!stop) {
+                if (merit > last) decision = 1;
+                else { inc = last - merit < a.pr.too_small_merit_change; last = merit; }
+            } else decision = 2;
+            shown = merit;
+        }
+        if (by_residual) {  // stop only on the complementarity residual
+            shown = res;
+            if (res <= a.pr.residual_tolerance) { stop = true; exitcode = 3; decision = 3; }
+            else if (fixed_r) { stop = false; exitcode = 0; decision = 0; inc = false; }
+            else {
+                stop = false;
+                exitcode = 0;
+                if (decision == 2) {   // a merit test would have stopped: apply the accept/reject rule
+                    if (merit > last) decision = 1;
+                    else { inc = last - merit < a.pr.too_small_merit_change; last = merit; decision = 0; }
+                }
+            }
+        }
+        if (hist && g.rank() == 0) hist[it] = shown;
+        if (decision == 1) {
+            for (int i = 4 * R.c0 + g.rank(); i < 4 * R.c1; i += g.size()) {
+                r[i] = a.pr.nu_reduce * r[i];
+                x[i] = sol[i];
+            }
+        } else if (decision == 0) {
+            for (int i = 4 * R.c0 + g.rank(); i < 4 * R.c1; i += g.size()) {
+                sol[i] = x[i];
+                if (inc) r[i] = a.pr.nu_increase * r[i];
+            }
+        } else if (decision == 3) {   // converged by residual: the current iterate is the solution
+            for (int i = 4 * R.c0 + g.rank(); i < 4 * R.c1; i += g.size()) sol[i] = x[i];
+        }
+        // the residual pass computed w = WJT x; unless x was rolled back that is the next sweep's start
+        w_is_wjt_x = by_residual && decision != 1;
+        g.sync();
+        if (stop) { iterations = it; break; }
+    }
+    if (by_residual && exitcode != 3) shown = scene_residual(a, g, R, sol, w);   // residual of what is returned
+    if (g.rank() == 0) {
+        if (!post) {
+            st->iterations = iterations; st->exitcode = exitcode; st->merit = shown;
+            if (by_residual) st->residual = shown;
+        } else {
+            st->post_iterations = iterations; st->post_exitcode = exitcode;
+        }
+    }
+    g.sync();
+}
+
+constexpr int kWarpSceneMaxContacts = 2048;
+constexpr int kWarpSceneMaxBodies = 384;
+constexpr int kSolveWarpsPerBlock = 4;
+
+__device__ __forceinline__ int scene_contacts(const StepArgs& a, int s) {
+    const SceneRange R = scene_range(a, s);
+    return R.c1 - R.c0;
+}
+
+// scenes with at most kWarpSceneMaxContacts contacts and warp_bodies bodies: one warp each
+__global__ void __launch_bounds__(32 * kSolveWarpsPerBlock) k_solve_warps(const StepArgs a, int post, int warp_bodies) {
+    extern __shared__ double wsm[];
+    if (a.ws.counters[kAbort]) return;
+    const WarpGroup g;
+    const int wib = threadIdx.x >> 5;
+    double* w_smem = warp_bodies > 0 ? wsm + (size_t)wib * 6 * warp_bodies : nullptr;
+    for (int s = blockIdx.x * kSolveWarpsPerBlock + wib; s < a.bd.n_scenes; s += gridDim.x * kSolveWarpsPerBlock) {
+        const int nb = a.bd.scene_start[s + 1] - a.bd.scene_start[s];
+        if (scene_contacts(a, s) > kWarpSceneMaxContacts || nb > warp_bodies) continue;
+        solve_scene(a, g, s, post, w_smem, warp_bodies);
+    }
+}
+
+// the other scenes: one block each; the body accumulators are on chip up to smem_bodies bodies
+__global__ void __launch_bounds__(256) k_solve_blocks(const StepArgs a, int post, int warp_bodies, int smem_bodies) {
+    extern __shared__ double wsm[];
+    __shared__ double red[33];
+    __shared__ int ired[33];
+    if (a.ws.counters[kAbort]) return;
+    const BlockGroup g = {red, ired};
     for (int s = blockIdx.x; s < a.bd.n_scenes; s += gridDim.x) {
-        const SceneRange R = scene_range(a, s);
-        const int K = R.c1 - R.c0;
-        rb_scene_stats* st = a.out.stats + s;
-        if (threadIdx.x == 0) {
-            if (!post) {
-                st->n_contacts = K; st->contact_start = R.c0; st->iterations = -1; st->exitcode = -1;
-                st->merit = 0.0; st->residual = 0.0; st->post_iterations = -1; st->post_exitcode = -1;
-            }
-            else { st->post_iterations = -1; st->post_exitcode = -1; }
-        }
-        if (!post && a.out.residuals && a.pr.profiling)
-            for (int i = threadIdx.x; i < max_it; i += blockDim.x) a.out.residuals[(size_t)s * a.caps.max_iterations + i] = INFINITY;
-        if (K == 0) continue;
-        if (post) {   // steppers.py:32: no solve when no contact is deeper than min_gap
-            int any = 0;
-            for (int k = R.c0 + threadIdx.x; k < R.c1; k += blockDim.x) any |= (b[4 * k] != 0.0);
-            any = __syncthreads_or(any);
-            if (!any) continue;
-        }
-        if (threadIdx.x == 0) { ctl[0] = INFINITY; ctl[1] = INFINITY; ictl[0] = 0; ictl[1] = max_it; ictl[2] = 0; }
-        __syncthreads();
-        for (int it = 0; it < max_it; ++it) {
-            // w = WJT x for this scene's bodies
-            for (int bb = R.b0 + threadIdx.x; bb < R.b1; bb += blockDim.x) {
-                if (a.bd.fixed[bb]) { for (int d = 0; d < 6; ++d) a.ws.w[6 * bb + d] = 0.0; continue; }
-                body_wjt_dot(a.ws, bb, x, a.ws.w + 6 * bb);
-            }
-            __syncthreads();
-            if (scheme == RB_SCHEME_JACOBI || scheme == RB_SCHEME_JACOBI_HYBRID) {
-                const bool hybrid = scheme == RB_SCHEME_JACOBI_HYBRID;
-                for (int k = R.c0 + threadIdx.x; k < R.c1; k += blockDim.x) {
-                    const int lo = a.ws.lohi[2 * k], hi = a.ws.lohi[2 * k + 1];
-                    const double* J = a.ws.J + 48 * (size_t)k;
-                    double z[4];
-                    for (int row = 0; row < 4; ++row)
-                        z[row] = x[4 * k + row] - r[4 * k + row] * (jrow_dot(J + 12 * row, a.ws.w + 6 * lo, a.ws.w + 6 * hi) + b[4 * k + row]);
-                    const double xn = z[0] > 0.0 ? z[0] : 0.0;
-                    double f[3];
-                    prox_sphere(z[1], z[2], z[3], a.ws.mu[k], hybrid ? xn : x[4 * k], f);
-                    x[4 * k] = xn; x[4 * k + 1] = f[0]; x[4 * k + 2] = f[1]; x[4 * k + 3] = f[2];
-                }
-            } else {
-                if (threadIdx.x < 32) gs_sweep_warp(a, R.c0, R.c1, b, r, x, post != 0);
-            }
-            __syncthreads();
-            // merit = ||x - sol||_inf (problem.py:53)
-            double m = 0.0;
-            for (int i = 4 * R.c0 + threadIdx.x; i < 4 * R.c1; i += blockDim.x) {
-                const double e = fabs(x[i] - sol[i]);
-                m = (e > m || e != e) ? e : m;
-            }
-            const double merit = block_max(m, red);
-            const bool by_residual = !post && a.pr.termination == RB_TERMINATE_RESIDUAL;
-            double res = 0.0;
-            if (by_residual) res = scene_residual(a, R, x, red);
-            if (threadIdx.x == 0) {
-                const double last = ctl[0];
-                int decision = 0;  // 0 accept, 1 reject
-                int stop = 0;
-                if (rigid) {   // gauss_seidel_solver.py:439-482
-                    double gm;
-                    if (merit > last) { decision = 1; gm = last > 0.0 ? last : 0.0; }
-                    else {
-                        decision = 0;
-                        ctl[3] = (last - merit < a.pr.too_small_merit_change) ? 1.0 : 0.0;
-                        ctl[0] = merit;
-                        gm = merit > 0.0 ? merit : 0.0;
-                    }
-                    if (!post && a.out.residuals && a.pr.profiling) a.out.residuals[(size_t)s * a.caps.max_iterations + it] = gm;
-                    if (gm < a.pr.absolute_tolerance) { stop = 1; ictl[2] = 1; }
-                    else if (fabs(gm - ctl[1]) < a.pr.relative_tolerance * ctl[1]) { stop = 1; ictl[2] = 2; }
-                    ctl[1] = gm;
-                    ctl[2] = gm;
-                } else {       // solver_interface.py:88-113 then :50-69
-                    if (!post && a.out.residuals && a.pr.profiling) a.out.residuals[(size_t)s * a.caps.max_iterations + it] = merit;
-                    if (merit < a.pr.absolute_tolerance) { stop = 1; ictl[2] = 1; }
-                    else if (fabs(merit - last) < a.pr.relative_tolerance * last) { stop = 1; ictl[2] = 2; }
-                    if (!stop) {
-                        if (merit > last) decision = 1;
-                        else { decision = 0; ctl[3] = (last - merit < a.pr.too_small_merit_change) ? 1.0 : 0.0; ctl[0] = merit; }
-                    } else decision = 2;   // converged: keep sol as it is
-                    ctl[2] = merit;
-                }
-                if (by_residual) {
-                    // stop only on the complementarity residual; the merit logic still adapts r
-                    if (!post && a.out.residuals && a.pr.profiling) a.out.residuals[(size_t)s * a.caps.max_iterations + it] = res;
-                    ctl[2] = res;
-                    if (res <= a.pr.residual_tolerance) { stop = 1; ictl[2] = 3; decision = 3; }
-                    else {
-                        stop = 0;
-                        ictl[2] = 0;
-                        if (decision == 2) {   // a merit test would have stopped: apply the accept/reject rule
-                            if (merit > last) decision = 1;
-                            else { decision = 0; ctl[3] = (last - merit < a.pr.too_small_merit_change) ? 1.0 : 0.0; ctl[0] = merit; }
-                        }
-                    }
-                }
-                ictl[3] = decision;
-                if (stop) { ictl[0] = 1; ictl[1] = it; }
-            }
-            __syncthreads();
-            const int decision = ictl[3];
-            const double inc = ctl[3];
-            if (decision == 1) {
-                for (int i = 4 * R.c0 + threadIdx.x; i < 4 * R.c1; i += blockDim.x) {
-                    r[i] = a.pr.nu_reduce * r[i];
-                    x[i] = sol[i];
-                }
-            } else if (decision == 0) {
-                for (int i = 4 * R.c0 + threadIdx.x; i < 4 * R.c1; i += blockDim.x) {
-                    sol[i] = x[i];
-                    if (inc != 0.0) r[i] = a.pr.nu_increase * r[i];
-                }
-            } else if (decision == 3) {   // converged by residual: the current iterate is the solution
-                for (int i = 4 * R.c0 + threadIdx.x; i < 4 * R.c1; i += blockDim.x) sol[i] = x[i];
-            }
-            __syncthreads();
-            if (ictl[0]) break;
-        }
-        if (!post && a.pr.termination == RB_TERMINATE_RESIDUAL) {
-            if (ictl[2] != 3) {   // not converged: report the residual of the returned (last accepted) solution
-                const double rs = scene_residual(a, R, sol, red);
-                if (threadIdx.x == 0) ctl[2] = rs;
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) st->residual = ctl[2];
-        }
-        if (threadIdx.x == 0) {
-            if (!post) { st->iterations = ictl[1]; st->exitcode = ictl[2]; st->merit = ctl[2]; }
-            else { st->post_iterations = ictl[1]; st->post_exitcode = ictl[2]; }
-        }
-        __syncthreads();
+        const int nb = a.bd.scene_start[s + 1] - a.bd.scene_start[s];
+        if (scene_contacts(a, s) <= kWarpSceneMaxContacts && nb <= warp_bodies) continue;
+        solve_scene(a, g, s, post, smem_bodies > 0 ? wsm : nullptr, smem_bodies);
     }
 }
 
@@ -1054,9 +1230,10 @@ __global__ void k_scene_summary(const StepArgs a) {
     {
         const int p0 = a.ws.pair_cnt[R.b0], p1 = a.ws.pair_cnt[R.b1];
         st->n_pairs = p1 - p0;
-        st->n_candidates = a.ws.pair_items[p1] - a.ws.pair_items[p0];
-        int ovl = 0;
-        if (a.pr.profiling) for (int p = p0; p < p1; ++p) ovl += a.ws.pair_ovl[p];
+        int ovl = 0, cand = 0;
+        if (a.pr.profiling)
+            for (int p = p0; p < p1; ++p) { ovl += a.ws.pair_ovl[p]; cand += a.ws.pair_itemsA[p]; }
+        st->n_candidates = cand;
         st->n_leaf_overlaps = ovl;
     }
     if (!a.pr.profiling) return;
@@ -1092,8 +1269,27 @@ __global__ void k_scene_summary(const StepArgs a) {
     st->potential_energy = potential;
 }
 
+// keep this step's contact keys and impulses for the next step's warm start
+__global__ void k_cache_store(const StepArgs a) {
+    if (!a.out.cache_key || !a.out.cache_sol || !a.out.cache_count) return;
+    if (a.ws.counters[kAbort]) return;
+    const int K = min(a.ws.counters[kNContacts], a.caps.contact_capacity);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
+        a.out.cache_key[2 * k] = a.ws.ckey[2 * k];
+        a.out.cache_key[2 * k + 1] = a.ws.ckey[2 * k + 1];
+        for (int row = 0; row < 4; ++row) a.out.cache_sol[4 * k + row] = a.out.contact_sol[4 * k + row];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *a.out.cache_count = K;
+}
+
 __global__ void k_finish(const StepArgs a) {
     if (a.out.n_contacts_total) *a.out.n_contacts_total = a.ws.counters[kNContacts];
+    if (a.out.needed) {   // a stage after an overflow did not run: its total is reported as 0
+        const int ab = a.ws.counters[kAbort];
+        a.out.needed[0] = a.ws.counters[kNPairs];
+        a.out.needed[1] = (ab & RB_STATUS_PAIR_OVERFLOW) ? 0 : a.ws.counters[kNItems];
+        a.out.needed[2] = (ab & (RB_STATUS_PAIR_OVERFLOW | RB_STATUS_ITEM_OVERFLOW)) ? 0 : a.ws.counters[kNContacts];
+    }
 }
 
 // ---------------------------------------------------------------------------------------------------------
@@ -1159,7 +1355,7 @@ int rb_workspace_bytes(const rb_bodies* bd, const rb_caps* caps, size_t* bytes) 
         caps->pair_capacity < 0 || caps->item_capacity < 0 || caps->contact_capacity < 0)
         return fail(RB_ERR_ARG, "rb_workspace_bytes: negative size");
     *bytes = rb::layout(nullptr, nullptr, bd->n_bodies, bd->n_body_vertices, bd->n_body_triangles, bd->n_clusters,
-                        caps->pair_capacity, caps->item_capacity, caps->contact_capacity);
+                        caps->pair_capacity, caps->item_capacity, caps->contact_capacity, bd->n_scenes);
     return RB_OK;
 }
 
@@ -1184,7 +1380,7 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     StepArgs a;
     a.sh = *sh; a.bd = *bd; a.caps = *caps; a.pr = *pr; a.out = *out;
     rb::layout(&a.ws, (char*)workspace, bd->n_bodies, n_body_vertices, n_body_triangles, n_clusters,
-               caps->pair_capacity, caps->item_capacity, caps->contact_capacity);
+               caps->pair_capacity, caps->item_capacity, caps->contact_capacity, bd->n_scenes);
     if (n_body_vertices <= 0 || n_body_triangles <= 0 || n_clusters <= 0)
         return fail(RB_ERR_ARG, "rb_step: bodies without geometry");
     const int N = bd->n_bodies;
@@ -1206,10 +1402,8 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     k_check<<<1, 1, 0, st>>>(a.ws.counters, kNPairs, caps->pair_capacity, RB_STATUS_PAIR_OVERFLOW, out->status);
     k_pairs<true><<<blocks_for(32 * (int64_t)N, kBlock), kBlock, 0, st>>>(a);
     // mid phase
-    k_mid<false><<<G, kBlock, 0, st>>>(a);
-    scan(a.ws.pair_items, a.ws.counters + kNPairs, caps->pair_capacity, a.ws.scan_tmp, a.ws.counters + kNItems, st);
+    k_mid<<<G, kBlock, 0, st>>>(a);
     k_check<<<1, 1, 0, st>>>(a.ws.counters, kNItems, caps->item_capacity, RB_STATUS_ITEM_OVERFLOW, out->status);
-    k_mid<true><<<G, kBlock, 0, st>>>(a);
     prof_mark(prof, 2, st);
     // narrow phase
     k_narrow<<<G, 256, 0, st>>>(a);
@@ -1225,18 +1419,32 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     k_body_contacts_count<<<G, 256, 0, st>>>(a);
     scan(a.ws.bc_ptr, nullptr, N, a.ws.scan_tmp, nullptr, st);
     k_body_contacts_fill<<<G, 256, 0, st>>>(a);
+    k_preds_init<<<G, 256, 0, st>>>(a);
     k_body_contacts_sort<<<blocks_for(N, 128), 128, 0, st>>>(a);
     // solve, integrate, post-stabilise
-    const int sg = bd->n_scenes < 148 * 16 ? bd->n_scenes : 148 * 16;
-    k_solve<<<sg, 256, 0, st>>>(a, 0);
+    // small scenes: one warp each with its body accumulators in shared memory; large scenes: one block each
+    // a warp per scene only pays off once the scenes alone fill the GPU (>= 32 per SM); otherwise blocks
+    const int warp_bodies = bd->n_scenes < 148 * 32 ? 0
+                          : (bd->max_scene_bodies < kWarpSceneMaxBodies ? bd->max_scene_bodies : kWarpSceneMaxBodies);
+    const size_t warp_smem = (size_t)kSolveWarpsPerBlock * 6 * sizeof(double) * (warp_bodies > 0 ? warp_bodies : 1);
+    const int wg = (bd->n_scenes + kSolveWarpsPerBlock - 1) / kSolveWarpsPerBlock;
+    const int smem_bodies = bd->max_scene_bodies <= kSolveSmemBodies ? bd->max_scene_bodies : 0;
+    const size_t block_smem = (size_t)6 * sizeof(double) * (smem_bodies > 0 ? smem_bodies : 1);
+    const int bg = bd->n_scenes < 148 * 8 ? bd->n_scenes : 148 * 8;
+    if (warp_smem > 48 * 1024) cudaFuncSetAttribute(k_solve_warps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)warp_smem);
+    if (block_smem > 48 * 1024) cudaFuncSetAttribute(k_solve_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)block_smem);
+    if (warp_bodies > 0) k_solve_warps<<<wg, 32 * kSolveWarpsPerBlock, warp_smem, st>>>(a, 0, warp_bodies);
+    k_solve_blocks<<<bg, 256, block_smem, st>>>(a, 0, warp_bodies, smem_bodies);
     prof_mark(prof, 5, st);
     k_integrate<<<blocks_for(N, 128), 128, 0, st>>>(a);
     if (pr->use_post_stabilization) {
         k_post_setup<<<G, 128, 0, st>>>(a);
-        k_solve<<<sg, 256, 0, st>>>(a, 1);
+        if (warp_bodies > 0) k_solve_warps<<<wg, 32 * kSolveWarpsPerBlock, warp_smem, st>>>(a, 1, warp_bodies);
+        k_solve_blocks<<<bg, 256, block_smem, st>>>(a, 1, warp_bodies, smem_bodies);
         k_post_apply<<<blocks_for(N, 128), 128, 0, st>>>(a);
     }
     k_scene_summary<<<blocks_for(bd->n_scenes, 64), 64, 0, st>>>(a);
+    k_cache_store<<<G, 256, 0, st>>>(a);
     k_finish<<<1, 1, 0, st>>>(a);
     prof_mark(prof, 6, st);
     cudaError_t e = cudaGetLastError();

@@ -141,7 +141,7 @@ def direction_of_most_variance(P):
     """Row of the eigenvector matrix of the covariance at the largest eigenvalue (functions.py)."""
     C = P - np.mean(P.T, axis=1)
     values, vectors = np.linalg.eig(np.cov(C.T))
-    return vectors[np.argmax(values)]
+    return np.real(vectors[np.argmax(np.real(values))])
 
 
 def axis_sort(mesh, axis):

@@ -104,7 +104,8 @@ class GpuStepper:
         world = self._world_for(engine)
         scheme = getattr(engine.params, "proximal_solver", None) or "rigid_gauss_seidel"
         rp = W.make_rb_params(engine.params, dt=dt, scheme=scheme, termination=self.termination,
-                              residual_tolerance=self.residual_tolerance, profiling=profiling_on)
+                              residual_tolerance=self.residual_tolerance, profiling=profiling_on,
+                              warm_start=bool(getattr(engine.params, "warm_start", False)))
         status = world.step(rp)
         if status & 16:
             raise RuntimeError("ContactPoint.init() was called with non-unit size normal")

@@ -169,6 +169,7 @@ class Parameters:
         self.envelope = 0.1
         self.resolution = 64
         self.proximal_solver = None
+        self.warm_start = False   # start each solve from the previous step's impulses (the reference starts at 0)
 
 
 class Engine:

@@ -34,7 +34,7 @@ def params_from_vector(vec):
 
 
 def make_rb_params(p, dt=None, scheme="rigid_gauss_seidel", termination="merit", residual_tolerance=1e-6,
-                   profiling=False):
+                   profiling=False, warm_start=False):
     """rb_params from a Parameters-like mapping (types.py:356 field names)."""
     g = p.__getitem__ if isinstance(p, dict) else (lambda k: getattr(p, k))
     rp = N.RbParams()
@@ -50,9 +50,11 @@ def make_rb_params(p, dt=None, scheme="rigid_gauss_seidel", termination="merit",
     if scheme not in SCHEME_NAMES:
         raise NotImplementedError("Unknown solver scheme: %s" % scheme)
     rp.scheme = SCHEME_NAMES[scheme]
-    rp.termination = {"merit": N.TERMINATE_MERIT, "residual": N.TERMINATE_RESIDUAL}[termination]
+    rp.termination = {"merit": N.TERMINATE_MERIT, "residual": N.TERMINATE_RESIDUAL,
+                      "residual_fixed_r": N.TERMINATE_RESIDUAL_FIXED_R}[termination]
     rp.residual_tolerance = float(residual_tolerance)
     rp.profiling = int(bool(profiling))
+    rp.warm_start = int(bool(warm_start))
     return rp
 
 
@@ -249,6 +251,7 @@ class DeviceWorld:
         bd.n_bodies, bd.n_scenes = self.n_bodies, self.n_scenes
         bd.n_forces = self.n_forces
         bd.n_body_vertices, bd.n_body_triangles, bd.n_clusters = self.n_body_vertices, self.n_body_triangles, self.n_clusters
+        bd.max_scene_bodies = int(np.diff(self.scene_start).max())
         for f, key in BODY_FIELDS.items():
             setattr(bd, f, T[key].data_ptr())
         self.rb_bodies = bd
@@ -263,12 +266,26 @@ class DeviceWorld:
         self.t_csol = torch.zeros(4 * K, dtype=torch.float64, device=dev)
         self.t_stats = torch.zeros(self.n_scenes * ctypes.sizeof(N.RbSceneStats), dtype=torch.uint8, device=dev)
         self.t_resid = torch.zeros(self.n_scenes * self.caps.max_iterations, dtype=torch.float64, device=dev)
-        self.t_status = torch.zeros(2, dtype=torch.int32, device=dev)
+        self.t_status = torch.zeros(8, dtype=torch.int32, device=dev)   # status, n_contacts, needed[3]
         out = N.RbOutputs()
         out.contact_ids, out.contact_p, out.contact_n = self.t_cids.data_ptr(), self.t_cp.data_ptr(), self.t_cn.data_ptr()
         out.contact_g, out.contact_sol = self.t_cg.data_ptr(), self.t_csol.data_ptr()
         out.stats, out.residuals = self.t_stats.data_ptr(), self.t_resid.data_ptr()
         out.status, out.n_contacts_total = self.t_status.data_ptr(), self.t_status.data_ptr() + 4
+        out.needed = self.t_status.data_ptr() + 8
+        # warm-start cache: keep the previous contents across capacity growth
+        old_key = getattr(self, "t_cache_key", None)
+        old_sol = getattr(self, "t_cache_sol", None)
+        self.t_cache_key = torch.zeros(2 * K, dtype=torch.int64, device=dev)
+        self.t_cache_sol = torch.zeros(4 * K, dtype=torch.float64, device=dev)
+        if old_key is not None:
+            n = min(old_key.numel(), self.t_cache_key.numel()) // 2
+            self.t_cache_key[:2 * n].copy_(old_key[:2 * n])
+            self.t_cache_sol[:4 * n].copy_(old_sol[:4 * n])
+        else:
+            self.t_cache_count = torch.zeros(1, dtype=torch.int32, device=dev)
+        out.cache_key, out.cache_sol = self.t_cache_key.data_ptr(), self.t_cache_sol.data_ptr()
+        out.cache_count = self.t_cache_count.data_ptr()
         self.rb_outputs = out
         nbytes = ctypes.c_size_t(0)
         N.check(self.lib.rb_workspace_bytes(ctypes.byref(self.rb_bodies), ctypes.byref(self.caps), ctypes.byref(nbytes)),
@@ -277,12 +294,14 @@ class DeviceWorld:
         self.t_ws = torch.empty(self.workspace_bytes, dtype=torch.uint8, device=dev)
 
     def _grow(self, status):
+        need = self.t_status[2:5].cpu().numpy()
+        grow = lambda cap, n: int(max(2 * cap, 1.25 * int(n) + 64))  # noqa: E731
         if status & N.STATUS_PAIR_OVERFLOW:
-            self.caps.pair_capacity *= 2
+            self.caps.pair_capacity = grow(self.caps.pair_capacity, need[0])
         if status & N.STATUS_ITEM_OVERFLOW:
-            self.caps.item_capacity *= 2
+            self.caps.item_capacity = grow(self.caps.item_capacity, need[1])
         if status & N.STATUS_CONTACT_OVERFLOW:
-            self.caps.contact_capacity *= 2
+            self.caps.contact_capacity = grow(self.caps.contact_capacity, need[2])
         self._alloc()
 
     # ------------------------------------------------------------------------------------------------------
@@ -337,6 +356,11 @@ class DeviceWorld:
         hu.copy_(self.t_u, non_blocking=True)
         torch.cuda.current_stream(self.device).synchronize()
         return hx.numpy().reshape(-1, 7).copy(), hu.numpy().reshape(-1, 6).copy()
+
+
+    def reset_warm_start(self):
+        """Forget the contact impulses carried between steps."""
+        self.t_cache_count.zero_()
 
     def set_state(self, x, u):
         """Upload (x, u) through pinned staging buffers (asynchronous on the current stream)."""

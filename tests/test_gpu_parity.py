@@ -143,3 +143,47 @@ def test_profile_counts_match_oracle(oracle_lib):
     assert st.max_penetration == o["max_penetration"]
     times = world.profile_times()
     assert len(times) == 7 and times[6] > 0.0
+
+
+@pytest.mark.parametrize("termination,mode", [("residual", 1), ("residual_fixed_r", 2)])
+@pytest.mark.parametrize("scheme", ["rigid_gauss_seidel", "gauss_seidel"])
+def test_residual_termination_matches_oracle(oracle_lib, termination, mode, scheme):
+    """Solves stopped by the complementarity residual (tolerance 1e-6) stay bit-identical to the oracle."""
+    from rainbow_b200 import world as W
+    d = load_fixture("c1_boxes64")
+    p = W.params_from_vector(d["params"])
+    p["max_iterations"] = 200
+    world = _world(d, max_iterations=200)
+    sc = oracle_lib.OracleScene(d)
+    sc.set_param("max_iterations", 200)
+    for _ in range(3):
+        world.step(W.make_rb_params(p, scheme=scheme, termination=termination, residual_tolerance=1e-6))
+        o = sc.step(scheme=scheme, tol_mode=mode, tol=1e-6)
+        st = world.stats()[0]
+        assert (st.iterations, st.exitcode) == (o["iterations"], o["exitcode"])
+        np.testing.assert_array_equal(world.contacts()["sol"], o["sol"])
+        x, u = world.state()
+        np.testing.assert_array_equal(x.ravel(), o["x"])
+        np.testing.assert_array_equal(u.ravel(), o["u"])
+
+
+def test_warm_start_reuses_previous_impulses():
+    """Warm-started solves reach the same residual tolerance in fewer sweeps; the cache holds every contact."""
+    from rainbow_b200 import world as W
+    d = load_fixture("c1_boxes64")
+    p = W.params_from_vector(d["params"])
+    p["max_iterations"] = 200
+    sweeps = {}
+    for warm in (False, True):
+        world = _world(d, max_iterations=200)
+        total = 0
+        for s in range(int(d["steps"])):
+            world.step(W.make_rb_params(p, termination="residual_fixed_r", residual_tolerance=1e-6, warm_start=warm))
+            st = world.stats()[0]
+            assert st.exitcode == 3 and st.residual <= 1e-6
+            total += st.iterations + 1
+        assert int(world.t_cache_count.item()) == st.n_contacts
+        keys = world.t_cache_key[:2 * st.n_contacts].view(-1, 2).cpu().numpy()
+        assert all(tuple(keys[i]) < tuple(keys[i + 1]) for i in range(len(keys) - 1))
+        sweeps[warm] = total
+    assert sweeps[True] < sweeps[False]
