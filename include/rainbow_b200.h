@@ -214,6 +214,19 @@ int rb_step(const rb_shapes* shapes, const rb_bodies* bodies, const rb_caps* cap
    post-stabilisation, out[6] the whole step.  Returns RB_ERR_ARG if no profiled step was issued. */
 int rb_profile_times(float* out, int32_t n);
 
+/* rb_step without a workspace argument, for callers that cannot allocate device memory themselves -- for
+   example a host application that owns every device allocation through its own fixed pool, or a real-time
+   loop that must not call into an allocator once it runs.  The per-step temporaries live in a scratch array
+   that this library keeps in device global memory, RB_NOALLOC_SCRATCH_BYTES (16 MiB) on every device that
+   loads the library, held until the process exits.  Batches whose rb_workspace_bytes() exceeds that size are
+   rejected with RB_ERR_WORKSPACE.  The first call on a device looks up the array's device address (with that
+   device current); make that first call before any stream capture.  All calls share the one array: calls
+   that may overlap on the GPU (different streams, or different host threads) race and must be serialised by
+   the caller.  This entry point calls no allocator.  It has no counterpart in the reference. */
+#define RB_NOALLOC_SCRATCH_BYTES (16u << 20)
+int rb_step_noalloc(const rb_shapes* shapes, const rb_bodies* bodies, const rb_caps* caps, const rb_params* params,
+                    const rb_outputs* out, void* stream);
+
 /* Signed distance grid of a closed triangle mesh (replaces grid3.py:320 create_signed_distance's call to
    igl.signed_distance at grid3.py:338): values[i + I*(j + J*k)] for nodes min + spacing*(i,j,k).
    Unsigned distance by closest point on each triangle, sign by the generalized winding number. */

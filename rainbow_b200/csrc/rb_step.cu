@@ -25,6 +25,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "rainbow_b200.h"
@@ -1450,6 +1451,62 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(RB_ERR_CUDA, std::string("rb_step: ") + cudaGetErrorString(e));
     return RB_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------------------
+// rb_step_noalloc: the same step with its temporaries in a fixed scratch array of this library
+// ---------------------------------------------------------------------------------------------------------
+namespace {
+
+// Scratch of rb_step_noalloc.  In host code this name only stands for the array: the kernels receive the
+// device address looked up with cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[RB_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+// device address of the scratch array on the current device, looked up once per device
+int noalloc_scratch(void** ptr) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(RB_ERR_CUDA, std::string("rb_step_noalloc: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return fail(RB_ERR_UNSUPPORTED, "rb_step_noalloc: device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(RB_ERR_CUDA, std::string("rb_step_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = p;
+    }
+    *ptr = g_noalloc_ptr[dev];
+    return RB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rb_step_noalloc(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const rb_params* pr,
+                    const rb_outputs* out, void* stream) {
+    if (!sh || !bd || !caps || !pr || !out) return fail(RB_ERR_ARG, "rb_step_noalloc: null argument");
+    size_t need = 0;
+    int rc = rb_workspace_bytes(bd, caps, &need);
+    if (rc != RB_OK) return rc;
+    if (need > (size_t)RB_NOALLOC_SCRATCH_BYTES)
+        return fail(RB_ERR_WORKSPACE, "rb_step_noalloc: this batch needs " + std::to_string(need) +
+                                          " bytes of scratch, more than the " +
+                                          std::to_string((size_t)RB_NOALLOC_SCRATCH_BYTES) +
+                                          " bytes available; use rb_step with a workspace");
+    void* scratch = nullptr;
+    rc = noalloc_scratch(&scratch);
+    if (rc != RB_OK) return rc;
+    // rb_step clears the counters and per-body tallies it needs at the start of every step, so the
+    // previous call's contents of the shared array do no harm
+    return rb_step(sh, bd, caps, pr, out, scratch, (size_t)RB_NOALLOC_SCRATCH_BYTES, stream);
 }
 
 int rb_profile_times(float* out, int32_t n) {
