@@ -50,6 +50,7 @@ extern "C" {
 
 /* termination rules */
 #define RB_TERMINATE_MERIT 0          /* the reference's iterate-change merit (problem.py:53) */
+/* complementarity residual: ||x - prox(x - D^-1 (A x + b))||_inf / max(1, ||x||_inf), D = diag(A), A = J W J^T */
 #define RB_TERMINATE_RESIDUAL 1       /* complementarity residual <= residual_tolerance; the reference's merit
                                          rule still rejects iterates and adapts r */
 #define RB_TERMINATE_RESIDUAL_FIXED_R 2 /* complementarity residual <= residual_tolerance; every sweep is
@@ -65,6 +66,7 @@ typedef struct rb_shapes {
     const double* grid;         /* SDF node values, index i + I*(j + J*k) (grid3.py:71) */
     const int64_t* g_off;       /* n_shapes+1 value offsets */
     const double* grid_meta;    /* 12 doubles per shape: min[3], max[3], spacing[3], I, J, K (grid3.py:16) */
+    int32_t max_shape_triangles; /* triangles of the largest shape (at most 16384) */
 } rb_shapes;
 
 /* Bodies of one or more independent scenes; scene s owns bodies scene_start[s] .. scene_start[s+1]-1 in the
@@ -137,6 +139,8 @@ typedef struct rb_params {
     int32_t termination;          /* RB_TERMINATE_* */
     double residual_tolerance;    /* used by RB_TERMINATE_RESIDUAL */
     int32_t profiling;            /* nonzero: fill energies and residual histories */
+    int32_t residual_interval;    /* RB_TERMINATE_RESIDUAL_FIXED_R: test the residual every this many sweeps
+                                     (values below 1 mean every sweep); the other rules test every sweep */
     int32_t warm_start;           /* nonzero: start each contact's impulse from the previous step's solution for
                                      the same (body pair, side, triangle) found in rb_outputs.cache_*; the
                                      reference always starts from zero (contacts.py:53), so this is off for
@@ -155,6 +159,8 @@ typedef struct rb_scene_stats {
     int32_t n_candidates;         /* triangles searched (profiling only) */
     int32_t n_leaf_overlaps;      /* overlapping leaf (triangle) pairs: profile key number_of_overlaps (profiling only) */
     int32_t n_grid_lookups;       /* signed distance lookups of the contact search (profiling only) */
+    int32_t n_levels;             /* Gauss-Seidel wavefront levels of the scene's contact order */
+    int32_t reserved;
     double merit;                 /* last global merit */
     double residual;              /* complementarity residual of the returned solution (when computed) */
     double kinetic_energy;        /* state_storage.py:188 (profiling only) */

@@ -816,14 +816,20 @@ int rbo_colour_contacts(int K, int N, const int32_t* ids, const uint8_t* fixed, 
     return n_colours;
 }
 
-/* complementarity residual: max_k | x - prox(x - (A x + b)) |_inf / max(1, |x|_inf), unit r */
+/* complementarity residual: max | x - prox(x - D^-1 (A x + b)) |_inf / max(1, |x|_inf) with D = diag(A).
+   Every solver of the reference scales the prox argument by a positive multiple of D^-1 (r = 1/diag,
+   0.1/diag, and uniform factors of them), so all of them share this map's zeros as their fixed points. */
+static const double* g_residual_diag = NULL;
+static int g_residual_interval = 1;   /* tol_mode 2: residual tested every this many sweeps */
+void rbo_set_residual_interval(int n) { g_residual_interval = n > 1 ? n : 1; }
 static double complementarity_residual(const Problem* P, const double* b, const double* mu, const double* x,
                                        double* w) {
     wjt_dot(P, x, w);
     double res = 0.0, xm = 0.0;
     for (int k = 0; k < P->K; ++k) {
         double z[4];
-        for (int i = 0; i < 4; ++i) z[i] = x[4 * k + i] - (jrow_dot(P, k, i, w) + b[4 * k + i]);
+        for (int i = 0; i < 4; ++i)
+            z[i] = x[4 * k + i] - (1.0 / g_residual_diag[4 * k + i]) * (jrow_dot(P, k, i, w) + b[4 * k + i]);
         double pn = z[0] > 0.0 ? z[0] : 0.0;
         double f[3];
         prox_sphere(z[1], z[2], z[3], mu[k], pn, f);
@@ -863,6 +869,10 @@ static void solve_rigid(const Problem* P, const double* params, double* r, const
         double global_merit = 0.0;
         sweep_gs(P, r, b, mu, x, w, normal_only);
         double merit = merit_inf(x, sol, n);
+        if (tol_mode == 2 && g_residual_interval > 1 && (it + 1) % g_residual_interval != 0 && it + 1 != max_it) {
+            memcpy(sol, x, sizeof(double) * n);   /* fixed r between residual tests: accept */
+            continue;
+        }
         if (tol_mode >= 1) {   /* stop on the complementarity residual only; merit still adapts r (mode 1) */
             double res = complementarity_residual(P, b, mu, x, w);
             if (residuals) residuals[it] = res;
@@ -921,6 +931,10 @@ static void solve_interface(const Problem* P, const double* params, int scheme, 
         else sweep_coloured(P, r, b, mu, x, w, colour_ptr, colour_list, n_colours);
         double merit = merit_inf(x, sol, n);
         if (residuals) residuals[it] = merit;
+        if (tol_mode == 2 && g_residual_interval > 1 && (it + 1) % g_residual_interval != 0 && it + 1 != max_it) {
+            memcpy(sol, x, sizeof(double) * n);
+            continue;
+        }
         if (tol_mode == 0) {
             if (merit < params[P_ABS_TOL]) { *iterations = it; *exitcode = 1; break; }
             if (fabs(merit - last_merit) < params[P_REL_TOL] * last_merit) { *iterations = it; *exitcode = 2; break; }
@@ -1117,6 +1131,7 @@ int rbo_step(const OScene* sc, const double* params, double dt, double* r, doubl
         free(vv); free(jd); free(dtd);
         problem_diag(&P, diag);
         for (int i = 0; i < 4 * K; ++i) rr[i] = 1.0 / diag[i];
+        g_residual_diag = diag;
 
         int iters = 0, exitc = 0;
         if (out->scheme == S_RIGID_GS) {

@@ -28,7 +28,7 @@ _i32 = ctypes.c_int32
 
 class RbShapes(ctypes.Structure):
     _fields_ = [("n_shapes", _i32), ("V", _vp), ("v_off", _vp), ("T", _vp), ("t_off", _vp), ("grid", _vp),
-                ("g_off", _vp), ("grid_meta", _vp)]
+                ("g_off", _vp), ("grid_meta", _vp), ("max_shape_triangles", _i32)]
 
 
 class RbBodies(ctypes.Structure):
@@ -58,7 +58,7 @@ class RbParams(ctypes.Structure):
         ("too_small_merit_change", ctypes.c_double), ("contact_optimization_max_iterations", _i32),
         ("contact_optimization_tolerance", ctypes.c_double), ("envelope", ctypes.c_double), ("scheme", _i32),
         ("termination", _i32), ("residual_tolerance", ctypes.c_double), ("profiling", _i32),
-        ("warm_start", _i32),
+        ("residual_interval", _i32), ("warm_start", _i32),
     ]
 
 
@@ -66,7 +66,8 @@ class RbSceneStats(ctypes.Structure):
     _fields_ = [
         ("n_contacts", _i32), ("contact_start", _i32), ("iterations", _i32), ("exitcode", _i32),
         ("post_iterations", _i32), ("post_exitcode", _i32), ("n_pairs", _i32), ("n_candidates", _i32),
-        ("n_leaf_overlaps", _i32), ("n_grid_lookups", _i32), ("merit", ctypes.c_double), ("residual", ctypes.c_double), ("kinetic_energy", ctypes.c_double),
+        ("n_leaf_overlaps", _i32), ("n_grid_lookups", _i32),
+        ("n_levels", _i32), ("reserved", _i32), ("merit", ctypes.c_double), ("residual", ctypes.c_double), ("kinetic_energy", ctypes.c_double),
         ("potential_energy", ctypes.c_double), ("max_penetration", ctypes.c_double),
     ]
 

@@ -62,7 +62,7 @@ struct Workspace {
     int32_t* counters;   // 16
 };
 
-enum Counter { kNPairs = 0, kNItems = 1, kNRaw = 2, kNContacts = 3 };
+enum Counter { kNPairs = 0, kNItems = 1, kNRaw = 2, kNContacts = 3, kMidNext = 4 };
 
 inline size_t align_up(size_t v) { return (v + 255) & ~size_t(255); }
 

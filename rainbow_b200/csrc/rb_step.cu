@@ -331,22 +331,34 @@ __global__ void k_pairs(const StepArgs a) {
 // each inner volume is the exact union of its children; np.unique of each column (collision_detection.py:234)
 // makes both sets ascending.  Clusters of 32 triangles with exact union boxes prune the same way.
 // ---------------------------------------------------------------------------------------------------------
-struct MidShared {
-    int16_t listA[kMaxClustersPerShape];
-    int16_t listB[kMaxClustersPerShape];
-    uint32_t maskA[kMaxClustersPerShape];
-    uint32_t maskB[kMaxClustersPerShape];
-};
+// per-warp shared arrays of k_mid, sized at launch by the largest shape: lists of the clusters of A (of B)
+// whose box overlaps B's (A's) body box, and the hit masks of their 32 triangles
+__device__ __forceinline__ void mid_arrays(int max_clusters, int warp, int16_t*& listA, int16_t*& listB,
+                                           uint32_t*& maskA, uint32_t*& maskB) {
+    extern __shared__ uint32_t mid_smem[];
+    const int words = 3 * max_clusters;   // 2 lists of int16 + 2 masks of uint32 = 3 words per cluster
+    uint32_t* base = mid_smem + (size_t)warp * words;
+    maskA = base;
+    maskB = base + max_clusters;
+    listA = reinterpret_cast<int16_t*>(base + 2 * max_clusters);
+    listB = listA + max_clusters;
+}
 
-// single pass: each pair reserves room for its candidates with one atomic and writes them in ascending
-// (side, triangle) order; pair_items[p] = first candidate of the pair, pair_itemsA[p] = number of candidates
-__global__ void __launch_bounds__(kBlock) k_mid(const StepArgs a) {
-    __shared__ MidShared sm[kWarpsPerBlock];
-    MidShared& S = sm[threadIdx.x >> 5];
+// single pass: warps take pairs from a shared counter, find the pair's candidate triangles, reserve room
+// with one atomic and write them in ascending (side, triangle) order; pair_items[p] = first candidate of
+// the pair, pair_itemsA[p] = number of candidates
+__global__ void __launch_bounds__(kBlock) k_mid(const StepArgs a, int max_clusters) {
+    int16_t *listA, *listB;
+    uint32_t *maskA, *maskB;
+    mid_arrays(max_clusters, threadIdx.x >> 5, listA, listB, maskA, maskB);
     const int lane = threadIdx.x & 31;
     if (a.ws.counters[kAbort]) return;
     const int n_pairs = a.ws.counters[kNPairs];
-    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < n_pairs; p += (gridDim.x * blockDim.x) >> 5) {
+    for (;;) {
+        int p = 0;
+        if (lane == 0) p = atomicAdd(a.ws.counters + kMidNext, 1);
+        p = __shfl_sync(0xffffffffu, p, 0);
+        if (p >= n_pairs) break;
         const int A = a.ws.pairs[2 * p], B = a.ws.pairs[2 * p + 1];
         const int cA0 = a.bd.body_c0[A], ncA = a.bd.body_c0[A + 1] - cA0;
         const int cB0 = a.bd.body_c0[B], ncB = a.bd.body_c0[B + 1] - cB0;
@@ -354,9 +366,12 @@ __global__ void __launch_bounds__(kBlock) k_mid(const StepArgs a) {
         const int tB0 = a.bd.body_t0[B], ntB = a.bd.body_t0[B + 1] - tB0;
         const double* rootA = a.ws.root + 6 * A;
         const double* rootB = a.ws.root + 6 * B;
-        if (ncA > kMaxClustersPerShape || ncB > kMaxClustersPerShape) {
-            if (lane == 0) { atomicOr(a.out.status, RB_STATUS_MESH_TOO_LARGE); atomicOr(a.ws.counters + kAbort, RB_STATUS_MESH_TOO_LARGE); }
-            if (lane == 0) { a.ws.pair_items[p] = 0; a.ws.pair_itemsA[p] = 0; a.ws.pair_ovl[p] = 0; }
+        if (ncA > max_clusters || ncB > max_clusters) {
+            if (lane == 0) {
+                atomicOr(a.out.status, RB_STATUS_MESH_TOO_LARGE);
+                atomicOr(a.ws.counters + kAbort, RB_STATUS_MESH_TOO_LARGE);
+                a.ws.pair_items[p] = 0; a.ws.pair_itemsA[p] = 0; a.ws.pair_ovl[p] = 0;
+            }
             continue;
         }
         int nA = 0, nB = 0;
@@ -364,48 +379,61 @@ __global__ void __launch_bounds__(kBlock) k_mid(const StepArgs a) {
             const int c = c0 + lane;
             const bool ok = c < ncA && overlap(a.ws.clu + 6 * (size_t)(cA0 + c), rootB);
             const unsigned bal = __ballot_sync(0xffffffffu, ok);
-            if (ok) S.listA[nA + __popc(bal & lanemask_lt())] = (int16_t)c;
+            if (ok) listA[nA + __popc(bal & lanemask_lt())] = (int16_t)c;
             nA += __popc(bal);
         }
         for (int c0 = 0; c0 < ncB; c0 += 32) {
             const int c = c0 + lane;
             const bool ok = c < ncB && overlap(a.ws.clu + 6 * (size_t)(cB0 + c), rootA);
             const unsigned bal = __ballot_sync(0xffffffffu, ok);
-            if (ok) S.listB[nB + __popc(bal & lanemask_lt())] = (int16_t)c;
+            if (ok) listB[nB + __popc(bal & lanemask_lt())] = (int16_t)c;
             nB += __popc(bal);
         }
-        for (int k = lane; k < nA; k += 32) S.maskA[k] = 0u;
-        for (int k = lane; k < nB; k += 32) S.maskB[k] = 0u;
+        for (int k = lane; k < nA; k += 32) maskA[k] = 0u;
+        for (int k = lane; k < nB; k += 32) maskB[k] = 0u;
         __syncwarp();
         int n_ovl = 0;
         for (int ia = 0; ia < nA; ++ia) {
-            const int ca = S.listA[ia];
-            const double* CA = a.ws.clu + 6 * (size_t)(cA0 + ca);
+            const int ca = listA[ia];
+            double CA[6];
+            for (int k = 0; k < 6; ++k) CA[k] = a.ws.clu[6 * (size_t)(cA0 + ca) + k];
             const int ta = 32 * ca + lane;
             const bool validA = ta < ntA;
             double LA[6];
-            if (validA) for (int k = 0; k < 6; ++k) LA[k] = a.ws.leaf[6 * (size_t)(tA0 + ta) + k];
+            for (int k = 0; k < 6; ++k) LA[k] = validA ? a.ws.leaf[6 * (size_t)(tA0 + ta) + k] : 0.0;
             bool hitA = false;
             for (int ib = 0; ib < nB; ++ib) {
-                const int cb = S.listB[ib];
-                if (!overlap(CA, a.ws.clu + 6 * (size_t)(cB0 + cb))) continue;
-                const int nbt = min(32, ntB - 32 * cb);
+                const int cb = listB[ib];
+                const double* CB = a.ws.clu + 6 * (size_t)(cB0 + cb);
+                if (!overlap(CA, CB)) continue;
+                // a leaf pair can only overlap if each leaf overlaps the other leaf's cluster box
+                const unsigned amask = __ballot_sync(0xffffffffu, validA && overlap(LA, CB));
+                if (!amask) continue;
+                const int tb = 32 * cb + lane;
+                const bool validB = tb < ntB;
+                double LB[6];
+                for (int k = 0; k < 6; ++k) LB[k] = validB ? a.ws.leaf[6 * (size_t)(tB0 + tb) + k] : 0.0;
+                unsigned bmask = __ballot_sync(0xffffffffu, validB && overlap(LB, CA));
                 unsigned hitB = 0u;
-                for (int jb = 0; jb < nbt; ++jb) {
-                    const double* LB = a.ws.leaf + 6 * (size_t)(tB0 + 32 * cb + jb);
-                    if (validA && overlap(LA, LB)) { hitA = true; hitB |= 1u << jb; }
+                const bool mine = (amask >> lane) & 1u;
+                while (bmask) {
+                    const int jb = __ffs(bmask) - 1;
+                    bmask &= bmask - 1;
+                    double Lj[6];
+                    for (int k = 0; k < 6; ++k) Lj[k] = __shfl_sync(0xffffffffu, LB[k], jb);
+                    if (mine && overlap(LA, Lj)) { hitA = true; hitB |= 1u << jb; }
                 }
                 n_ovl += __popc(hitB);
                 hitB = __reduce_or_sync(0xffffffffu, hitB);
-                if (lane == 0) S.maskB[ib] |= hitB;
+                if (lane == 0) maskB[ib] |= hitB;
             }
             const unsigned bal = __ballot_sync(0xffffffffu, hitA);
-            if (lane == 0) S.maskA[ia] = bal;
+            if (lane == 0) maskA[ia] = bal;
         }
         __syncwarp();
         int cntA = 0, cntB = 0;
-        for (int k = lane; k < nA; k += 32) cntA += __popc(S.maskA[k]);
-        for (int k = lane; k < nB; k += 32) cntB += __popc(S.maskB[k]);
+        for (int k = lane; k < nA; k += 32) cntA += __popc(maskA[k]);
+        for (int k = lane; k < nB; k += 32) cntB += __popc(maskB[k]);
         cntA = __reduce_add_sync(0xffffffffu, cntA);
         cntB = __reduce_add_sync(0xffffffffu, cntB);
         n_ovl = __reduce_add_sync(0xffffffffu, n_ovl);
@@ -416,8 +444,8 @@ __global__ void __launch_bounds__(kBlock) k_mid(const StepArgs a) {
         if (pos + cntA + cntB <= a.caps.item_capacity) {   // otherwise k_check aborts the step
             for (int side = 0; side < 2; ++side) {
                 const int n = side ? nB : nA;
-                const int16_t* list = side ? S.listB : S.listA;
-                const uint32_t* mask = side ? S.maskB : S.maskA;
+                const int16_t* list = side ? listB : listA;
+                const uint32_t* mask = side ? maskB : maskA;
                 for (int k = 0; k < n; ++k) {
                     const uint32_t bits = mask[k];
                     if (bits & (1u << lane)) {
@@ -961,15 +989,28 @@ __device__ __forceinline__ void gs_sweep_levels(const StepArgs& a, const G& g, c
     const int* ptr = a.ws.lev_ptr + R.c0 + s;
     for (int l = 1; l <= L; ++l) {
         const int start = ptr[l - 1], end = ptr[l];
+        if (l < L) {   // pull the next level's Jacobian blocks into L1 while this level runs
+            const int i = end + g.rank();
+            if (i < ptr[l + 1]) {
+                const int kn = a.ws.lev_order[R.c0 + i];
+                const char* pj = reinterpret_cast<const char*>(a.ws.J + 48 * (size_t)kn);
+                const char* pw = reinterpret_cast<const char*>(a.ws.WJT + 48 * (size_t)kn);
+                for (int off = 0; off < 384; off += 128) {
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(pj + off));
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(pw + off));
+                }
+            }
+        }
         for (int i = start + g.rank(); i < end; i += g.size())
             gs_contact(a, a.ws.lev_order[R.c0 + i], b, r, x, w, normal_only);
         g.sync();
     }
 }
 
-// complementarity residual ||x - prox(x - (A x + b))||_inf / max(1, ||x||_inf) with unit r (the tolerance
-// the solver modes are compared at); A x = J W J^T x through w = WJT x (the accumulators are rebuilt from x
-// at the start of every sweep, so they are free to hold this product here).
+// complementarity residual ||x - prox(x - D^-1 (A x + b))||_inf / max(1, ||x||_inf), D = diag(A): the
+// tolerance the solver modes are compared at.  Every scheme scales the prox argument by a positive multiple of
+// D^-1, so they all share this map's zeros as fixed points.  A x = J W J^T x through w = WJT x (the
+// accumulators are rebuilt from x at the start of every sweep, so they are free to hold this product here).
 template <class G>
 __device__ double scene_residual(const StepArgs& a, const G& g, const SceneRange& R, const double* x, WView w) {
     scene_wjt(a, g, R, x, w);
@@ -979,7 +1020,8 @@ __device__ double scene_residual(const StepArgs& a, const G& g, const SceneRange
         const double* J = a.ws.J + 48 * (size_t)k;
         double z[4];
         for (int row = 0; row < 4; ++row)
-            z[row] = x[4 * k + row] - (jrow_dot(J + 12 * row, w.at(lo), w.at(hi)) + a.ws.b[4 * k + row]);
+            z[row] = x[4 * k + row] -
+                     (1.0 / a.ws.diag[4 * k + row]) * (jrow_dot(J + 12 * row, w.at(lo), w.at(hi)) + a.ws.b[4 * k + row]);
         const double pn = z[0] > 0.0 ? z[0] : 0.0;
         double f[3];
         prox_sphere(z[1], z[2], z[3], a.ws.mu[k], pn, f);
@@ -1015,6 +1057,7 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
         if (!post) {
             st->n_contacts = K; st->contact_start = R.c0; st->iterations = -1; st->exitcode = -1;
             st->merit = 0.0; st->residual = 0.0; st->post_iterations = -1; st->post_exitcode = -1;
+            st->n_levels = 0;
         } else {
             st->post_iterations = -1; st->post_exitcode = -1;
         }
@@ -1029,8 +1072,10 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
     const bool on_chip = w_smem != nullptr && nb <= smem_bodies;
     const WView w = {on_chip ? w_smem : a.ws.w + 6 * R.b0, R.b0};
     const int L = jacobi ? 0 : scene_levels(a, g, R, s);
+    if (!post && g.rank() == 0) st->n_levels = L;
     const bool by_residual = !post && a.pr.termination != RB_TERMINATE_MERIT;
     const bool fixed_r = !post && a.pr.termination == RB_TERMINATE_RESIDUAL_FIXED_R;
+    const int interval = a.pr.residual_interval > 1 ? a.pr.residual_interval : 1;
     double last = INFINITY, global_last = INFINITY, shown = 0.0;
     int iterations = max_it, exitcode = 0;
     bool w_is_wjt_x = false;   // w already holds WJT x for the current x (left by the residual pass)
@@ -1053,11 +1098,15 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
         } else {
             gs_sweep_levels(a, g, R, s, L, b, r, x, w, post != 0);
         }
-        // merit = ||x - sol||_inf (problem.py:53)
-        double m = 0.0;
-        for (int i = 4 * R.c0 + g.rank(); i < 4 * R.c1; i += g.size()) m = nanmax(m, fabs(x[i] - sol[i]));
-        const double merit = g.max(m);
-        const double res = by_residual ? scene_residual(a, g, R, x, w) : 0.0;
+        // merit = ||x - sol||_inf (problem.py:53); the fixed-r rule never looks at it
+        double merit = 0.0;
+        if (!fixed_r) {
+            double m = 0.0;
+            for (int i = 4 * R.c0 + g.rank(); i < 4 * R.c1; i += g.size()) m = nanmax(m, fabs(x[i] - sol[i]));
+            merit = g.max(m);
+        }
+        const bool check = by_residual && (!fixed_r || (it + 1) % interval == 0 || it + 1 == max_it);
+        const double res = check ? scene_residual(a, g, R, x, w) : 0.0;
         int decision = 0;   // 0 accept, 1 reject, 2 keep sol, 3 take x
         bool stop = false, inc = false;
         if (rigid) {        // gauss_seidel_solver.py:439-482
@@ -1081,7 +1130,9 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
             } else decision = 2;
             shown = merit;
         }
-        if (by_residual) {  // stop only on the complementarity residual
+        if (by_residual && !check) {   // fixed r between residual tests: accept the sweep
+            stop = false; exitcode = 0; decision = 0; inc = false;
+        } else if (by_residual) {      // stop only on the complementarity residual
             shown = res;
             if (res <= a.pr.residual_tolerance) { stop = true; exitcode = 3; decision = 3; }
             else if (fixed_r) { stop = false; exitcode = 0; decision = 0; inc = false; }
@@ -1109,7 +1160,7 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
             for (int i = 4 * R.c0 + g.rank(); i < 4 * R.c1; i += g.size()) sol[i] = x[i];
         }
         // the residual pass computed w = WJT x; unless x was rolled back that is the next sweep's start
-        w_is_wjt_x = by_residual && decision != 1;
+        w_is_wjt_x = check && decision != 1;
         g.sync();
         if (stop) { iterations = it; break; }
     }
@@ -1371,6 +1422,8 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     if (pr->max_iterations < 0 || pr->max_iterations > caps->max_iterations)
         return fail(RB_ERR_ARG, "rb_step: max_iterations exceeds rb_caps.max_iterations");
     if (!(pr->dt > 0.0)) return fail(RB_ERR_ARG, "rb_step: dt must be positive");
+    if (sh->max_shape_triangles <= 0 || sh->max_shape_triangles > 32 * kMaxClustersPerShape)
+        return fail(RB_ERR_ARG, "rb_step: max_shape_triangles must be in 1..16384");
     size_t need = 0;
     int rc = rb_workspace_bytes(bd, caps, &need);
     if (rc != RB_OK) return rc;
@@ -1403,7 +1456,11 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     k_check<<<1, 1, 0, st>>>(a.ws.counters, kNPairs, caps->pair_capacity, RB_STATUS_PAIR_OVERFLOW, out->status);
     k_pairs<true><<<blocks_for(32 * (int64_t)N, kBlock), kBlock, 0, st>>>(a);
     // mid phase
-    k_mid<<<G, kBlock, 0, st>>>(a);
+    {
+        const int max_clusters = (sh->max_shape_triangles + 31) / 32;
+        const size_t mid_smem = (size_t)kWarpsPerBlock * 3 * sizeof(uint32_t) * (max_clusters > 0 ? max_clusters : 1);
+        k_mid<<<148 * 16, kBlock, mid_smem, st>>>(a, max_clusters > 0 ? max_clusters : 1);
+    }
     k_check<<<1, 1, 0, st>>>(a.ws.counters, kNItems, caps->item_capacity, RB_STATUS_ITEM_OVERFLOW, out->status);
     prof_mark(prof, 2, st);
     // narrow phase

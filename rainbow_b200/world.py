@@ -34,7 +34,7 @@ def params_from_vector(vec):
 
 
 def make_rb_params(p, dt=None, scheme="rigid_gauss_seidel", termination="merit", residual_tolerance=1e-6,
-                   profiling=False, warm_start=False):
+                   profiling=False, warm_start=False, residual_interval=1):
     """rb_params from a Parameters-like mapping (types.py:356 field names)."""
     g = p.__getitem__ if isinstance(p, dict) else (lambda k: getattr(p, k))
     rp = N.RbParams()
@@ -55,6 +55,7 @@ def make_rb_params(p, dt=None, scheme="rigid_gauss_seidel", termination="merit",
     rp.residual_tolerance = float(residual_tolerance)
     rp.profiling = int(bool(profiling))
     rp.warm_start = int(bool(warm_start))
+    rp.residual_interval = int(residual_interval)
     return rp
 
 
@@ -246,6 +247,7 @@ class DeviceWorld:
         for f in ("V", "v_off", "T", "t_off", "grid", "g_off"):
             setattr(sh, f, T["shape_" + f].data_ptr())
         sh.grid_meta = T["shape_grid_meta"].data_ptr()
+        sh.max_shape_triangles = int(np.diff(P["shape_t_off"]).max())
         self.rb_shapes = sh
         bd = N.RbBodies()
         bd.n_bodies, bd.n_scenes = self.n_bodies, self.n_scenes

@@ -187,3 +187,22 @@ def test_warm_start_reuses_previous_impulses():
         assert all(tuple(keys[i]) < tuple(keys[i + 1]) for i in range(len(keys) - 1))
         sweeps[warm] = total
     assert sweeps[True] < sweeps[False]
+
+
+def test_residual_interval_matches_oracle(oracle_lib):
+    """Fixed-r solves that test the residual every fourth sweep stay bit-identical to the oracle."""
+    from rainbow_b200 import world as W
+    d = load_fixture("c1_boxes64")
+    p = W.params_from_vector(d["params"])
+    p["max_iterations"] = 200
+    world = _world(d, max_iterations=200)
+    sc = oracle_lib.OracleScene(d)
+    sc.set_param("max_iterations", 200)
+    for _ in range(3):
+        world.step(W.make_rb_params(p, termination="residual_fixed_r", residual_tolerance=1e-6, residual_interval=4))
+        o = sc.step(tol_mode=2, tol=1e-6, residual_interval=4)
+        st = world.stats()[0]
+        assert (st.iterations, st.exitcode) == (o["iterations"], o["exitcode"])
+        assert st.exitcode == 3 and (st.iterations + 1) % 4 == 0
+        np.testing.assert_array_equal(world.contacts()["sol"], o["sol"])
+        np.testing.assert_array_equal(world.state()[0].ravel(), o["x"])
