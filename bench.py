@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--pre-roll", type=int, default=60)
     ap.add_argument("--plain-scenes", type=int, default=32, help="scenes of the one-scene-per-launch baseline")
     ap.add_argument("--no-warm-start", action="store_true", help="start every solve from zero impulses")
+    ap.add_argument("--precision", default="fp32_refine", choices=["fp64", "fp32_refine", "fp32"],
+                    help="precision of the batched solve (the plain baseline is always FP64)")
+    ap.add_argument("--residual-interval", type=int, default=4)
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     ap.add_argument("--cpu-scenes", type=int, default=16, help="scenes in the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
@@ -221,24 +224,54 @@ def run_ours(args):
     arrays, params, cfg, engine = build_workload(args.workload, dev, args.scenes)
     max_it = int(params.max_iterations)
     world = W.DeviceWorld(arrays, device=dev, max_iterations=max_it)
-    kw = dict(scheme=args.scheme, termination=args.termination, residual_tolerance=args.tolerance)
+    kw = dict(scheme=args.scheme, termination=args.termination, residual_tolerance=args.tolerance,
+              residual_interval=args.residual_interval if args.termination == "residual_fixed_r" else 1)
     warm = not args.no_warm_start
-    rp = W.make_rb_params(params, warm_start=warm, **kw)
-    rp_prof = W.make_rb_params(params, profiling=True, warm_start=warm, **kw)
-    # the plain baseline runs the same solver with the same settings one scene per launch sequence: its results
-    # are bit-identical to the batched ones (tests/test_gpu_parity.py), so both stop at the same residual
-    rp_plain = rp
+    prec = args.precision if args.termination == "residual_fixed_r" else "fp64"
+    rp = W.make_rb_params(params, warm_start=warm, precision=prec, **kw)
+    rp_prof = W.make_rb_params(params, profiling=True, warm_start=warm, precision=prec, **kw)
+    # the plain baseline: the same FP64 solver and settings, one scene per launch sequence (FP64 results are
+    # bit-identical alone and batched, tests/test_gpu_parity.py), stopping at the same residual tolerance
+    rp_plain = W.make_rb_params(params, warm_start=warm, precision="fp64", **kw)
+    rp64 = rp_plain
     stream = torch.cuda.current_stream()
     for _ in range(args.pre_roll):
         world.step(rp)
     x0, u0 = world.state()                 # state the timed region (and every baseline) starts from
+    cache = (world.t_cache_key.clone(), world.t_cache_sol.clone(), world.t_cache_count.clone())
+
+    def restore():
+        world.set_state(x0, u0)
+        world.t_cache_key.copy_(cache[0]); world.t_cache_sol.copy_(cache[1]); world.t_cache_count.copy_(cache[2])
+
     world.step(rp_prof)                    # phase split and byte accounting (outside the timed region)
     phases = world.profile_times()
     stats = world.stats()
-    world.set_state(x0, u0)
+    x_m, u_m = world.state()
+    # error of this precision mode against the FP64 step from the same state (the FP64 GPU step is
+    # bit-identical to the oracle)
+    restore()
+    world.step(rp64)
+    x_64, u_64 = world.state()
+    stats64 = world.stats()
+    # compare velocities on the scenes where both solves met the tolerance (unconverged iterates of different
+    # precisions are different points of the same unfinished iteration, not a precision error)
+    both = [i for i in range(world.n_scenes) if stats[i].n_contacts > 0 and stats[i].exitcode == 3
+            and stats64[i].exitcode == 3]
+    um, u6 = u_m.reshape(-1, 6), u_64.reshape(-1, 6)
+    rel = []
+    for i in both:
+        b0, b1 = world.scene_start[i], world.scene_start[i + 1]
+        rel.append(np.abs(um[b0:b1] - u6[b0:b1]).max() / max(1e-30, np.abs(u6[b0:b1]).max()))
+    err = {"scenes_compared": len(both),
+           "rel_velocity_error_p50_max": [float(np.median(rel)), float(np.max(rel))] if rel else None,
+           "fp64_converged_scenes": int(sum(1 for s_ in stats64 if s_.n_contacts > 0 and s_.exitcode == 3)),
+           "mode_converged_scenes": int(sum(1 for s_ in stats if s_.n_contacts > 0 and s_.exitcode == 3)),
+           "fp32_sweeps_mean": float(np.mean([s_.fp32_sweeps for s_ in stats if s_.n_contacts > 0] or [0]))}
+    restore()
     for _ in range(max(3, args.warmup)):
         world.step(rp)
-    world.set_state(x0, u0)
+    restore()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     if world_size > 1:
         dist.barrier()
@@ -260,6 +293,7 @@ def run_ours(args):
     residuals = np.array([s.residual for s in after if s.n_contacts > 0])
     iters = np.array([s.iterations + 1 if s.exitcode == 3 else max_it for s in after if s.n_contacts > 0])
     ncont = np.array([s.n_contacts for s in after])
+    levels = np.array([s.n_levels for s in after if s.n_contacts > 0])
     unconverged = int(sum(1 for s in after if s.n_contacts > 0 and s.exitcode != 3)) \
         if args.termination != "merit" else None
 
@@ -353,23 +387,26 @@ def run_ours(args):
         cpu = dict(value=cv, unit="scene-steps/s", **info)
 
     cfg.update({"scheme": args.scheme, "termination": args.termination, "tolerance": args.tolerance,
-                "precision": "fp64", "warm_start": warm, "pre_roll_steps": args.pre_roll, "contacts_per_step": int(K),
+                "precision": prec, "warm_start": warm, "residual_interval": kw["residual_interval"], "pre_roll_steps": args.pre_roll, "contacts_per_step": int(K),
                 "sweeps_per_step_contacts": int(sweeps), "l2": "256 MB buffer written between timed steps",
                 "parallelism": "replicas" if world_size > 1 else "single"})
     line = {
         "metric": "scene-steps/s", "value": value, "unit": "scene-steps/s", "n_gpus": world_size,
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,
         "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if prec != "fp64" else "f64", "data": "synthetic",
         "config": cfg,
         "plain": plain,
+        "error_vs_fp64": err,
         "speedup_vs_plain": (value / world_size) / plain["value"] if plain else None,
         "residual": {"max": float(residuals.max()) if len(residuals) else 0.0,
                      "median": float(np.median(residuals)) if len(residuals) else 0.0,
                      "unconverged_scenes": unconverged,
                      "sweeps_p50_p90_max": [float(np.percentile(iters, 50)), float(np.percentile(iters, 90)),
                                             int(iters.max())] if len(iters) else None,
-                     "contacts_per_scene_p50_max": [float(np.percentile(ncont, 50)), int(ncont.max())]},
+                     "contacts_per_scene_p50_max": [float(np.percentile(ncont, 50)), int(ncont.max())],
+                     "levels_per_scene_p50_max": [float(np.percentile(levels, 50)), int(levels.max())]
+                     if len(levels) else None},
         "roofline": {"bound": "hbm", "kernel_phase": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None, "algorithmic_bytes": int(nbytes),
                      "bytes_model": model, "phase_ms": dt_s * 1000.0,

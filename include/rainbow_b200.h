@@ -56,6 +56,12 @@ extern "C" {
 #define RB_TERMINATE_RESIDUAL_FIXED_R 2 /* complementarity residual <= residual_tolerance; every sweep is
                                          accepted and r stays at its initial value */
 
+/* solver precision */
+#define RB_PRECISION_FP64 0           /* every sweep in FP64 (bit-exact with the reference's NumPy step) */
+#define RB_PRECISION_FP32_REFINE 1    /* sweeps in FP32 on chip until the residual tolerance, then FP64 sweeps until
+                                         the FP64 residual meets it */
+#define RB_PRECISION_FP32 2           /* FP32 sweeps only; the FP64 residual of the result is reported */
+
 /* Shapes (rainbow/simulators/prox_rigid_bodies/types.py:82 Shape): body-frame mesh and signed distance grid. */
 typedef struct rb_shapes {
     int32_t n_shapes;
@@ -139,8 +145,13 @@ typedef struct rb_params {
     int32_t termination;          /* RB_TERMINATE_* */
     double residual_tolerance;    /* used by RB_TERMINATE_RESIDUAL */
     int32_t profiling;            /* nonzero: fill energies and residual histories */
+    double relaxation;            /* RB_TERMINATE_RESIDUAL_FIXED_R: r = relaxation / diag (over-relaxation of the
+                                     projected Gauss-Seidel update; values <= 0 mean 1) */
     int32_t residual_interval;    /* RB_TERMINATE_RESIDUAL_FIXED_R: test the residual every this many sweeps
                                      (values below 1 mean every sweep); the other rules test every sweep */
+    int32_t precision;            /* RB_PRECISION_*; the FP32 modes need RB_TERMINATE_RESIDUAL_FIXED_R and a
+                                     Gauss-Seidel scheme */
+    int32_t refine_iterations;    /* RB_PRECISION_FP32_REFINE: cap of the FP64 sweeps after the FP32 phase */
     int32_t warm_start;           /* nonzero: start each contact's impulse from the previous step's solution for
                                      the same (body pair, side, triangle) found in rb_outputs.cache_*; the
                                      reference always starts from zero (contacts.py:53), so this is off for
@@ -160,7 +171,7 @@ typedef struct rb_scene_stats {
     int32_t n_leaf_overlaps;      /* overlapping leaf (triangle) pairs: profile key number_of_overlaps (profiling only) */
     int32_t n_grid_lookups;       /* signed distance lookups of the contact search (profiling only) */
     int32_t n_levels;             /* Gauss-Seidel wavefront levels of the scene's contact order */
-    int32_t reserved;
+    int32_t fp32_sweeps;          /* sweeps done in FP32 (FP32 precision modes; included in iterations) */
     double merit;                 /* last global merit */
     double residual;              /* complementarity residual of the returned solution (when computed) */
     double kinetic_energy;        /* state_storage.py:188 (profiling only) */

@@ -821,6 +821,8 @@ int rbo_colour_contacts(int K, int N, const int32_t* ids, const uint8_t* fixed, 
    0.1/diag, and uniform factors of them), so all of them share this map's zeros as their fixed points. */
 static const double* g_residual_diag = NULL;
 static int g_residual_interval = 1;   /* tol_mode 2: residual tested every this many sweeps */
+static double g_relaxation = 1.0;     /* tol_mode 2: r = relaxation / diag */
+void rbo_set_relaxation(double w) { g_relaxation = w; }
 void rbo_set_residual_interval(int n) { g_residual_interval = n > 1 ? n : 1; }
 static double complementarity_residual(const Problem* P, const double* b, const double* mu, const double* x,
                                        double* w) {
@@ -921,7 +923,7 @@ static void solve_interface(const Problem* P, const double* params, int scheme, 
     double* w = (double*)malloc(sizeof(double) * 6 * (P->N ? P->N : 1));
     double* xold = (double*)malloc(sizeof(double) * (n ? n : 1));
     double* r = (double*)malloc(sizeof(double) * (n ? n : 1));
-    for (int i = 0; i < n; ++i) r[i] = 0.1 / diag[i];
+    for (int i = 0; i < n; ++i) r[i] = (tol_mode == 2 && g_relaxation > 0.0 ? 0.1 * g_relaxation : 0.1) / diag[i];
     double last_merit = INFINITY;
     *iterations = max_it; *exitcode = 0;
     for (int it = 0; it < max_it; ++it) {
@@ -1130,7 +1132,11 @@ int rbo_step(const OScene* sc, const double* params, double dt, double* r, doubl
         }
         free(vv); free(jd); free(dtd);
         problem_diag(&P, diag);
-        for (int i = 0; i < 4 * K; ++i) rr[i] = 1.0 / diag[i];
+        {
+            /* fixed-r rule: r = relaxation / diag (1/diag without relaxation) */
+            const double om = (tol_mode == 2 && g_relaxation > 0.0) ? g_relaxation : 1.0;
+            for (int i = 0; i < 4 * K; ++i) rr[i] = om / diag[i];
+        }
         g_residual_diag = diag;
 
         int iters = 0, exitc = 0;

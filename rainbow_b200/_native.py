@@ -21,6 +21,7 @@ STATUS_MESH_TOO_LARGE = 32
 
 SCHEME_RIGID_GS, SCHEME_GS, SCHEME_JACOBI, SCHEME_JACOBI_HYBRID, SCHEME_COLOURED_GS = 0, 1, 2, 3, 4
 TERMINATE_MERIT, TERMINATE_RESIDUAL, TERMINATE_RESIDUAL_FIXED_R = 0, 1, 2
+PRECISION_FP64, PRECISION_FP32_REFINE, PRECISION_FP32 = 0, 1, 2
 
 _vp = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -58,7 +59,8 @@ class RbParams(ctypes.Structure):
         ("too_small_merit_change", ctypes.c_double), ("contact_optimization_max_iterations", _i32),
         ("contact_optimization_tolerance", ctypes.c_double), ("envelope", ctypes.c_double), ("scheme", _i32),
         ("termination", _i32), ("residual_tolerance", ctypes.c_double), ("profiling", _i32),
-        ("residual_interval", _i32), ("warm_start", _i32),
+        ("relaxation", ctypes.c_double), ("residual_interval", _i32), ("precision", _i32),
+        ("refine_iterations", _i32), ("warm_start", _i32),
     ]
 
 
@@ -67,7 +69,7 @@ class RbSceneStats(ctypes.Structure):
         ("n_contacts", _i32), ("contact_start", _i32), ("iterations", _i32), ("exitcode", _i32),
         ("post_iterations", _i32), ("post_exitcode", _i32), ("n_pairs", _i32), ("n_candidates", _i32),
         ("n_leaf_overlaps", _i32), ("n_grid_lookups", _i32),
-        ("n_levels", _i32), ("reserved", _i32), ("merit", ctypes.c_double), ("residual", ctypes.c_double), ("kinetic_energy", ctypes.c_double),
+        ("n_levels", _i32), ("fp32_sweeps", _i32), ("merit", ctypes.c_double), ("residual", ctypes.c_double), ("kinetic_energy", ctypes.c_double),
         ("potential_energy", ctypes.c_double), ("max_penetration", ctypes.c_double),
     ]
 

@@ -618,7 +618,8 @@ __global__ void k_contacts(const StepArgs a) {
     if (a.ws.counters[kAbort]) return;
     const int K = a.ws.counters[kNContacts];
     const double dt = a.pr.dt;
-    const double r_scale = a.pr.scheme == RB_SCHEME_RIGID_GS ? 1.0 : 0.1;   // solver_interface.py:48
+    double r_scale = a.pr.scheme == RB_SCHEME_RIGID_GS ? 1.0 : 0.1;   // solver_interface.py:48
+    if (a.pr.termination == RB_TERMINATE_RESIDUAL_FIXED_R && a.pr.relaxation > 0.0) r_scale *= a.pr.relaxation;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
         const int A = a.out.contact_ids[2 * k], B = a.out.contact_ids[2 * k + 1];
         const d3 p = ld3(a.out.contact_p + 3 * k);
@@ -1057,7 +1058,7 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
         if (!post) {
             st->n_contacts = K; st->contact_start = R.c0; st->iterations = -1; st->exitcode = -1;
             st->merit = 0.0; st->residual = 0.0; st->post_iterations = -1; st->post_exitcode = -1;
-            st->n_levels = 0;
+            st->n_levels = 0; st->fp32_sweeps = 0;
         } else {
             st->post_iterations = -1; st->post_exitcode = -1;
         }
@@ -1079,7 +1080,30 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
     double last = INFINITY, global_last = INFINITY, shown = 0.0;
     int iterations = max_it, exitcode = 0;
     bool w_is_wjt_x = false;   // w already holds WJT x for the current x (left by the residual pass)
-    for (int it = 0; it < max_it; ++it) {
+    // FP32 modes: the scene's FP32 phase left its iterate in x; test it in FP64, then refine in FP64
+    const int sweeps32 = (!post && a.pr.precision != RB_PRECISION_FP64) ? a.ws.sweeps32[s] : -1;
+    int loop_max = max_it;
+    if (sweeps32 >= 0) {
+        const double res0 = scene_residual(a, g, R, x, w);
+        w_is_wjt_x = true;
+        shown = res0;
+        if (g.rank() == 0) st->fp32_sweeps = sweeps32;
+        if (res0 <= a.pr.residual_tolerance || a.pr.precision == RB_PRECISION_FP32) {
+            for (int i = 4 * R.c0 + g.rank(); i < 4 * R.c1; i += g.size()) sol[i] = x[i];
+            g.sync();
+            const bool ok = res0 <= a.pr.residual_tolerance;
+            if (g.rank() == 0) {
+                st->iterations = ok ? max(sweeps32 - 1, 0) : max_it;
+                st->exitcode = ok ? 3 : 0;
+                st->merit = res0;
+                st->residual = res0;
+            }
+            g.sync();
+            return;
+        }
+        loop_max = a.pr.refine_iterations > 0 ? min(a.pr.refine_iterations, max_it) : 1;
+    }
+    for (int it = 0; it < loop_max; ++it) {
         if (!w_is_wjt_x) scene_wjt(a, g, R, x, w);   // every sweep starts from w = WJT x (contacts.py:72)
         if (jacobi) {               // proximal_contact/jacobi_solver.py:41-79
             const bool hybrid = scheme == RB_SCHEME_JACOBI_HYBRID;
@@ -1105,7 +1129,7 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
             for (int i = 4 * R.c0 + g.rank(); i < 4 * R.c1; i += g.size()) m = nanmax(m, fabs(x[i] - sol[i]));
             merit = g.max(m);
         }
-        const bool check = by_residual && (!fixed_r || (it + 1) % interval == 0 || it + 1 == max_it);
+        const bool check = by_residual && (!fixed_r || (it + 1) % interval == 0 || it + 1 == loop_max);
         const double res = check ? scene_residual(a, g, R, x, w) : 0.0;
         int decision = 0;   // 0 accept, 1 reject, 2 keep sol, 3 take x
         bool stop = false, inc = false;
@@ -1164,6 +1188,7 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
         g.sync();
         if (stop) { iterations = it; break; }
     }
+    if (sweeps32 >= 0) iterations = exitcode == 3 ? sweeps32 + iterations : max_it;
     if (by_residual && exitcode != 3) shown = scene_residual(a, g, R, sol, w);   // residual of what is returned
     if (g.rank() == 0) {
         if (!post) {
@@ -1176,6 +1201,209 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
     g.sync();
 }
 
+// ---------------------------------------------------------------------------------------------------------
+// FP32 phase of the FP32 precision modes: the scene's whole contact problem is copied into shared memory as
+// FP32 (J and WJT blocks, b, r, 1/diag, x, mu, body indices, the level order) and swept there, level by
+// level, with the fixed-r rule until the FP32 residual meets the tolerance or stops improving.  The FP64
+// solver then tests the iterate in FP64 and refines it.  Body accumulators are rebuilt from x at every
+// residual test (in the order of each body's contact list, so results are deterministic).
+// ---------------------------------------------------------------------------------------------------------
+struct F32Scene {
+    float *J, *W, *b, *r, *dinv, *x, *mu, *w;
+    int16_t *lo, *hi;
+    uint16_t *order, *lptr;
+    uint8_t* fixed;
+};
+__host__ __device__ inline size_t f32_align(size_t v) { return (v + 15) & ~size_t(15); }
+__host__ __device__ inline size_t f32_bytes(int K, int nb) {
+    size_t o = 0;
+    o += f32_align(sizeof(float) * (size_t)K * 48) * 2;             // J, W
+    o += f32_align(sizeof(float) * (size_t)K * 4) * 4;              // b, r, dinv, x
+    o += f32_align(sizeof(float) * (size_t)K);                      // mu
+    o += f32_align(sizeof(float) * (size_t)nb * 6);                 // w
+    o += f32_align(sizeof(int16_t) * (size_t)K) * 2;                // lo, hi
+    o += f32_align(sizeof(uint16_t) * (size_t)K);                   // order
+    o += f32_align(sizeof(uint16_t) * (size_t)(K + 1));             // lptr
+    o += f32_align((size_t)nb);                                     // fixed
+    return o;
+}
+__device__ inline F32Scene f32_carve(char* base, int K, int nb) {
+    F32Scene f;
+    size_t o = 0;
+    auto take = [&](size_t bytes) { char* p = base + o; o += f32_align(bytes); return p; };
+    f.J = (float*)take(sizeof(float) * (size_t)K * 48);
+    f.W = (float*)take(sizeof(float) * (size_t)K * 48);
+    f.b = (float*)take(sizeof(float) * (size_t)K * 4);
+    f.r = (float*)take(sizeof(float) * (size_t)K * 4);
+    f.dinv = (float*)take(sizeof(float) * (size_t)K * 4);
+    f.x = (float*)take(sizeof(float) * (size_t)K * 4);
+    f.mu = (float*)take(sizeof(float) * (size_t)K);
+    f.w = (float*)take(sizeof(float) * (size_t)nb * 6);
+    f.lo = (int16_t*)take(sizeof(int16_t) * (size_t)K);
+    f.hi = (int16_t*)take(sizeof(int16_t) * (size_t)K);
+    f.order = (uint16_t*)take(sizeof(uint16_t) * (size_t)K);
+    f.lptr = (uint16_t*)take(sizeof(uint16_t) * (size_t)(K + 1));
+    f.fixed = (uint8_t*)take((size_t)nb);
+    return f;
+}
+
+__device__ __forceinline__ void f32_prox(float zs, float zt, float ztau, float mu, float xn, float* o) {
+    if (xn <= 0.0f) { o[0] = 0.0f; o[1] = 0.0f; o[2] = 0.0f; return; }
+    const float radius = mu * xn;
+    const float sqr = fmaf(zs, zs, fmaf(zt, zt, ztau * ztau));
+    if (sqr <= radius * radius) { o[0] = zs; o[1] = zt; o[2] = ztau; return; }
+    const float scale = radius * rsqrtf(sqr);
+    o[0] = zs * scale; o[1] = zt * scale; o[2] = ztau * scale;
+}
+
+// w = WJT x from the shared copies (each body sums its contacts in ascending order)
+__device__ void f32_wjt(const StepArgs& a, const SceneRange& R, const F32Scene& f) {
+    const int nb = R.b1 - R.b0;
+    for (int bl = threadIdx.x; bl < nb; bl += blockDim.x) {
+        float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (!f.fixed[bl]) {
+            const int b = R.b0 + bl;
+            for (int e = a.ws.bc_ptr[b]; e < a.ws.bc_ptr[b + 1]; ++e) {
+                const int code = a.ws.bc_list[e];
+                const int kl = (code >> 1) - R.c0, side = code & 1;
+                const float* Wk = f.W + 48 * kl + 6 * side;
+                const float* xk = f.x + 4 * kl;
+                for (int d = 0; d < 6; ++d)
+                    acc[d] = fmaf(Wk[36 + d], xk[3], fmaf(Wk[24 + d], xk[2], fmaf(Wk[12 + d], xk[1], fmaf(Wk[d], xk[0], acc[d]))));
+            }
+        }
+        for (int d = 0; d < 6; ++d) f.w[6 * bl + d] = acc[d];
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ float f32_jw(const float* Jr, const float* wlo, const float* whi) {
+    float s = 0.0f;
+    for (int c = 0; c < 6; ++c) s = fmaf(Jr[c], wlo[c], s);
+    for (int c = 0; c < 6; ++c) s = fmaf(Jr[6 + c], whi[c], s);
+    return s;
+}
+
+// FP32 residual ||x - prox(x - D^-1 (A x + b))||_inf / max(1, ||x||_inf); rebuilds w first
+__device__ float f32_residual(const StepArgs& a, const SceneRange& R, const F32Scene& f, const BlockGroup& g) {
+    f32_wjt(a, R, f);
+    const int K = R.c1 - R.c0;
+    float m = 0.0f, xm = 0.0f;
+    for (int kl = threadIdx.x; kl < K; kl += blockDim.x) {
+        const float* J = f.J + 48 * kl;
+        const float* wlo = f.w + 6 * f.lo[kl];
+        const float* whi = f.w + 6 * f.hi[kl];
+        float z[4];
+        for (int row = 0; row < 4; ++row)
+            z[row] = f.x[4 * kl + row] - f.dinv[4 * kl + row] * (f32_jw(J + 12 * row, wlo, whi) + f.b[4 * kl + row]);
+        const float pn = fmaxf(z[0], 0.0f);
+        float fr[3];
+        f32_prox(z[1], z[2], z[3], f.mu[kl], pn, fr);
+        const float d[4] = {f.x[4 * kl] - pn, f.x[4 * kl + 1] - fr[0], f.x[4 * kl + 2] - fr[1], f.x[4 * kl + 3] - fr[2]};
+        for (int i = 0; i < 4; ++i) {
+            m = fmaxf(m, fabsf(d[i]));
+            if (d[i] != d[i]) m = d[i];
+            xm = fmaxf(xm, fabsf(f.x[4 * kl + i]));
+        }
+    }
+    const double mres = g.max((double)m);
+    const double mx = g.max((double)xm);
+    return (float)(mres / (mx > 1.0 ? mx : 1.0));
+}
+
+constexpr int kFp32Block = 128;
+
+// scenes whose FP32 copy takes lo_bytes < bytes <= hi_bytes of shared memory
+__global__ void __launch_bounds__(kFp32Block) k_solve_fp32(const StepArgs a, size_t lo_bytes, size_t hi_bytes) {
+    extern __shared__ __align__(16) char f32_smem[];
+    __shared__ double red[33];
+    __shared__ int ired[33];
+    if (a.ws.counters[kAbort]) return;
+    const BlockGroup g = {red, ired};
+    const int max_it = a.pr.max_iterations;
+    const int interval = a.pr.residual_interval > 1 ? a.pr.residual_interval : 1;
+    const float tol = (float)a.pr.residual_tolerance;
+    for (int s = blockIdx.x; s < a.bd.n_scenes; s += gridDim.x) {
+        const SceneRange R = scene_range(a, s);
+        const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
+        if (K == 0 || K > 65535) continue;
+        const size_t bytes = f32_bytes(K, nb);
+        if (bytes <= lo_bytes || bytes > hi_bytes) continue;
+        const int L = scene_levels(a, g, R, s);
+        const F32Scene f = f32_carve(f32_smem, K, nb);
+        for (int i = threadIdx.x; i < 48 * K; i += blockDim.x) {
+            f.J[i] = (float)a.ws.J[48 * (size_t)R.c0 + i];
+            f.W[i] = (float)a.ws.WJT[48 * (size_t)R.c0 + i];
+        }
+        for (int i = threadIdx.x; i < 4 * K; i += blockDim.x) {
+            const size_t gi = 4 * (size_t)R.c0 + i;
+            f.b[i] = (float)a.ws.b[gi];
+            f.r[i] = (float)a.ws.r[gi];
+            f.dinv[i] = (float)(1.0 / a.ws.diag[gi]);
+            f.x[i] = (float)a.ws.x[gi];
+        }
+        for (int kl = threadIdx.x; kl < K; kl += blockDim.x) {
+            const int k = R.c0 + kl;
+            f.mu[kl] = (float)a.ws.mu[k];
+            f.lo[kl] = (int16_t)(a.ws.lohi[2 * k] - R.b0);
+            f.hi[kl] = (int16_t)(a.ws.lohi[2 * k + 1] - R.b0);
+            f.order[kl] = (uint16_t)(a.ws.lev_order[R.c0 + kl] - R.c0);
+        }
+        for (int l = threadIdx.x; l <= L; l += blockDim.x) f.lptr[l] = (uint16_t)a.ws.lev_ptr[R.c0 + s + l];
+        for (int bl = threadIdx.x; bl < nb; bl += blockDim.x) f.fixed[bl] = a.bd.fixed[R.b0 + bl];
+        __syncthreads();
+        float res = f32_residual(a, R, f, g);   // the warm-started iterate may already be good enough
+        float best = res;
+        int sweeps = 0, stalls = 0;
+        while (res > tol && sweeps < max_it) {
+            for (int l = 1; l <= L; ++l) {
+                for (int i = f.lptr[l - 1] + threadIdx.x; i < f.lptr[l]; i += blockDim.x) {
+                    const int kl = f.order[i];
+                    const int lo = f.lo[kl], hi = f.hi[kl];
+                    const float* J = f.J + 48 * kl;
+                    float* wlo = f.w + 6 * lo;
+                    float* whi = f.w + 6 * hi;
+                    float xo[4], z[4];
+                    for (int row = 0; row < 4; ++row) {
+                        xo[row] = f.x[4 * kl + row];
+                        z[row] = xo[row] - f.r[4 * kl + row] * (f32_jw(J + 12 * row, wlo, whi) + f.b[4 * kl + row]);
+                    }
+                    const float xn = fmaxf(z[0], 0.0f);
+                    float fr[3];
+                    f32_prox(z[1], z[2], z[3], f.mu[kl], xn, fr);
+                    const float d[4] = {xn - xo[0], fr[0] - xo[1], fr[1] - xo[2], fr[2] - xo[3]};
+                    f.x[4 * kl] = xn; f.x[4 * kl + 1] = fr[0]; f.x[4 * kl + 2] = fr[1]; f.x[4 * kl + 3] = fr[2];
+                    const float* Wk = f.W + 48 * kl;
+                    for (int side = 0; side < 2; ++side) {
+                        if (f.fixed[side ? hi : lo]) continue;
+                        float* wb = side ? whi : wlo;
+                        const float* Ws = Wk + 6 * side;
+                        for (int dd = 0; dd < 6; ++dd)
+                            wb[dd] += fmaf(Ws[36 + dd], d[3], fmaf(Ws[24 + dd], d[2], fmaf(Ws[12 + dd], d[1], Ws[dd] * d[0])));
+                    }
+                }
+                __syncthreads();
+            }
+            ++sweeps;
+            if (sweeps % interval == 0 || sweeps == max_it) {
+                res = f32_residual(a, R, f, g);
+                // FP32 floor: hand over to FP64 once the FP32 residual stops improving
+                if (res < 0.95f * best) { best = res; stalls = 0; }
+                else if (++stalls >= 3) break;
+            }
+        }
+        for (int i = threadIdx.x; i < 4 * K; i += blockDim.x) a.ws.x[4 * (size_t)R.c0 + i] = (double)f.x[i];
+        if (threadIdx.x == 0) a.ws.sweeps32[s] = sweeps;
+        __syncthreads();
+    }
+}
+
+__global__ void k_sweeps32_init(const StepArgs a) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.bd.n_scenes; s += gridDim.x * blockDim.x)
+        a.ws.sweeps32[s] = -1;
+}
+
+constexpr int kSolveBlock = 128;   // threads per scene in the block solver (levels rarely hold more contacts)
 constexpr int kWarpSceneMaxContacts = 2048;
 constexpr int kWarpSceneMaxBodies = 384;
 constexpr int kSolveWarpsPerBlock = 4;
@@ -1200,7 +1428,7 @@ __global__ void __launch_bounds__(32 * kSolveWarpsPerBlock) k_solve_warps(const 
 }
 
 // the other scenes: one block each; the body accumulators are on chip up to smem_bodies bodies
-__global__ void __launch_bounds__(256) k_solve_blocks(const StepArgs a, int post, int warp_bodies, int smem_bodies) {
+__global__ void __launch_bounds__(kSolveBlock) k_solve_blocks(const StepArgs a, int post, int warp_bodies, int smem_bodies) {
     extern __shared__ double wsm[];
     __shared__ double red[33];
     __shared__ int ired[33];
@@ -1422,6 +1650,12 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     if (pr->max_iterations < 0 || pr->max_iterations > caps->max_iterations)
         return fail(RB_ERR_ARG, "rb_step: max_iterations exceeds rb_caps.max_iterations");
     if (!(pr->dt > 0.0)) return fail(RB_ERR_ARG, "rb_step: dt must be positive");
+    if (pr->precision != RB_PRECISION_FP64 &&
+        (pr->termination != RB_TERMINATE_RESIDUAL_FIXED_R ||
+         !(pr->scheme == RB_SCHEME_RIGID_GS || pr->scheme == RB_SCHEME_GS)))
+        return fail(RB_ERR_UNSUPPORTED, "rb_step: FP32 precision needs the fixed-r residual rule and a Gauss-Seidel scheme");
+    if (pr->precision < RB_PRECISION_FP64 || pr->precision > RB_PRECISION_FP32)
+        return fail(RB_ERR_ARG, "rb_step: unknown precision");
     if (sh->max_shape_triangles <= 0 || sh->max_shape_triangles > 32 * kMaxClustersPerShape)
         return fail(RB_ERR_ARG, "rb_step: max_shape_triangles must be in 1..16384");
     size_t need = 0;
@@ -1488,17 +1722,25 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     const int wg = (bd->n_scenes + kSolveWarpsPerBlock - 1) / kSolveWarpsPerBlock;
     const int smem_bodies = bd->max_scene_bodies <= kSolveSmemBodies ? bd->max_scene_bodies : 0;
     const size_t block_smem = (size_t)6 * sizeof(double) * (smem_bodies > 0 ? smem_bodies : 1);
-    const int bg = bd->n_scenes < 148 * 8 ? bd->n_scenes : 148 * 8;
+    const int bg = bd->n_scenes < 148 * 16 ? bd->n_scenes : 148 * 16;
     if (warp_smem > 48 * 1024) cudaFuncSetAttribute(k_solve_warps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)warp_smem);
     if (block_smem > 48 * 1024) cudaFuncSetAttribute(k_solve_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)block_smem);
+    k_sweeps32_init<<<blocks_for(bd->n_scenes, 256), 256, 0, st>>>(a);
+    if (pr->precision != RB_PRECISION_FP64) {
+        // FP32 phase in shared memory: small scenes several per SM, larger ones one per SM
+        const size_t small = 48 * 1024 - 1024, large = 200 * 1024;
+        cudaFuncSetAttribute(k_solve_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)large);
+        k_solve_fp32<<<bg, kFp32Block, small, st>>>(a, 0, small);
+        k_solve_fp32<<<148, kFp32Block, large, st>>>(a, small, large);
+    }
     if (warp_bodies > 0) k_solve_warps<<<wg, 32 * kSolveWarpsPerBlock, warp_smem, st>>>(a, 0, warp_bodies);
-    k_solve_blocks<<<bg, 256, block_smem, st>>>(a, 0, warp_bodies, smem_bodies);
+    k_solve_blocks<<<bg, kSolveBlock, block_smem, st>>>(a, 0, warp_bodies, smem_bodies);
     prof_mark(prof, 5, st);
     k_integrate<<<blocks_for(N, 128), 128, 0, st>>>(a);
     if (pr->use_post_stabilization) {
         k_post_setup<<<G, 128, 0, st>>>(a);
         if (warp_bodies > 0) k_solve_warps<<<wg, 32 * kSolveWarpsPerBlock, warp_smem, st>>>(a, 1, warp_bodies);
-        k_solve_blocks<<<bg, 256, block_smem, st>>>(a, 1, warp_bodies, smem_bodies);
+        k_solve_blocks<<<bg, kSolveBlock, block_smem, st>>>(a, 1, warp_bodies, smem_bodies);
         k_post_apply<<<blocks_for(N, 128), 128, 0, st>>>(a);
     }
     k_scene_summary<<<blocks_for(bd->n_scenes, 64), 64, 0, st>>>(a);

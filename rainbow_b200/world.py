@@ -34,7 +34,8 @@ def params_from_vector(vec):
 
 
 def make_rb_params(p, dt=None, scheme="rigid_gauss_seidel", termination="merit", residual_tolerance=1e-6,
-                   profiling=False, warm_start=False, residual_interval=1):
+                   profiling=False, warm_start=False, residual_interval=1, relaxation=1.0, precision="fp64",
+                   refine_iterations=20):
     """rb_params from a Parameters-like mapping (types.py:356 field names)."""
     g = p.__getitem__ if isinstance(p, dict) else (lambda k: getattr(p, k))
     rp = N.RbParams()
@@ -56,6 +57,10 @@ def make_rb_params(p, dt=None, scheme="rigid_gauss_seidel", termination="merit",
     rp.profiling = int(bool(profiling))
     rp.warm_start = int(bool(warm_start))
     rp.residual_interval = int(residual_interval)
+    rp.relaxation = float(relaxation)
+    rp.precision = {"fp64": N.PRECISION_FP64, "fp32_refine": N.PRECISION_FP32_REFINE,
+                    "fp32": N.PRECISION_FP32}[precision]
+    rp.refine_iterations = int(refine_iterations)
     return rp
 
 

@@ -206,3 +206,36 @@ def test_residual_interval_matches_oracle(oracle_lib):
         assert st.exitcode == 3 and (st.iterations + 1) % 4 == 0
         np.testing.assert_array_equal(world.contacts()["sol"], o["sol"])
         np.testing.assert_array_equal(world.state()[0].ravel(), o["x"])
+
+
+@pytest.mark.parametrize("name", ["c1_boxes64", "spheres"])
+def test_fp32_refine_meets_the_fp64_tolerance(name):
+    """FP32 sweeps on chip followed by FP64 refinement: the FP64 residual meets the tolerance and the step's
+    velocities agree with the FP64 solve to a small fraction of their scale."""
+    from rainbow_b200 import world as W
+    d = load_fixture(name)
+    p = W.params_from_vector(d["params"])
+    p["max_iterations"] = 400
+    kw = dict(termination="residual_fixed_r", residual_tolerance=1e-6, residual_interval=4)
+    w64 = _world(d, max_iterations=400)
+    w32 = _world(d, max_iterations=400)
+    w64.step(W.make_rb_params(p, precision="fp64", **kw))
+    w32.step(W.make_rb_params(p, precision="fp32_refine", refine_iterations=100, **kw))
+    s64, s32 = w64.stats()[0], w32.stats()[0]
+    assert s64.exitcode == 3 and s32.exitcode == 3
+    assert s32.residual <= 1e-6 and s32.fp32_sweeps > 0
+    np.testing.assert_array_equal(w32.contacts()["ids"], w64.contacts()["ids"])
+    u64, u32 = w64.state()[1], w32.state()[1]
+    scale = np.abs(u64).max()
+    assert np.abs(u32 - u64).max() <= 1e-3 * scale + 1e-9
+
+
+def test_fp32_only_reports_its_fp64_residual():
+    from rainbow_b200 import world as W
+    d = load_fixture("c1_boxes64")
+    p = W.params_from_vector(d["params"])
+    w32 = _world(d)
+    w32.step(W.make_rb_params(p, precision="fp32", termination="residual_fixed_r", residual_tolerance=1e-6))
+    st = w32.stats()[0]
+    assert st.fp32_sweeps > 0 and np.isfinite(st.residual) and st.residual < 1e-2
+    assert st.exitcode in (0, 3) and (st.exitcode == 3) == (st.residual <= 1e-6)
