@@ -33,7 +33,6 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-LAUNCHES_PER_STEP = 36          # kernels issued by one rb_step without post-stabilisation, batches below 4736 scenes
 
 
 def parse():
@@ -277,8 +276,12 @@ def run_ours(args):
         dist.barrier()
     torch.cuda.synchronize()
     world.t_status.zero_()
+    from rainbow_b200 import _native
+    lib = _native.load()
+    launches0 = lib.rb_launch_count()
     with ClockSampler(local) as clocks:
         times = timed_steps(world, rp, args.steps, stream, flush)
+    launches = lib.rb_launch_count() - launches0
     if world_size > 1:
         dist.barrier()
     status = int(world.t_status[0].item())
@@ -415,7 +418,7 @@ def run_ours(args):
                                                      "contact_setup_solve", "integrate", "total"], phases)},
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+        "gpu_launches": int(launches),
         "clocks": clocks.summary(),
         "status": status,
     }

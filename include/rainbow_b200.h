@@ -231,6 +231,11 @@ int rb_step(const rb_shapes* shapes, const rb_bodies* bodies, const rb_caps* cap
    post-stabilisation, out[6] the whole step.  Returns RB_ERR_ARG if no profiled step was issued. */
 int rb_profile_times(float* out, int32_t n);
 
+/* Number of kernels this library has launched in this process so far (every entry point, all threads and
+   devices).  Callers take the difference around a region to count the device work it issued.  It has no
+   counterpart in the reference. */
+int64_t rb_launch_count(void);
+
 /* rb_step without a workspace argument, for callers that cannot allocate device memory themselves -- for
    example a host application that owns every device allocation through its own fixed pool, or a real-time
    loop that must not call into an allocator once it runs.  The per-step temporaries live in a scratch array

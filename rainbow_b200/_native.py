@@ -92,6 +92,7 @@ SIGNATURES = {
                                ctypes.POINTER(RbParams), ctypes.POINTER(RbOutputs), _vp, ctypes.c_size_t, _vp]),
     "rb_signed_distance_grid": (ctypes.c_int, [_vp, _i32, _vp, _i32, _vp, _vp, _vp]),
     "rb_profile_times": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), _i32]),
+    "rb_launch_count": (ctypes.c_int64, []),
     "rb_step_noalloc": (ctypes.c_int, [ctypes.POINTER(RbShapes), ctypes.POINTER(RbBodies), ctypes.POINTER(RbCaps),
                                        ctypes.POINTER(RbParams), ctypes.POINTER(RbOutputs), _vp]),
 }

@@ -14,6 +14,8 @@
 #include "rb_device.cuh"
 
 namespace rb {
+
+void note_launch();   // rb_step.cu: counts kernels launched by this library
 extern thread_local std::string g_error;
 }
 
@@ -118,6 +120,7 @@ extern "C" int rb_signed_distance_grid(const double* V, int32_t n_vertices, cons
     const int block = 128;
     k_sdf<<<(unsigned)((n_nodes + block - 1) / block), block, 0, (cudaStream_t)stream>>>(V, T, n_triangles,
                                                                                       grid_meta_dev, values);
+    rb::note_launch();
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         rb::g_error = std::string("rb_signed_distance_grid: ") + cudaGetErrorString(e);

@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -33,6 +34,10 @@
 #include "rb_layout.h"
 
 namespace rb {
+
+// kernels launched by this library in this process (rb_launch_count)
+std::atomic<int64_t> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 constexpr int kWarpsPerBlock = 4;
 constexpr int kBlock = 32 * kWarpsPerBlock;
@@ -137,9 +142,9 @@ __global__ void k_scan_down(int32_t* __restrict__ data, const int32_t* n_dev, in
 static void scan(int32_t* data, const int32_t* n_dev, int n_host, int32_t* partial, int32_t* total_out,
                  cudaStream_t st) {
     const int G = 592;   // 4 x 148 SMs
-    k_scan_reduce<<<G, 256, 0, st>>>(data, n_dev, n_host, partial);
-    k_scan_top<<<1, 1024, 0, st>>>(partial, G, total_out);
-    k_scan_down<<<G, 256, 0, st>>>(data, n_dev, n_host, partial);
+    k_scan_reduce<<<G, 256, 0, st>>>(data, n_dev, n_host, partial); note_launch();
+    k_scan_top<<<1, 1024, 0, st>>>(partial, G, total_out); note_launch();
+    k_scan_down<<<G, 256, 0, st>>>(data, n_dev, n_host, partial); note_launch();
 }
 
 __global__ void k_zero_i32(int32_t* p, int n) {
@@ -1675,44 +1680,44 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     const int G = 148 * 8;
     const bool prof = pr->profiling != 0;
     prof_mark(prof, 0, st);
-    k_zero_i32<<<1, 32, 0, st>>>(a.ws.counters, 16);
-    k_zero_stats<<<blocks_for(bd->n_scenes, 128), 128, 0, st>>>(a);
-    k_zero_i32<<<blocks_for(N + 1, 256), 256, 0, st>>>(a.ws.bc_ptr, N + 1);
-    k_zero_i32<<<blocks_for(N, 256), 256, 0, st>>>(a.ws.bc_fill, N);
-    k_bodies<<<blocks_for(N, 128), 128, 0, st>>>(a);
-    k_world_vertices<<<blocks_for(n_body_vertices, 256), 256, 0, st>>>(a, (int)n_body_vertices);
-    k_clusters<<<blocks_for(32 * n_clusters, kBlock), kBlock, 0, st>>>(a, (int)n_clusters);
-    k_roots<<<blocks_for(32 * (int64_t)N, kBlock), kBlock, 0, st>>>(a);
+    k_zero_i32<<<1, 32, 0, st>>>(a.ws.counters, 16); note_launch();
+    k_zero_stats<<<blocks_for(bd->n_scenes, 128), 128, 0, st>>>(a); note_launch();
+    k_zero_i32<<<blocks_for(N + 1, 256), 256, 0, st>>>(a.ws.bc_ptr, N + 1); note_launch();
+    k_zero_i32<<<blocks_for(N, 256), 256, 0, st>>>(a.ws.bc_fill, N); note_launch();
+    k_bodies<<<blocks_for(N, 128), 128, 0, st>>>(a); note_launch();
+    k_world_vertices<<<blocks_for(n_body_vertices, 256), 256, 0, st>>>(a, (int)n_body_vertices); note_launch();
+    k_clusters<<<blocks_for(32 * n_clusters, kBlock), kBlock, 0, st>>>(a, (int)n_clusters); note_launch();
+    k_roots<<<blocks_for(32 * (int64_t)N, kBlock), kBlock, 0, st>>>(a); note_launch();
     prof_mark(prof, 1, st);
     // broad phase
-    k_pairs<false><<<blocks_for(32 * (int64_t)N, kBlock), kBlock, 0, st>>>(a);
+    k_pairs<false><<<blocks_for(32 * (int64_t)N, kBlock), kBlock, 0, st>>>(a); note_launch();
     scan(a.ws.pair_cnt, nullptr, N, a.ws.scan_tmp, a.ws.counters + kNPairs, st);
-    k_check<<<1, 1, 0, st>>>(a.ws.counters, kNPairs, caps->pair_capacity, RB_STATUS_PAIR_OVERFLOW, out->status);
-    k_pairs<true><<<blocks_for(32 * (int64_t)N, kBlock), kBlock, 0, st>>>(a);
+    k_check<<<1, 1, 0, st>>>(a.ws.counters, kNPairs, caps->pair_capacity, RB_STATUS_PAIR_OVERFLOW, out->status); note_launch();
+    k_pairs<true><<<blocks_for(32 * (int64_t)N, kBlock), kBlock, 0, st>>>(a); note_launch();
     // mid phase
     {
         const int max_clusters = (sh->max_shape_triangles + 31) / 32;
         const size_t mid_smem = (size_t)kWarpsPerBlock * 3 * sizeof(uint32_t) * (max_clusters > 0 ? max_clusters : 1);
-        k_mid<<<148 * 16, kBlock, mid_smem, st>>>(a, max_clusters > 0 ? max_clusters : 1);
+        k_mid<<<148 * 16, kBlock, mid_smem, st>>>(a, max_clusters > 0 ? max_clusters : 1); note_launch();
     }
-    k_check<<<1, 1, 0, st>>>(a.ws.counters, kNItems, caps->item_capacity, RB_STATUS_ITEM_OVERFLOW, out->status);
+    k_check<<<1, 1, 0, st>>>(a.ws.counters, kNItems, caps->item_capacity, RB_STATUS_ITEM_OVERFLOW, out->status); note_launch();
     prof_mark(prof, 2, st);
     // narrow phase
-    k_narrow<<<G, 256, 0, st>>>(a);
+    k_narrow<<<G, 256, 0, st>>>(a); note_launch();
     prof_mark(prof, 3, st);
     // reduction and compaction
-    k_dedup<false><<<G, kBlock, 0, st>>>(a);
+    k_dedup<false><<<G, kBlock, 0, st>>>(a); note_launch();
     scan(a.ws.pair_cont, a.ws.counters + kNPairs, caps->pair_capacity, a.ws.scan_tmp, a.ws.counters + kNContacts, st);
-    k_check<<<1, 1, 0, st>>>(a.ws.counters, kNContacts, caps->contact_capacity, RB_STATUS_CONTACT_OVERFLOW, out->status);
-    k_dedup<true><<<G, kBlock, 0, st>>>(a);
+    k_check<<<1, 1, 0, st>>>(a.ws.counters, kNContacts, caps->contact_capacity, RB_STATUS_CONTACT_OVERFLOW, out->status); note_launch();
+    k_dedup<true><<<G, kBlock, 0, st>>>(a); note_launch();
     prof_mark(prof, 4, st);
     // contact problem
-    k_contacts<<<G, 128, 0, st>>>(a);
-    k_body_contacts_count<<<G, 256, 0, st>>>(a);
+    k_contacts<<<G, 128, 0, st>>>(a); note_launch();
+    k_body_contacts_count<<<G, 256, 0, st>>>(a); note_launch();
     scan(a.ws.bc_ptr, nullptr, N, a.ws.scan_tmp, nullptr, st);
-    k_body_contacts_fill<<<G, 256, 0, st>>>(a);
-    k_preds_init<<<G, 256, 0, st>>>(a);
-    k_body_contacts_sort<<<blocks_for(N, 128), 128, 0, st>>>(a);
+    k_body_contacts_fill<<<G, 256, 0, st>>>(a); note_launch();
+    k_preds_init<<<G, 256, 0, st>>>(a); note_launch();
+    k_body_contacts_sort<<<blocks_for(N, 128), 128, 0, st>>>(a); note_launch();
     // solve, integrate, post-stabilise
     // small scenes: one warp each with its body accumulators in shared memory; large scenes: one block each
     // a warp per scene only pays off once the scenes alone fill the GPU (>= 32 per SM); otherwise blocks
@@ -1725,27 +1730,27 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     const int bg = bd->n_scenes < 148 * 16 ? bd->n_scenes : 148 * 16;
     if (warp_smem > 48 * 1024) cudaFuncSetAttribute(k_solve_warps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)warp_smem);
     if (block_smem > 48 * 1024) cudaFuncSetAttribute(k_solve_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)block_smem);
-    k_sweeps32_init<<<blocks_for(bd->n_scenes, 256), 256, 0, st>>>(a);
+    k_sweeps32_init<<<blocks_for(bd->n_scenes, 256), 256, 0, st>>>(a); note_launch();
     if (pr->precision != RB_PRECISION_FP64) {
         // FP32 phase in shared memory: small scenes several per SM, larger ones one per SM
         const size_t small = 48 * 1024 - 1024, large = 200 * 1024;
         cudaFuncSetAttribute(k_solve_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)large);
-        k_solve_fp32<<<bg, kFp32Block, small, st>>>(a, 0, small);
-        k_solve_fp32<<<148, kFp32Block, large, st>>>(a, small, large);
+        k_solve_fp32<<<bg, kFp32Block, small, st>>>(a, 0, small); note_launch();
+        k_solve_fp32<<<148, kFp32Block, large, st>>>(a, small, large); note_launch();
     }
-    if (warp_bodies > 0) k_solve_warps<<<wg, 32 * kSolveWarpsPerBlock, warp_smem, st>>>(a, 0, warp_bodies);
-    k_solve_blocks<<<bg, kSolveBlock, block_smem, st>>>(a, 0, warp_bodies, smem_bodies);
+    if (warp_bodies > 0) { k_solve_warps<<<wg, 32 * kSolveWarpsPerBlock, warp_smem, st>>>(a, 0, warp_bodies); note_launch(); }
+    k_solve_blocks<<<bg, kSolveBlock, block_smem, st>>>(a, 0, warp_bodies, smem_bodies); note_launch();
     prof_mark(prof, 5, st);
-    k_integrate<<<blocks_for(N, 128), 128, 0, st>>>(a);
+    k_integrate<<<blocks_for(N, 128), 128, 0, st>>>(a); note_launch();
     if (pr->use_post_stabilization) {
-        k_post_setup<<<G, 128, 0, st>>>(a);
-        if (warp_bodies > 0) k_solve_warps<<<wg, 32 * kSolveWarpsPerBlock, warp_smem, st>>>(a, 1, warp_bodies);
-        k_solve_blocks<<<bg, kSolveBlock, block_smem, st>>>(a, 1, warp_bodies, smem_bodies);
-        k_post_apply<<<blocks_for(N, 128), 128, 0, st>>>(a);
+        k_post_setup<<<G, 128, 0, st>>>(a); note_launch();
+        if (warp_bodies > 0) { k_solve_warps<<<wg, 32 * kSolveWarpsPerBlock, warp_smem, st>>>(a, 1, warp_bodies); note_launch(); }
+        k_solve_blocks<<<bg, kSolveBlock, block_smem, st>>>(a, 1, warp_bodies, smem_bodies); note_launch();
+        k_post_apply<<<blocks_for(N, 128), 128, 0, st>>>(a); note_launch();
     }
-    k_scene_summary<<<blocks_for(bd->n_scenes, 64), 64, 0, st>>>(a);
-    k_cache_store<<<G, 256, 0, st>>>(a);
-    k_finish<<<1, 1, 0, st>>>(a);
+    k_scene_summary<<<blocks_for(bd->n_scenes, 64), 64, 0, st>>>(a); note_launch();
+    k_cache_store<<<G, 256, 0, st>>>(a); note_launch();
+    k_finish<<<1, 1, 0, st>>>(a); note_launch();
     prof_mark(prof, 6, st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(RB_ERR_CUDA, std::string("rb_step: ") + cudaGetErrorString(e));
@@ -1807,6 +1812,8 @@ int rb_step_noalloc(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* cap
     // previous call's contents of the shared array do no harm
     return rb_step(sh, bd, caps, pr, out, scratch, (size_t)RB_NOALLOC_SCRATCH_BYTES, stream);
 }
+
+int64_t rb_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int rb_profile_times(float* out, int32_t n) {
     if (!out || n < 7) return fail(RB_ERR_ARG, "rb_profile_times: need room for 7 values");

@@ -84,3 +84,9 @@ def test_no_cpu_fallback():
     from conftest import load_fixture
     with pytest.raises(NativeError):
         W.DeviceWorld(load_fixture("boxes8"))
+
+
+def test_launch_counter_is_exported_and_starts_without_device_work():
+    from rainbow_b200 import _native as N
+    lib = N.load()
+    assert lib.rb_launch_count() >= 0
