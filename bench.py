@@ -35,6 +35,9 @@ sys.path.insert(0, ROOT)
 
 
 
+LONG_SWEEPS = 4000   # iteration cap of the converged reference solve the error figures are measured against
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -52,6 +55,8 @@ def parse():
     ap.add_argument("--precision", default="fp32_refine", choices=["fp64", "fp32_refine", "fp32"],
                     help="precision of the batched solve (the plain baseline is always FP64)")
     ap.add_argument("--residual-interval", type=int, default=4)
+    ap.add_argument("--ordering", default="serial", choices=["serial", "coloured"],
+                    help="contact order of the Gauss-Seidel sweeps (both arms use the same)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     ap.add_argument("--cpu-scenes", type=int, default=16, help="scenes in the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
@@ -131,15 +136,15 @@ class ClockSampler:
 def _cpu_worker(job):
     sys.path.insert(0, ROOT)
     from oracle import oracle as O
-    scenes, scheme, tol_mode, tol, pre_roll, seconds = job
+    scenes, scheme, tol_mode, tol, pre_roll, seconds, kw = job
     objs = [O.OracleScene(a) for a in scenes]
     for sc in objs:
         for _ in range(pre_roll):
-            sc.step(scheme=scheme, tol_mode=tol_mode, tol=tol)
+            sc.step(scheme=scheme, tol_mode=tol_mode, tol=tol, **kw)
     steps, t0 = 0, time.perf_counter()
     while True:
         for sc in objs:
-            sc.step(scheme=scheme, tol_mode=tol_mode, tol=tol)
+            sc.step(scheme=scheme, tol_mode=tol_mode, tol=tol, **kw)
             steps += 1
         el = time.perf_counter() - t0
         if el >= seconds or steps >= 400:
@@ -155,7 +160,9 @@ def cpu_baseline(arrays, args, workers):
     tol_mode = {"merit": 0, "residual": 1, "residual_fixed_r": 2}[args.termination]
     sample = arrays[:max(1, min(len(arrays), args.cpu_scenes))]
     workers = max(1, min(workers, len(sample)))
-    jobs = [(sample[w::workers], args.scheme, tol_mode, args.tolerance, args.pre_roll, args.cpu_seconds)
+    kw = {"ordering": args.ordering,
+          "residual_interval": args.residual_interval if args.termination == "residual_fixed_r" else 1}
+    jobs = [(sample[w::workers], args.scheme, tol_mode, args.tolerance, args.pre_roll, args.cpu_seconds, kw)
             for w in range(workers)]
     if workers == 1:
         res = [_cpu_worker(jobs[0])]
@@ -178,7 +185,8 @@ def run_reference(args):
     dev = "cuda:0" if torch.cuda.is_available() else "cpu"
     arrays, params, cfg, _ = build_workload(args.workload, dev, args.scenes)
     value, info = cpu_baseline(arrays, args, workers if len(arrays) > 1 else 1)
-    cfg.update({"scheme": args.scheme, "termination": args.termination, "tolerance": args.tolerance})
+    cfg.update({"scheme": args.scheme, "ordering": args.ordering, "termination": args.termination,
+                "tolerance": args.tolerance})
     line = {
         "impl": "reference", "metric": "scene-steps/s", "value": value, "unit": "scene-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
@@ -193,13 +201,14 @@ def run_reference(args):
 # --------------------------------------------------------------------------------------------------------------
 # GPU
 # --------------------------------------------------------------------------------------------------------------
-def timed_steps(world, rp, steps, stream, flush):
+def timed_steps(step_fn, steps, stream, flush):
+    """Device time (ms) of each of `steps` calls of step_fn, which enqueues one step on `stream`."""
     import torch
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     for k in range(steps):
         flush.zero_()                      # evict L2 (126 MB) between timed steps
         ev[k][0].record(stream)
-        world.launch(rp)
+        step_fn()
         ev[k][1].record(stream)
     torch.cuda.synchronize()
     return np.array([a.elapsed_time(b) for a, b in ev])   # ms
@@ -222,9 +231,10 @@ def run_ours(args):
     from rainbow_b200.stepper import GpuStepper
     arrays, params, cfg, engine = build_workload(args.workload, dev, args.scenes)
     max_it = int(params.max_iterations)
-    world = W.DeviceWorld(arrays, device=dev, max_iterations=max_it)
+    world = W.DeviceWorld(arrays, device=dev, max_iterations=max(max_it, LONG_SWEEPS))
     kw = dict(scheme=args.scheme, termination=args.termination, residual_tolerance=args.tolerance,
-              residual_interval=args.residual_interval if args.termination == "residual_fixed_r" else 1)
+              residual_interval=args.residual_interval if args.termination == "residual_fixed_r" else 1,
+              ordering=args.ordering)
     warm = not args.no_warm_start
     prec = args.precision if args.termination == "residual_fixed_r" else "fp64"
     rp = W.make_rb_params(params, warm_start=warm, precision=prec, **kw)
@@ -253,20 +263,40 @@ def run_ours(args):
     world.step(rp64)
     x_64, u_64 = world.state()
     stats64 = world.stats()
-    # compare velocities on the scenes where both solves met the tolerance (unconverged iterates of different
-    # precisions are different points of the same unfinished iteration, not a precision error)
-    both = [i for i in range(world.n_scenes) if stats[i].n_contacts > 0 and stats[i].exitcode == 3
-            and stats64[i].exitcode == 3]
-    um, u6 = u_m.reshape(-1, 6), u_64.reshape(-1, 6)
-    rel = []
-    for i in both:
-        b0, b1 = world.scene_start[i], world.scene_start[i + 1]
-        rel.append(np.abs(um[b0:b1] - u6[b0:b1]).max() / max(1e-30, np.abs(u6[b0:b1]).max()))
-    err = {"scenes_compared": len(both),
-           "rel_velocity_error_p50_max": [float(np.median(rel)), float(np.max(rel))] if rel else None,
-           "fp64_converged_scenes": int(sum(1 for s_ in stats64 if s_.n_contacts > 0 and s_.exitcode == 3)),
-           "mode_converged_scenes": int(sum(1 for s_ in stats if s_.n_contacts > 0 and s_.exitcode == 3)),
+    # the same step solved far past the iteration cap: the converged answer both are measured against
+    rp_long = W.make_rb_params(params, warm_start=warm, precision="fp64", **kw)
+    rp_long.max_iterations = LONG_SWEEPS
+    restore()
+    world.step(rp_long)
+    _, u_long = world.state()
+    stats_long = world.stats()
+    um, u6, ul = u_m.reshape(-1, 6), u_64.reshape(-1, 6), u_long.reshape(-1, 6)
+
+    def rel_err(a, b, scenes_):
+        out = []
+        for i in scenes_:
+            b0, b1 = world.scene_start[i], world.scene_start[i + 1]
+            out.append(np.abs(a[b0:b1] - b[b0:b1]).max() / max(1e-30, np.abs(b[b0:b1]).max()))
+        return np.array(out)
+
+    def pct(v):
+        return [float(np.percentile(v, 50)), float(np.percentile(v, 99)), float(v.max())] if len(v) else None
+
+    active = [i for i in range(world.n_scenes) if stats64[i].n_contacts > 0]
+    conv_long = [i for i in active if stats_long[i].exitcode == 3]
+    err = {"per_scene_max_rel_velocity_error_p50_p99_max": {
+               "mode_vs_fp64_same_sweeps": pct(rel_err(um, u6, active)),
+               "mode_vs_fp64_converged": pct(rel_err(um, ul, conv_long)),
+               "fp64_vs_fp64_converged": pct(rel_err(u6, ul, conv_long))},
+           "converged_reference": "FP64, same step, up to %d sweeps; %d of %d scenes met the tolerance"
+                                  % (LONG_SWEEPS, len(conv_long), len(active)),
+           "fp64_converged_scenes": int(sum(1 for i in active if stats64[i].exitcode == 3)),
+           "mode_converged_scenes": int(sum(1 for i in active if stats[i].exitcode == 3)),
            "fp32_sweeps_mean": float(np.mean([s_.fp32_sweeps for s_ in stats if s_.n_contacts > 0] or [0]))}
+    # sizing pass: the timed trajectory once with work-list growth, so no timed step can overflow
+    restore()
+    for _ in range(args.steps):
+        world.step(rp)
     restore()
     for _ in range(max(3, args.warmup)):
         world.step(rp)
@@ -276,12 +306,18 @@ def run_ours(args):
         dist.barrier()
     torch.cuda.synchronize()
     world.t_status.zero_()
+    # the timed steps replay one CUDA graph of the whole step; its kernel count is taken while capturing
     from rainbow_b200 import _native
     lib = _native.load()
     launches0 = lib.rb_launch_count()
+    graph = world.capture(rp)
+    per_replay = lib.rb_launch_count() - launches0
+    restore()
+    torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
-        times = timed_steps(world, rp, args.steps, stream, flush)
-    launches = lib.rb_launch_count() - launches0
+        times = timed_steps(graph.replay, args.steps, stream, flush)
+    launches = per_replay * args.steps
+    del graph
     if world_size > 1:
         dist.barrier()
     status = int(world.t_status[0].item())
@@ -304,7 +340,7 @@ def run_ours(args):
     plain = None
     if n_scenes > 1 and args.plain_scenes > 0:
         x0r, u0r = x0.reshape(-1, 7), u0.reshape(-1, 6)
-        pts = []
+        pts, gts = [], []
         for s in range(min(args.plain_scenes, n_scenes)):
             b0, b1 = world.scene_start[s], world.scene_start[s + 1]
             w1 = W.DeviceWorld(arrays[s], device=dev, max_iterations=max_it)
@@ -312,12 +348,20 @@ def run_ours(args):
             w1.step(rp_plain)              # sizes its work lists
             w1.set_state(x0r[b0:b1], u0r[b0:b1])
             torch.cuda.synchronize()
-            pts.append(timed_steps(w1, rp_plain, args.steps, stream, flush))
-        pt = np.concatenate(pts)
+            pts.append(timed_steps(lambda: w1.launch(rp_plain), args.steps, stream, flush))
+            g1 = w1.capture(rp_plain)      # the same scene-steps replayed from a CUDA graph
+            w1.set_state(x0r[b0:b1], u0r[b0:b1])
+            torch.cuda.synchronize()
+            gts.append(timed_steps(g1.replay, args.steps, stream, flush))
+            del g1
+        pt, gt = np.concatenate(pts), np.concatenate(gts)
         plain = {"value": len(pt) / (pt.sum() / 1000.0), "unit": "scene-steps/s", "scenes_sampled": len(pts),
                  "p50_ms": float(np.percentile(pt, 50)), "p99_ms": float(np.percentile(pt, 99)),
+                 "graph_value": len(gt) / (gt.sum() / 1000.0),
+                 "graph_p50_ms": float(np.percentile(gt, 50)), "graph_p99_ms": float(np.percentile(gt, 99)),
                  "method": "each scene alone: one rb_step launch sequence per scene-step, FP64, same solver settings "
-                           "(bit-identical results to the batch)"}
+                           "(bit-identical results to the batch); graph_* = the same steps replayed from a CUDA "
+                           "graph per scene"}
 
     # end to end through the public API, host buffers in and out every step
     e2e = None
@@ -389,9 +433,11 @@ def run_ours(args):
         cv, info = cpu_baseline(arrays, args, cpu_pool_workers if n_scenes > 1 else 1)
         cpu = dict(value=cv, unit="scene-steps/s", **info)
 
-    cfg.update({"scheme": args.scheme, "termination": args.termination, "tolerance": args.tolerance,
+    cfg.update({"scheme": args.scheme, "ordering": args.ordering, "termination": args.termination,
+                "tolerance": args.tolerance,
                 "precision": prec, "warm_start": warm, "residual_interval": kw["residual_interval"], "pre_roll_steps": args.pre_roll, "contacts_per_step": int(K),
                 "sweeps_per_step_contacts": int(sweeps), "l2": "256 MB buffer written between timed steps",
+                "launch": "each timed step replays one CUDA graph of the whole rb_step",
                 "parallelism": "replicas" if world_size > 1 else "single"})
     line = {
         "metric": "scene-steps/s", "value": value, "unit": "scene-steps/s", "n_gpus": world_size,

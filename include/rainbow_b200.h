@@ -46,7 +46,8 @@ extern "C" {
 #define RB_SCHEME_GS 1                /* proximal_contact/gauss_seidel_solver.py:8 GaussSeidelSolver */
 #define RB_SCHEME_JACOBI 2            /* proximal_contact/jacobi_solver.py:41 ParallelJacobiSolver */
 #define RB_SCHEME_JACOBI_HYBRID 3     /* proximal_contact/jacobi_solver.py:60 ParallelJacobiHybridSolver */
-#define RB_SCHEME_COLOURED_GS 4       /* graph-coloured Gauss-Seidel (proximal_contact/gauss_seidel_solver.py:89) */
+#define RB_SCHEME_COLOURED_GS 4       /* graph-coloured Gauss-Seidel (proximal_contact/gauss_seidel_solver.py:89
+                                         ParallelGaussSeidelSolver): the RB_SCHEME_GS rules swept in RB_ORDER_COLOURED */
 
 /* termination rules */
 #define RB_TERMINATE_MERIT 0          /* the reference's iterate-change merit (problem.py:53) */
@@ -57,6 +58,11 @@ extern "C" {
                                          accepted and r stays at its initial value */
 
 /* solver precision */
+#define RB_ORDER_SERIAL 0             /* ascending contact order, as the reference sweeps (contacts.py:74) */
+#define RB_ORDER_COLOURED 1           /* colour by colour: contacts that share no non-fixed body form a colour
+                                         (deterministic Jones-Plassmann colouring with hashed priorities); the
+                                         order RB_SCHEME_COLOURED_GS always uses */
+
 #define RB_PRECISION_FP64 0           /* every sweep in FP64 (bit-exact with the reference's NumPy step) */
 #define RB_PRECISION_FP32_REFINE 1    /* sweeps in FP32 on chip until the residual tolerance, then FP64 sweeps until
                                          the FP64 residual meets it */
@@ -151,11 +157,15 @@ typedef struct rb_params {
                                      (values below 1 mean every sweep); the other rules test every sweep */
     int32_t precision;            /* RB_PRECISION_*; the FP32 modes need RB_TERMINATE_RESIDUAL_FIXED_R and a
                                      Gauss-Seidel scheme */
-    int32_t refine_iterations;    /* RB_PRECISION_FP32_REFINE: cap of the FP64 sweeps after the FP32 phase */
+    int32_t refine_iterations;    /* RB_PRECISION_FP32_REFINE: FP64 sweeps reserved after the FP32 phase (at least 1,
+                                     at most max_iterations).  The FP32 phase sweeps until its residual meets the
+                                     tolerance, stalls below 1e-4, or max_iterations - refine_iterations sweeps
+                                     are done; the FP64 refinement then gets the sweeps left of max_iterations */
     int32_t warm_start;           /* nonzero: start each contact's impulse from the previous step's solution for
                                      the same (body pair, side, triangle) found in rb_outputs.cache_*; the
                                      reference always starts from zero (contacts.py:53), so this is off for
                                      parity runs */
+    int32_t ordering;             /* RB_ORDER_*: contact visiting order of the Gauss-Seidel schemes */
 } rb_params;
 
 /* Per-scene results of one step. */

@@ -78,6 +78,7 @@ def lib():
                                ctypes.c_double]
         L.rbo_set_residual_interval.argtypes = [ctypes.c_int]
         L.rbo_set_relaxation.argtypes = [ctypes.c_double]
+        L.rbo_set_ordering.argtypes = [ctypes.c_int]
         L.rbo_colour_contacts.restype = ctypes.c_int
         L.rbo_colour_contacts.argtypes = [ctypes.c_int, ctypes.c_int, _i32, _u8, _i32]
         L.rbo_grid_value.restype = ctypes.c_double
@@ -249,8 +250,11 @@ class OracleScene:
         self.params[PARAM_FIELDS.index(name)] = float(value)
 
     def step(self, dt=None, scheme="rigid_gauss_seidel", capacity=None, tol_mode=0, tol=0.0, residual_interval=1,
-             relaxation=1.0):
-        """Advance one step; returns a dict with the contact set, solver result and statistics."""
+             relaxation=1.0, ordering="serial"):
+        """Advance one step; returns a dict with the contact set, solver result and statistics.
+
+        ordering="coloured" makes the Gauss-Seidel schemes visit contacts colour by colour (the colouring of
+        rbo_colour_contacts); scheme "parallel_gauss_seidel" always does."""
         dt = float(self.params[0] if dt is None else dt)
         cap = int(capacity or max(1024, 64 * self.n_bodies))
         max_it = int(self.params[PARAM_FIELDS.index("max_iterations")])
@@ -265,6 +269,7 @@ class OracleScene:
             setattr(out, k, _ptr(bufs[k], _d))
         lib().rbo_set_residual_interval(int(residual_interval))
         lib().rbo_set_relaxation(float(relaxation))
+        lib().rbo_set_ordering({"serial": 0, "coloured": 1}[ordering])
         rc = lib().rbo_step(ctypes.byref(self.scene), _ptr(self.params, _d), dt, _ptr(self.r, _d), _ptr(self.q, _d),
                             _ptr(self.v, _d), _ptr(self.w, _d), ctypes.byref(out), int(tol_mode), float(tol))
         if rc == 2:

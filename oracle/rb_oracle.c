@@ -675,10 +675,14 @@ static void problem_diag(const Problem* P, double* diag) {
 /* Sweeps                                                                                                   */
 /* ------------------------------------------------------------------------------------------------------ */
 /* constraints/contacts.py:66 Contacts.sweep (serial Gauss-Seidel with incremental w) */
+/* order: contact visiting order (NULL = ascending, the reference's serial sweep).  A colour-grouped order
+   gives the graph-coloured Gauss-Seidel sweep: contacts of one colour share no non-fixed body, so visiting them
+   one after the other equals updating them together from the w left by the earlier colours. */
 static void sweep_gs(const Problem* P, const double* r, const double* b, const double* mu, double* x, double* w,
-                     int normal_only) {
+                     int normal_only, const int32_t* order) {
     wjt_dot(P, x, w);
-    for (int k = 0; k < P->K; ++k) {
+    for (int e = 0; e < P->K; ++e) {
+        const int k = order ? order[e] : e;
         double xb[4], delta[4], z[4];
         for (int i = 0; i < 4; ++i) { xb[i] = x[4 * k + i]; delta[i] = xb[i]; }
         for (int i = 0; i < 4; ++i) z[i] = xb[i] - r[4 * k + i] * (jrow_dot(P, k, i, w) + b[4 * k + i]);
@@ -715,35 +719,6 @@ static void sweep_jacobi(const Problem* P, const double* r, const double* b, con
         double f[3];
         prox_sphere(z[1], z[2], z[3], mu[k], hybrid ? xn : xold[4 * k], f);
         x[4 * k] = xn; x[4 * k + 1] = f[0]; x[4 * k + 2] = f[1]; x[4 * k + 3] = f[2];
-    }
-}
-
-/* Graph-coloured Gauss-Seidel: contacts of one colour share no non-fixed body, so they update together
-   from the w left by all previous colours.  colour_ptr/colour_list: contacts grouped by colour, ascending. */
-static void sweep_coloured(const Problem* P, const double* r, const double* b, const double* mu, double* x,
-                           double* w, const int32_t* colour_ptr, const int32_t* colour_list, int n_colours) {
-    wjt_dot(P, x, w);
-    for (int c = 0; c < n_colours; ++c) {
-        for (int e = colour_ptr[c]; e < colour_ptr[c + 1]; ++e) {
-            const int k = colour_list[e];
-            double xb[4], delta[4], z[4];
-            for (int i = 0; i < 4; ++i) { xb[i] = x[4 * k + i]; delta[i] = xb[i]; }
-            for (int i = 0; i < 4; ++i) z[i] = xb[i] - r[4 * k + i] * (jrow_dot(P, k, i, w) + b[4 * k + i]);
-            xb[0] = z[0] > 0.0 ? z[0] : 0.0;
-            double f[3];
-            prox_sphere(z[1], z[2], z[3], mu[k], xb[0], f);
-            xb[1] = f[0]; xb[2] = f[1]; xb[3] = f[2];
-            for (int i = 0; i < 4; ++i) { x[4 * k + i] = xb[i]; delta[i] = xb[i] - delta[i]; }
-            for (int side = 0; side < 2; ++side) {
-                if (!P->has_w[2 * k + side]) continue;
-                const int bb = P->lohi[2 * k + side];
-                for (int d = 0; d < 6; ++d) {
-                    double s = 0.0;
-                    for (int row = 0; row < 4; ++row) s += P->WJT[48 * k + 12 * row + 6 * side + d] * delta[row];
-                    w[6 * bb + d] = w[6 * bb + d] + s;
-                }
-            }
-        }
     }
 }
 
@@ -824,6 +799,8 @@ static int g_residual_interval = 1;   /* tol_mode 2: residual tested every this 
 static double g_relaxation = 1.0;     /* tol_mode 2: r = relaxation / diag */
 void rbo_set_relaxation(double w) { g_relaxation = w; }
 void rbo_set_residual_interval(int n) { g_residual_interval = n > 1 ? n : 1; }
+static int g_ordering = 0;             /* 1: Gauss-Seidel schemes visit contacts in graph-coloured order */
+void rbo_set_ordering(int o) { g_ordering = o; }
 static double complementarity_residual(const Problem* P, const double* b, const double* mu, const double* x,
                                        double* w) {
     wjt_dot(P, x, w);
@@ -862,14 +839,14 @@ static inline double merit_inf(const double* x, const double* sol, int n) {
 /* gauss_seidel_solver.py:14 solve, for a single problem (contacts or post-stabilisation) */
 static void solve_rigid(const Problem* P, const double* params, double* r, const double* b, const double* mu,
                         double* x, double* sol, double* residuals, int* iterations, int* exitcode, int normal_only,
-                        int tol_mode, double tol) {
+                        int tol_mode, double tol, const int32_t* order) {
     const int n = 4 * P->K, max_it = (int)params[P_MAX_ITER];
     double* w = (double*)malloc(sizeof(double) * 6 * (P->N ? P->N : 1));
     double last_merit = INFINITY, global_last = INFINITY;
     *iterations = max_it; *exitcode = 0;
     for (int it = 0; it < max_it; ++it) {
         double global_merit = 0.0;
-        sweep_gs(P, r, b, mu, x, w, normal_only);
+        sweep_gs(P, r, b, mu, x, w, normal_only, order);
         double merit = merit_inf(x, sol, n);
         if (tol_mode == 2 && g_residual_interval > 1 && (it + 1) % g_residual_interval != 0 && it + 1 != max_it) {
             memcpy(sol, x, sizeof(double) * n);   /* fixed r between residual tests: accept */
@@ -917,8 +894,7 @@ static void solve_rigid(const Problem* P, const double* params, double* r, const
    accepting the iterate.  tol_mode 1 replaces the merit tests by the complementarity residual. */
 static void solve_interface(const Problem* P, const double* params, int scheme, const double* diag, const double* b,
                             const double* mu, double* x, double* sol, double* residuals, int* iterations,
-                            int* exitcode, const int32_t* colour_ptr, const int32_t* colour_list, int n_colours,
-                            int tol_mode, double tol) {
+                            int* exitcode, const int32_t* order, int tol_mode, double tol) {
     const int n = 4 * P->K, max_it = (int)params[P_MAX_ITER];
     double* w = (double*)malloc(sizeof(double) * 6 * (P->N ? P->N : 1));
     double* xold = (double*)malloc(sizeof(double) * (n ? n : 1));
@@ -927,10 +903,9 @@ static void solve_interface(const Problem* P, const double* params, int scheme, 
     double last_merit = INFINITY;
     *iterations = max_it; *exitcode = 0;
     for (int it = 0; it < max_it; ++it) {
-        if (scheme == S_IFACE_GS) sweep_gs(P, r, b, mu, x, w, 0);
-        else if (scheme == S_JACOBI) sweep_jacobi(P, r, b, mu, x, w, xold, 0);
+        if (scheme == S_JACOBI) sweep_jacobi(P, r, b, mu, x, w, xold, 0);
         else if (scheme == S_JACOBI_HYBRID) sweep_jacobi(P, r, b, mu, x, w, xold, 1);
-        else sweep_coloured(P, r, b, mu, x, w, colour_ptr, colour_list, n_colours);
+        else sweep_gs(P, r, b, mu, x, w, 0, order);   /* S_IFACE_GS, S_COLOURED_GS */
         double merit = merit_inf(x, sol, n);
         if (residuals) residuals[it] = merit;
         if (tol_mode == 2 && g_residual_interval > 1 && (it + 1) % g_residual_interval != 0 && it + 1 != max_it) {
@@ -1140,26 +1115,27 @@ int rbo_step(const OScene* sc, const double* params, double dt, double* r, doubl
         g_residual_diag = diag;
 
         int iters = 0, exitc = 0;
-        if (out->scheme == S_RIGID_GS) {
-            solve_rigid(&P, params, rr, b, mu, x, sol, out->residuals, &iters, &exitc, 0, tol_mode, tol);
-        } else {
-            int32_t* colour = NULL; int32_t* cptr = NULL; int32_t* clist = NULL; int nc = 0;
-            if (out->scheme == S_COLOURED_GS) {
-                colour = (int32_t*)malloc(sizeof(int32_t) * K);
-                nc = rbo_colour_contacts(K, N, cl.ids, sc->fixed, colour);
-                cptr = (int32_t*)calloc((size_t)nc + 1, sizeof(int32_t));
-                clist = (int32_t*)malloc(sizeof(int32_t) * K);
-                for (int k = 0; k < K; ++k) cptr[colour[k] + 1]++;
-                for (int c = 0; c < nc; ++c) cptr[c + 1] += cptr[c];
-                int32_t* fill = (int32_t*)calloc((size_t)nc, sizeof(int32_t));
-                for (int k = 0; k < K; ++k) clist[cptr[colour[k]] + fill[colour[k]]++] = k;
-                free(fill);
-                out->n_colours = nc;
-            }
-            solve_interface(&P, params, out->scheme, diag, b, mu, x, sol, out->residuals, &iters, &exitc, cptr,
-                            clist, nc, tol_mode, tol);
-            free(colour); free(cptr); free(clist);
+        /* graph-coloured visiting order: always for S_COLOURED_GS, on request for the other Gauss-Seidel schemes */
+        int32_t* clist = NULL;
+        const int coloured = out->scheme == S_COLOURED_GS ||
+                             (g_ordering == 1 && (out->scheme == S_RIGID_GS || out->scheme == S_IFACE_GS));
+        if (coloured && K > 0) {
+            int32_t* colour = (int32_t*)malloc(sizeof(int32_t) * K);
+            const int nc = rbo_colour_contacts(K, N, cl.ids, sc->fixed, colour);
+            int32_t* cptr = (int32_t*)calloc((size_t)nc + 1, sizeof(int32_t));
+            clist = (int32_t*)malloc(sizeof(int32_t) * K);
+            for (int k = 0; k < K; ++k) cptr[colour[k] + 1]++;
+            for (int c = 0; c < nc; ++c) cptr[c + 1] += cptr[c];
+            for (int k = 0; k < K; ++k) clist[cptr[colour[k]]++] = k;   /* ascending within a colour */
+            free(colour); free(cptr);
+            out->n_colours = nc;
         }
+        if (out->scheme == S_RIGID_GS)
+            solve_rigid(&P, params, rr, b, mu, x, sol, out->residuals, &iters, &exitc, 0, tol_mode, tol, clist);
+        else
+            solve_interface(&P, params, out->scheme, diag, b, mu, x, sol, out->residuals, &iters, &exitc, clist,
+                            tol_mode, tol);
+        free(clist);
         out->iterations = iters; out->exitcode = exitc;
         /* finalize (contacts.py:57) and delta_u += WJT sol (steppers.py:84-85) */
         double* dc = (double*)malloc(sizeof(double) * 6 * N);
@@ -1181,7 +1157,7 @@ int rbo_step(const OScene* sc, const double* params, double dt, double* r, doubl
             double* ps = (double*)calloc((size_t)4 * K, sizeof(double));
             for (int i = 0; i < 4 * K; ++i) pr[i] = 1.0 / diag[i];
             int it2 = 0, ex2 = 0;
-            solve_rigid(&P, params, pr, g, mu, px, ps, NULL, &it2, &ex2, 1, 0, 0.0);
+            solve_rigid(&P, params, pr, g, mu, px, ps, NULL, &it2, &ex2, 1, 0, 0.0, NULL);
             out->post_iterations = it2; out->post_exitcode = ex2;
             double* dr = (double*)malloc(sizeof(double) * 6 * N);
             wjt_dot(&P, ps, dr);

@@ -22,6 +22,7 @@ STATUS_MESH_TOO_LARGE = 32
 SCHEME_RIGID_GS, SCHEME_GS, SCHEME_JACOBI, SCHEME_JACOBI_HYBRID, SCHEME_COLOURED_GS = 0, 1, 2, 3, 4
 TERMINATE_MERIT, TERMINATE_RESIDUAL, TERMINATE_RESIDUAL_FIXED_R = 0, 1, 2
 PRECISION_FP64, PRECISION_FP32_REFINE, PRECISION_FP32 = 0, 1, 2
+ORDER_SERIAL, ORDER_COLOURED = 0, 1
 
 _vp = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -60,7 +61,7 @@ class RbParams(ctypes.Structure):
         ("contact_optimization_tolerance", ctypes.c_double), ("envelope", ctypes.c_double), ("scheme", _i32),
         ("termination", _i32), ("residual_tolerance", ctypes.c_double), ("profiling", _i32),
         ("relaxation", ctypes.c_double), ("residual_interval", _i32), ("precision", _i32),
-        ("refine_iterations", _i32), ("warm_start", _i32),
+        ("refine_iterations", _i32), ("warm_start", _i32), ("ordering", _i32),
     ]
 
 

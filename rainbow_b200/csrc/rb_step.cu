@@ -953,6 +953,9 @@ __device__ __forceinline__ void gs_contact(const StepArgs& a, int k, const doubl
 // the serial sweep exactly.  The levels are the longest-path depths along the per-body predecessor chains,
 // found by parallel relaxation; contacts are then bucketed by level.  Returns the number of levels.
 template <class G>
+__device__ int bucket_classes(const StepArgs& a, const G& g, const SceneRange& R, int s);
+
+template <class G>
 __device__ int scene_levels(const StepArgs& a, const G& g, const SceneRange& R, int s) {
     for (int k = R.c0 + g.rank(); k < R.c1; k += g.size()) a.ws.lev_of[k] = 1;
     g.sync();
@@ -967,6 +970,13 @@ __device__ int scene_levels(const StepArgs& a, const G& g, const SceneRange& R, 
         }
         if (!g.any(changed)) break;
     }
+    return bucket_classes(a, g, R, s);
+}
+
+// Groups the scene's contacts by their class lev_of[k] (1-based level or colour): lev_ptr[c-1] .. lev_ptr[c]
+// index lev_order, which lists the contacts of class c.  Returns the number of classes.
+template <class G>
+__device__ int bucket_classes(const StepArgs& a, const G& g, const SceneRange& R, int s) {
     int L = 0;
     for (int k = R.c0 + g.rank(); k < R.c1; k += g.size()) L = max(L, a.ws.lev_of[k]);
     L = g.imax(L);
@@ -986,6 +996,77 @@ __device__ int scene_levels(const StepArgs& a, const G& g, const SceneRange& R, 
         a.ws.lev_order[R.c0 + atomicAdd(cur + a.ws.lev_of[k] - 1, 1)] = k;
     g.sync();
     return L;
+}
+
+// Graph colouring of the scene's contacts for RB_ORDER_COLOURED: two contacts are neighbours when they share a
+// non-fixed body.  Jones-Plassmann rounds with hashed priorities (higher hash first, then lower scene-local
+// index): in each round every uncoloured contact whose uncoloured neighbours all come later in priority takes
+// the smallest colour none of its coloured neighbours has.  Deterministic, so every launch shape gives the
+// same colours; the oracle's rbo_colour_contacts is the same procedure.
+__device__ __forceinline__ uint32_t jp_hash(uint32_t k) {
+    k ^= k >> 16; k *= 0x7feb352dU; k ^= k >> 15; k *= 0x846ca68bU; k ^= k >> 16;
+    return k;
+}
+__device__ __forceinline__ bool jp_before(int p, int q) {
+    const uint32_t hp = jp_hash((uint32_t)p), hq = jp_hash((uint32_t)q);
+    return hp > hq || (hp == hq && p < q);
+}
+// colour (0-based) contact k takes this round, or -1 while a neighbour of higher priority is uncoloured
+__device__ int colour_pick(const StepArgs& a, const SceneRange& R, int k) {
+    const int* col = a.ws.lev_of;   // colour + 1; 0 = uncoloured
+    uint64_t used = 0;
+    for (int side = 0; side < 2; ++side) {
+        const int b = a.ws.lohi[2 * k + side];
+        if (a.bd.fixed[b]) continue;
+        for (int e = a.ws.bc_ptr[b]; e < a.ws.bc_ptr[b + 1]; ++e) {
+            const int m = a.ws.bc_list[e] >> 1;
+            if (m == k) continue;
+            const int c = col[m];
+            if (c == 0) {
+                if (jp_before(m - R.c0, k - R.c0)) return -1;
+            } else if (c <= 64) {
+                used |= 1ull << (c - 1);
+            }
+        }
+    }
+    for (int c = 0;; ++c) {
+        bool taken = false;
+        if (c < 64) {
+            taken = (used >> c) & 1ull;
+        } else {
+            for (int side = 0; side < 2 && !taken; ++side) {
+                const int b = a.ws.lohi[2 * k + side];
+                if (a.bd.fixed[b]) continue;
+                for (int e = a.ws.bc_ptr[b]; e < a.ws.bc_ptr[b + 1] && !taken; ++e) {
+                    const int m = a.ws.bc_list[e] >> 1;
+                    taken = m != k && col[m] == c + 1;
+                }
+            }
+        }
+        if (!taken) return c;
+    }
+}
+template <class G>
+__device__ int scene_colours(const StepArgs& a, const G& g, const SceneRange& R, int s) {
+    int* col = a.ws.lev_of;
+    int* pick = a.ws.lev_cur + R.c0 + s;   // this round's choices (the class counters are built afterwards)
+    for (int k = R.c0 + g.rank(); k < R.c1; k += g.size()) col[k] = 0;
+    g.sync();
+    const int K = R.c1 - R.c0;
+    for (int round = 0; round <= K; ++round) {   // every round colours at least the top-priority contact
+        bool left = false;
+        for (int k = R.c0 + g.rank(); k < R.c1; k += g.size()) {
+            int c = -1;
+            if (col[k] == 0) { c = colour_pick(a, R, k); left = true; }
+            pick[k - R.c0] = c;
+        }
+        g.sync();
+        if (!g.any(left)) break;
+        for (int k = R.c0 + g.rank(); k < R.c1; k += g.size())
+            if (pick[k - R.c0] >= 0) col[k] = pick[k - R.c0] + 1;
+        g.sync();
+    }
+    return bucket_classes(a, g, R, s);
 }
 
 template <class G>
@@ -1077,7 +1158,9 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
     }
     const bool on_chip = w_smem != nullptr && nb <= smem_bodies;
     const WView w = {on_chip ? w_smem : a.ws.w + 6 * R.b0, R.b0};
-    const int L = jacobi ? 0 : scene_levels(a, g, R, s);
+    const bool coloured = !post && !jacobi &&
+                          (scheme == RB_SCHEME_COLOURED_GS || a.pr.ordering == RB_ORDER_COLOURED);
+    const int L = jacobi ? 0 : (coloured ? scene_colours(a, g, R, s) : scene_levels(a, g, R, s));
     if (!post && g.rank() == 0) st->n_levels = L;
     const bool by_residual = !post && a.pr.termination != RB_TERMINATE_MERIT;
     const bool fixed_r = !post && a.pr.termination == RB_TERMINATE_RESIDUAL_FIXED_R;
@@ -1106,7 +1189,7 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
             g.sync();
             return;
         }
-        loop_max = a.pr.refine_iterations > 0 ? min(a.pr.refine_iterations, max_it) : 1;
+        loop_max = max(max_it - sweeps32, 1);   // the sweeps the FP32 phase left over
     }
     for (int it = 0; it < loop_max; ++it) {
         if (!w_is_wjt_x) scene_wjt(a, g, R, x, w);   // every sweep starts from w = WJT x (contacts.py:72)
@@ -1317,6 +1400,9 @@ __device__ float f32_residual(const StepArgs& a, const SceneRange& R, const F32S
 }
 
 constexpr int kFp32Block = 128;
+constexpr int kFp32LargeSmem = 200 * 1024;   // shared memory of the one-scene-per-SM FP32 solve
+// relative residual below which a stalled FP32 iteration is taken to have met FP32 rounding
+constexpr float kFp32Floor = 1e-4f;
 
 // scenes whose FP32 copy takes lo_bytes < bytes <= hi_bytes of shared memory
 __global__ void __launch_bounds__(kFp32Block) k_solve_fp32(const StepArgs a, size_t lo_bytes, size_t hi_bytes) {
@@ -1328,13 +1414,18 @@ __global__ void __launch_bounds__(kFp32Block) k_solve_fp32(const StepArgs a, siz
     const int max_it = a.pr.max_iterations;
     const int interval = a.pr.residual_interval > 1 ? a.pr.residual_interval : 1;
     const float tol = (float)a.pr.residual_tolerance;
+    // sweeps left to the FP64 refinement; the two phases together make at most max_iterations sweeps
+    const int reserve = a.pr.precision == RB_PRECISION_FP32_REFINE
+                      ? min(max(a.pr.refine_iterations, 1), max_it) : 0;
+    const int budget = max_it - reserve;
     for (int s = blockIdx.x; s < a.bd.n_scenes; s += gridDim.x) {
         const SceneRange R = scene_range(a, s);
         const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
         if (K == 0 || K > 65535) continue;
         const size_t bytes = f32_bytes(K, nb);
         if (bytes <= lo_bytes || bytes > hi_bytes) continue;
-        const int L = scene_levels(a, g, R, s);
+        const bool coloured = a.pr.scheme == RB_SCHEME_COLOURED_GS || a.pr.ordering == RB_ORDER_COLOURED;
+        const int L = coloured ? scene_colours(a, g, R, s) : scene_levels(a, g, R, s);
         const F32Scene f = f32_carve(f32_smem, K, nb);
         for (int i = threadIdx.x; i < 48 * K; i += blockDim.x) {
             f.J[i] = (float)a.ws.J[48 * (size_t)R.c0 + i];
@@ -1360,7 +1451,7 @@ __global__ void __launch_bounds__(kFp32Block) k_solve_fp32(const StepArgs a, siz
         float res = f32_residual(a, R, f, g);   // the warm-started iterate may already be good enough
         float best = res;
         int sweeps = 0, stalls = 0;
-        while (res > tol && sweeps < max_it) {
+        while (res > tol && sweeps < budget) {
             for (int l = 1; l <= L; ++l) {
                 for (int i = f.lptr[l - 1] + threadIdx.x; i < f.lptr[l]; i += blockDim.x) {
                     const int kl = f.order[i];
@@ -1390,11 +1481,12 @@ __global__ void __launch_bounds__(kFp32Block) k_solve_fp32(const StepArgs a, siz
                 __syncthreads();
             }
             ++sweeps;
-            if (sweeps % interval == 0 || sweeps == max_it) {
+            if (sweeps % interval == 0 || sweeps == budget) {
                 res = f32_residual(a, R, f, g);
-                // FP32 floor: hand over to FP64 once the FP32 residual stops improving
+                // FP32 floor: hand over to FP64 once the residual, already small, stops improving.  Above
+                // the floor a pause is the Gauss-Seidel iteration itself (it is not monotone), so go on.
                 if (res < 0.95f * best) { best = res; stalls = 0; }
-                else if (++stalls >= 3) break;
+                else if (best < kFp32Floor && ++stalls >= 3) break;
             }
         }
         for (int i = threadIdx.x; i < 4 * K; i += blockDim.x) a.ws.x[4 * (size_t)R.c0 + i] = (double)f.x[i];
@@ -1644,20 +1736,48 @@ int rb_workspace_bytes(const rb_bodies* bd, const rb_caps* caps, size_t* bytes) 
     return RB_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// Largest dynamic shared memory of each solver kernel, granted once per device.  Done outside the launch
+// sequence so that a step can be captured into a CUDA graph once the device has seen one uncaptured step.
+std::mutex g_attr_mutex;
+bool g_attr_done[64] = {false};
+int ensure_kernel_attributes() {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 64) return fail(RB_ERR_CUDA, "rb_step: no current device");
+    std::lock_guard<std::mutex> lock(g_attr_mutex);
+    if (g_attr_done[dev]) return RB_OK;
+    const int warp_max = kSolveWarpsPerBlock * 6 * (int)sizeof(double) * kWarpSceneMaxBodies;
+    const int block_max = 6 * (int)sizeof(double) * kSolveSmemBodies;
+    e = cudaFuncSetAttribute(k_solve_warps, cudaFuncAttributeMaxDynamicSharedMemorySize, warp_max);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_solve_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, block_max);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_solve_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, kFp32LargeSmem);
+    if (e != cudaSuccess) return fail(RB_ERR_CUDA, std::string("rb_step: cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+    g_attr_done[dev] = true;
+    return RB_OK;
+}
+}  // namespace
+
+extern "C" {
+
 int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const rb_params* pr,
             const rb_outputs* out, void* workspace, size_t workspace_bytes, void* stream_ptr) {
     if (!sh || !bd || !caps || !pr || !out || !workspace) return fail(RB_ERR_ARG, "rb_step: null argument");
     if (bd->n_bodies <= 0 || bd->n_scenes <= 0) return fail(RB_ERR_ARG, "rb_step: empty scene batch");
     if (!bd->x || !bd->u || !out->contact_ids || !out->stats || !out->status)
         return fail(RB_ERR_ARG, "rb_step: null state or output buffer");
-    if (pr->scheme < 0 || pr->scheme > RB_SCHEME_JACOBI_HYBRID)
-        return fail(RB_ERR_UNSUPPORTED, "rb_step: solver scheme not available in this build");
+    if (pr->scheme < 0 || pr->scheme > RB_SCHEME_COLOURED_GS)
+        return fail(RB_ERR_UNSUPPORTED, "rb_step: unknown solver scheme");
+    if (pr->ordering != RB_ORDER_SERIAL && pr->ordering != RB_ORDER_COLOURED)
+        return fail(RB_ERR_ARG, "rb_step: unknown contact ordering");
     if (pr->max_iterations < 0 || pr->max_iterations > caps->max_iterations)
         return fail(RB_ERR_ARG, "rb_step: max_iterations exceeds rb_caps.max_iterations");
     if (!(pr->dt > 0.0)) return fail(RB_ERR_ARG, "rb_step: dt must be positive");
     if (pr->precision != RB_PRECISION_FP64 &&
         (pr->termination != RB_TERMINATE_RESIDUAL_FIXED_R ||
-         !(pr->scheme == RB_SCHEME_RIGID_GS || pr->scheme == RB_SCHEME_GS)))
+         !(pr->scheme == RB_SCHEME_RIGID_GS || pr->scheme == RB_SCHEME_GS || pr->scheme == RB_SCHEME_COLOURED_GS)))
         return fail(RB_ERR_UNSUPPORTED, "rb_step: FP32 precision needs the fixed-r residual rule and a Gauss-Seidel scheme");
     if (pr->precision < RB_PRECISION_FP64 || pr->precision > RB_PRECISION_FP32)
         return fail(RB_ERR_ARG, "rb_step: unknown precision");
@@ -1667,6 +1787,8 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     int rc = rb_workspace_bytes(bd, caps, &need);
     if (rc != RB_OK) return rc;
     if (workspace_bytes < need) return fail(RB_ERR_WORKSPACE, "rb_step: workspace too small");
+    rc = ensure_kernel_attributes();
+    if (rc != RB_OK) return rc;
     const int64_t n_body_vertices = bd->n_body_vertices, n_body_triangles = bd->n_body_triangles,
                   n_clusters = bd->n_clusters;
     cudaStream_t st = (cudaStream_t)stream_ptr;
@@ -1728,13 +1850,10 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     const int smem_bodies = bd->max_scene_bodies <= kSolveSmemBodies ? bd->max_scene_bodies : 0;
     const size_t block_smem = (size_t)6 * sizeof(double) * (smem_bodies > 0 ? smem_bodies : 1);
     const int bg = bd->n_scenes < 148 * 16 ? bd->n_scenes : 148 * 16;
-    if (warp_smem > 48 * 1024) cudaFuncSetAttribute(k_solve_warps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)warp_smem);
-    if (block_smem > 48 * 1024) cudaFuncSetAttribute(k_solve_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)block_smem);
     k_sweeps32_init<<<blocks_for(bd->n_scenes, 256), 256, 0, st>>>(a); note_launch();
     if (pr->precision != RB_PRECISION_FP64) {
         // FP32 phase in shared memory: small scenes several per SM, larger ones one per SM
-        const size_t small = 48 * 1024 - 1024, large = 200 * 1024;
-        cudaFuncSetAttribute(k_solve_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)large);
+        const size_t small = 48 * 1024 - 1024, large = kFp32LargeSmem;
         k_solve_fp32<<<bg, kFp32Block, small, st>>>(a, 0, small); note_launch();
         k_solve_fp32<<<148, kFp32Block, large, st>>>(a, small, large); note_launch();
     }

@@ -105,7 +105,9 @@ class GpuStepper:
         scheme = getattr(engine.params, "proximal_solver", None) or "rigid_gauss_seidel"
         rp = W.make_rb_params(engine.params, dt=dt, scheme=scheme, termination=self.termination,
                               residual_tolerance=self.residual_tolerance, profiling=profiling_on,
-                              warm_start=bool(getattr(engine.params, "warm_start", False)))
+                              warm_start=bool(getattr(engine.params, "warm_start", False)),
+                              ordering=getattr(engine.params, "contact_ordering", None) or "serial",
+                              precision=getattr(engine.params, "solver_precision", None) or "fp64")
         status = world.step(rp)
         if status & 16:
             raise RuntimeError("ContactPoint.init() was called with non-unit size normal")

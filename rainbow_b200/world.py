@@ -35,8 +35,11 @@ def params_from_vector(vec):
 
 def make_rb_params(p, dt=None, scheme="rigid_gauss_seidel", termination="merit", residual_tolerance=1e-6,
                    profiling=False, warm_start=False, residual_interval=1, relaxation=1.0, precision="fp64",
-                   refine_iterations=20):
-    """rb_params from a Parameters-like mapping (types.py:356 field names)."""
+                   refine_iterations=20, ordering="serial"):
+    """rb_params from a Parameters-like mapping (types.py:356 field names).
+
+    ordering="coloured" sweeps the Gauss-Seidel schemes colour by colour (the scheme
+    "parallel_gauss_seidel" always does); "serial" is the reference's ascending order."""
     g = p.__getitem__ if isinstance(p, dict) else (lambda k: getattr(p, k))
     rp = N.RbParams()
     rp.dt = float(g("time_step") if dt is None else dt)
@@ -61,6 +64,7 @@ def make_rb_params(p, dt=None, scheme="rigid_gauss_seidel", termination="merit",
     rp.precision = {"fp64": N.PRECISION_FP64, "fp32_refine": N.PRECISION_FP32_REFINE,
                     "fp32": N.PRECISION_FP32}[precision]
     rp.refine_iterations = int(refine_iterations)
+    rp.ordering = {"serial": N.ORDER_SERIAL, "coloured": N.ORDER_COLOURED}[ordering]
     return rp
 
 
@@ -319,6 +323,21 @@ class DeviceWorld:
                               ctypes.byref(rb_params), ctypes.byref(self.rb_outputs), self.t_ws.data_ptr(),
                               self.workspace_bytes, ctypes.c_void_p(st.cuda_stream))
         N.check(rc, "rb_step")
+
+    def capture(self, rb_params):
+        """Record one step of every scene into a CUDA graph and return it.
+
+        Replaying the graph (``graph.replay()``) advances the batch exactly like :meth:`launch` with the
+        parameters given here, on the stream that replays it.  The graph holds the device addresses of this
+        world's tensors, so capacity growth (which reallocates them) invalidates it: check ``t_status`` after
+        replays and capture again after a growing :meth:`step`.  The device must have run one uncaptured step
+        first (it grants the solver kernels their shared memory outside any capture)."""
+        if rb_params.profiling:
+            raise ValueError("profiling steps record host-side events and cannot be captured")
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            self.launch(rb_params)
+        return graph
 
     def step(self, rb_params, max_retries=8):
         """One synchronous step with automatic capacity growth.  Returns the status word."""

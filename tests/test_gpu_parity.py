@@ -239,3 +239,85 @@ def test_fp32_only_reports_its_fp64_residual():
     st = w32.stats()[0]
     assert st.fp32_sweeps > 0 and np.isfinite(st.residual) and st.residual < 1e-2
     assert st.exitcode in (0, 3) and (st.exitcode == 3) == (st.residual <= 1e-6)
+
+
+def test_graph_replay_equals_direct_steps():
+    """A step captured into a CUDA graph and replayed advances the batch with the same bits as direct calls."""
+    import torch
+    from rainbow_b200 import world as W
+    ds = [load_fixture(n) for n in ("boxes8", "spheres", "tower6")]
+    params = W.params_from_vector(ds[2]["params"])
+    rp = W.make_rb_params(params, warm_start=True, termination="residual_fixed_r", residual_tolerance=1e-6)
+    direct = W.DeviceWorld(ds, max_iterations=100)
+    graphed = W.DeviceWorld(ds, max_iterations=100)
+    for _ in range(4):
+        direct.step(rp)
+    graphed.step(rp)                       # uncaptured first step: sizes the work lists
+    graph = graphed.capture(rp)
+    graphed.t_status.zero_()
+    for _ in range(3):
+        graph.replay()
+    torch.cuda.synchronize()
+    assert int(graphed.t_status[0].item()) == 0
+    for a, b in zip(direct.state(), graphed.state()):
+        np.testing.assert_array_equal(b, a)
+    ca, cb = direct.contacts(), graphed.contacts()
+    for key in ("ids", "p", "sol"):
+        np.testing.assert_array_equal(cb[key], ca[key], err_msg=key)
+
+
+def test_fp32_refine_spends_the_same_sweep_budget():
+    """Unconverged FP32+FP64 solves use exactly max_iterations sweeps, like the FP64 solve they stand in for,
+    with the reserved FP64 sweeps at the end."""
+    from rainbow_b200 import world as W
+    d = load_fixture("c1_boxes64")
+    p = W.params_from_vector(d["params"])
+    p["max_iterations"] = 30
+    w = _world(d, max_iterations=30)
+    w.step(W.make_rb_params(p, precision="fp32_refine", refine_iterations=10, termination="residual_fixed_r",
+                            residual_tolerance=1e-12))
+    st = w.stats()[0]
+    assert st.exitcode == 0 and st.iterations == 30
+    assert 0 < st.fp32_sweeps <= 20
+
+
+@pytest.mark.parametrize("scheme,ordering,termination,mode", [
+    ("parallel_gauss_seidel", "serial", "merit", 0),
+    ("rigid_gauss_seidel", "coloured", "merit", 0),
+    ("rigid_gauss_seidel", "coloured", "residual_fixed_r", 2),
+    ("gauss_seidel", "coloured", "residual", 1),
+])
+@pytest.mark.parametrize("name", ["c1_boxes64", "tower6", "spheres"])
+def test_coloured_gauss_seidel_matches_oracle(oracle_lib, name, scheme, ordering, termination, mode):
+    """Graph-coloured sweeps: the GPU colours the contacts like the oracle (same number of colours) and the
+    chained steps stay bit-identical to it."""
+    from rainbow_b200 import world as W
+    d = load_fixture(name)
+    p = W.params_from_vector(d["params"])
+    world = _world(d)
+    sc = oracle_lib.OracleScene(d)
+    for _ in range(3):
+        world.step(W.make_rb_params(p, scheme=scheme, ordering=ordering, termination=termination,
+                                    residual_tolerance=1e-6))
+        o = sc.step(scheme=scheme, ordering=ordering, tol_mode=mode, tol=1e-6)
+        st = world.stats()[0]
+        assert st.n_contacts == o["n_contacts"]
+        if o["n_contacts"]:
+            assert st.n_levels == o["n_colours"]
+        assert (st.iterations, st.exitcode) == (o["iterations"], o["exitcode"])
+        np.testing.assert_array_equal(world.contacts()["sol"], o["sol"])
+        x, u = world.state()
+        np.testing.assert_array_equal(x.ravel(), o["x"])
+        np.testing.assert_array_equal(u.ravel(), o["u"])
+
+
+def test_coloured_fp32_refine_meets_the_tolerance():
+    from rainbow_b200 import world as W
+    d = load_fixture("c1_boxes64")
+    p = W.params_from_vector(d["params"])
+    p["max_iterations"] = 400
+    w = _world(d, max_iterations=400)
+    w.step(W.make_rb_params(p, precision="fp32_refine", ordering="coloured", refine_iterations=100,
+                            termination="residual_fixed_r", residual_tolerance=1e-6))
+    st = w.stats()[0]
+    assert st.exitcode == 3 and st.residual <= 1e-6 and st.fp32_sweeps > 0

@@ -143,3 +143,19 @@ def test_colouring_is_valid(oracle_lib):
     path = np.array([[i, i + 1] for i in range(1, 20)], np.int32)
     colour, nc = oracle_lib.colour_contacts(path, fixed, n_bodies)
     assert nc <= 3
+
+
+def test_coloured_order_is_a_valid_gauss_seidel_order(oracle_lib):
+    """The coloured sweep visits colour classes in order; inside a class no two contacts share a non-fixed body,
+    so the class order is a valid parallel schedule.  With the lattice scene the colouring needs far fewer
+    classes than the serial order's dependency levels."""
+    from conftest import load_fixture
+    d = load_fixture("c1_boxes64")
+    sc = oracle_lib.OracleScene(d)
+    o = sc.step(scheme="rigid_gauss_seidel", ordering="coloured")
+    ids, fixed = o["ids"], np.asarray(d["body_fixed"], np.uint8)
+    colour, nc = oracle_lib.colour_contacts(ids, fixed, len(fixed))
+    assert o["n_colours"] == nc
+    for c in range(nc):
+        bodies = [b for b in ids[colour == c].ravel() if not fixed[b]]
+        assert len(bodies) == len(set(bodies))
