@@ -60,6 +60,12 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     ap.add_argument("--cpu-scenes", type=int, default=16, help="scenes in the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=20.0,
+                    help="wall time of the serving run (Poisson arrivals, continuous batching); 0 skips it")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="request arrival rate (requests/s)")
+    ap.add_argument("--serve-max-bodies", type=int, default=131072,
+                    help="resident-body cap of the server (its step-latency target)")
+    ap.add_argument("--serve-templates", type=int, default=192, help="distinct scenes the requests draw from")
     return ap.parse_args()
 
 
@@ -196,6 +202,71 @@ def run_reference(args):
         "e2e": {"value": value, "unit": "scene-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------------------------------------------
+# serving: Poisson stream of scene simulations through the continuous-batching server
+# --------------------------------------------------------------------------------------------------------------
+def run_serving(args, dev, rp_kw, max_it):
+    """Requests arrive as a Poisson stream (rate --serve-rate) of scenes with 16..2048 bodies (log-uniform) and
+    horizons U[50, 500] steps; the server admits them by its memory budget (80 % of the device) and body cap.
+    Returns throughput and latency of the run and of the same scenes stepped alone, one per launch."""
+    import torch
+    from rainbow_b200 import scenes, serving, world as W
+    templates, params = scenes.batch_arrays(n_scenes=args.serve_templates, seed=1, pool=64,
+                                            body_range=(16, 2048), resolution=32, device=dev, ground=40.0)
+    rp = W.make_rb_params(params, **rp_kw)
+    rng = np.random.default_rng(7)
+    srv = serving.Server(rp, device=dev, max_iterations=max_it, hbm_fraction=0.8,
+                         max_active_bodies=args.serve_max_bodies)
+    t_start = time.perf_counter()
+    next_arrival = t_start
+    submitted = 0
+    while True:
+        now = time.perf_counter()
+        if now - t_start >= args.serve_seconds:
+            break
+        while next_arrival <= now:
+            srv.submit(templates[int(rng.integers(len(templates)))], int(rng.integers(50, 501)), arrival=next_arrival)
+            submitted += 1
+            next_arrival += rng.exponential(1.0 / args.serve_rate)
+        srv.tick()
+    rep = srv.report()
+    rep.update({"seconds": args.serve_seconds, "arrival_rate": args.serve_rate, "submitted": submitted,
+                "queued_at_end": len(srv.queue), "resident_body_cap": args.serve_max_bodies,
+                "memory_budget_gb": srv.budget / 1e9,
+                "workload": "Poisson requests, scenes of 16..2048 bodies (log-uniform; %d distinct), horizons "
+                            "U[50,500], boxes/spheres as the batch workload on a 40 x 1 x 40 ground"
+                            % len(templates)})
+    # plain: scenes resident at the end of the run, each stepped alone from its current state, one rb_step per
+    # scene-step (FP64, same solver settings)
+    rp64 = W.make_rb_params(params, **dict(rp_kw, precision="fp64"))
+    stream = torch.cuda.current_stream()
+    times = []
+    resident = [r for r in srv.active if r.done < r.horizon]
+    pick = rng.choice(len(resident), size=min(16, len(resident)), replace=False) if resident else []
+    for i in pick:
+        r = resident[int(i)]
+        x, u = srv.batch.scene_state(r.slot)
+        w1 = W.DeviceWorld(r.scene, device=dev, max_iterations=max_it)
+        w1.set_state(x, u)
+        w1.step(rp64)                      # sizes its work lists
+        w1.set_state(x, u)
+        torch.cuda.synchronize()
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            w1.launch(rp64)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+    times = np.array(times)
+    rep["plain"] = {"value": len(times) / (times.sum() / 1000.0), "unit": "scene-steps/s",
+                    "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
+                    "sample": "%d scenes resident at the end of the run, 5 steps each from their current state, one "
+                              "rb_step per scene-step, FP64" % len(pick)}
+    rep["served_vs_plain"] = rep["scene_steps_per_s"] / rep["plain"]["value"] if rep.get("scene_steps_per_s") else None
+    return rep
 
 
 # --------------------------------------------------------------------------------------------------------------
@@ -428,6 +499,10 @@ def run_ours(args):
     dt_s, nbytes, model = alg[dom]
     achieved = nbytes / dt_s / 1e9 if dt_s > 0 else 0.0
 
+    serving_rep = None
+    if args.serve_seconds > 0 and args.workload == "batch1024":
+        serving_rep = run_serving(args, dev, dict(warm_start=warm, precision=prec, **kw), max_it)
+
     cpu = None
     if rank == 0 and args.cpu_seconds > 0:
         cv, info = cpu_baseline(arrays, args, cpu_pool_workers if n_scenes > 1 else 1)
@@ -462,6 +537,7 @@ def run_ours(args):
                      "peak_source": "of measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "of fallback 6650 GB/s"},
         "phases_ms": {k: v * 1000.0 for k, v in zip(["bodies_bvh", "pairs_candidates", "contact_search", "dedup",
                                                      "contact_setup_solve", "integrate", "total"], phases)},
+        "serving": serving_rep,
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": int(launches),

@@ -259,6 +259,34 @@ int64_t rb_launch_count(void);
 int rb_step_noalloc(const rb_shapes* shapes, const rb_bodies* bodies, const rb_caps* caps, const rb_params* params,
                     const rb_outputs* out, void* stream);
 
+/* ---- continuous batching: re-laying out a resident batch between steps (no reference counterpart; the
+   reference steps one engine at a time) ---- */
+
+/* Derived topology arrays of `bodies` (body_v0, body_t0, body_c0, vert_body, tri_body, clu_body, written
+   through the struct's pointers) from bodies->shape and the shape table, on the device and on `stream`.
+   bodies->n_body_vertices / n_body_triangles / n_clusters must hold the totals (rb_topology_sizes) and the
+   arrays must have room for them; no owner entry is written past a declared total.  `scratch` is device
+   memory of at least RB_TOPOLOGY_SCRATCH_BYTES. */
+#define RB_TOPOLOGY_SCRATCH_BYTES 4096u
+int rb_build_topology(const rb_shapes* shapes, const rb_bodies* bodies, void* scratch, size_t scratch_bytes,
+                      void* stream);
+
+/* Device workspace bytes rb_repack needs for a warm-start cache of the given capacity. */
+int rb_repack_workspace_bytes(int32_t cache_capacity_old, size_t* bytes);
+
+/* Carries a batch's state into its next layout, on `stream`.  body_map[i] (device, n_old_bodies entries) is
+   the new index of old body i, or -1 when its scene leaves; the bodies that stay must keep their relative
+   order (new scenes are appended after them).  Rows x[7], u[6] of the staying bodies are copied from
+   x_old/u_old to x_new/u_new (distinct buffers); rows of new bodies are left for the caller to fill.  When
+   cache_key_old is not NULL the warm-start cache (rb_outputs.cache_*) is filtered to the staying scenes and
+   re-keyed with the new body indices into cache_*_new, keeping ascending key order; entries past
+   cache_capacity_new are dropped.  `workspace`: rb_repack_workspace_bytes(cache_capacity_old) bytes. */
+int rb_repack(const int32_t* body_map, int32_t n_old_bodies, const double* x_old, const double* u_old, double* x_new,
+              double* u_new, const int64_t* cache_key_old, const double* cache_sol_old,
+              const int32_t* cache_count_old, int32_t cache_capacity_old, int64_t* cache_key_new,
+              double* cache_sol_new, int32_t* cache_count_new, int32_t cache_capacity_new, void* workspace,
+              size_t workspace_bytes, void* stream);
+
 /* Signed distance grid of a closed triangle mesh (replaces grid3.py:320 create_signed_distance's call to
    igl.signed_distance at grid3.py:338): values[i + I*(j + J*k)] for nodes min + spacing*(i,j,k).
    Unsigned distance by closest point on each triangle, sign by the generalized winding number. */

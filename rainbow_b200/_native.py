@@ -23,8 +23,10 @@ SCHEME_RIGID_GS, SCHEME_GS, SCHEME_JACOBI, SCHEME_JACOBI_HYBRID, SCHEME_COLOURED
 TERMINATE_MERIT, TERMINATE_RESIDUAL, TERMINATE_RESIDUAL_FIXED_R = 0, 1, 2
 PRECISION_FP64, PRECISION_FP32_REFINE, PRECISION_FP32 = 0, 1, 2
 ORDER_SERIAL, ORDER_COLOURED = 0, 1
+RB_TOPOLOGY_SCRATCH_BYTES = 4096
 
 _vp = ctypes.c_void_p
+_sz = ctypes.c_size_t
 _i32 = ctypes.c_int32
 
 
@@ -94,6 +96,10 @@ SIGNATURES = {
     "rb_signed_distance_grid": (ctypes.c_int, [_vp, _i32, _vp, _i32, _vp, _vp, _vp]),
     "rb_profile_times": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), _i32]),
     "rb_launch_count": (ctypes.c_int64, []),
+    "rb_build_topology": (ctypes.c_int, [ctypes.POINTER(RbShapes), ctypes.POINTER(RbBodies), _vp, _sz, _vp]),
+    "rb_repack_workspace_bytes": (ctypes.c_int, [_i32, ctypes.POINTER(_sz)]),
+    "rb_repack": (ctypes.c_int, [_vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp, _vp, _vp, _i32, _vp, _sz,
+                                 _vp]),
     "rb_step_noalloc": (ctypes.c_int, [ctypes.POINTER(RbShapes), ctypes.POINTER(RbBodies), ctypes.POINTER(RbCaps),
                                        ctypes.POINTER(RbParams), ctypes.POINTER(RbOutputs), _vp]),
 }

@@ -5,8 +5,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SOURCES = ["csrc/rb_step.cu", "csrc/rb_sdf.cu"]
-HEADERS = ["csrc/rb_device.cuh", "csrc/rb_layout.h", "../include/rainbow_b200.h"]
+SOURCES = ["csrc/rb_step.cu", "csrc/rb_sdf.cu", "csrc/rb_batch.cu"]
+HEADERS = ["csrc/rb_device.cuh", "csrc/rb_layout.h", "csrc/rb_internal.h", "../include/rainbow_b200.h"]
 OUT = os.path.join(HERE, "lib", "librainbow_b200.so")
 
 NVCC_FLAGS = [

@@ -12,12 +12,7 @@
 
 #include "rainbow_b200.h"
 #include "rb_device.cuh"
-
-namespace rb {
-
-void note_launch();   // rb_step.cu: counts kernels launched by this library
-extern thread_local std::string g_error;
-}
+#include "rb_internal.h"
 
 namespace {
 

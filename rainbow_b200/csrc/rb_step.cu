@@ -31,6 +31,7 @@
 
 #include "rainbow_b200.h"
 #include "rb_device.cuh"
+#include "rb_internal.h"
 #include "rb_layout.h"
 
 namespace rb {
@@ -139,9 +140,8 @@ __global__ void k_scan_down(int32_t* __restrict__ data, const int32_t* n_dev, in
     }
     if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) data[n] = partial[gridDim.x];
 }
-static void scan(int32_t* data, const int32_t* n_dev, int n_host, int32_t* partial, int32_t* total_out,
-                 cudaStream_t st) {
-    const int G = 592;   // 4 x 148 SMs
+void scan(int32_t* data, const int32_t* n_dev, int n_host, int32_t* partial, int32_t* total_out, cudaStream_t st) {
+    const int G = kScanGrid;
     k_scan_reduce<<<G, 256, 0, st>>>(data, n_dev, n_host, partial); note_launch();
     k_scan_top<<<1, 1024, 0, st>>>(partial, G, total_out); note_launch();
     k_scan_down<<<G, 256, 0, st>>>(data, n_dev, n_host, partial); note_launch();

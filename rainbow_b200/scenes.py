@@ -172,10 +172,10 @@ def _shape_arrays(V, T, resolution, envelope, device):
                 inertia=np.asarray(inertia, np.float64), r=np.asarray(r, np.float64), q=np.asarray(q, np.float64))
 
 
-def batch_arrays(n_scenes=1024, seed=0, pool=64, body_range=(8, 256), resolution=32, device="cuda"):
+def batch_arrays(n_scenes=1024, seed=0, pool=64, body_range=(8, 256), resolution=32, device="cuda", ground=24.0):
     """``n_scenes`` independent scenes: body count log-uniform in body_range, random boxes (side U(0.5, 2))
     and spheres (radius U(0.25, 1), 16 x 16 sweep) with uniformly random orientations, density 1000, dropped
-    onto a fixed ground box; friction mu U(0.2, 0.8) per scene; dt 0.01.
+    onto a fixed ground box (ground x 1 x ground); friction mu U(0.2, 0.8) per scene; dt 0.01.
 
     Shape sizes are drawn from a pool of ``pool`` boxes and ``pool`` spheres shared by all scenes, so the
     signed distance grids are built once per pool entry.  Returns the list of per-scene arrays (sharing the
@@ -187,7 +187,7 @@ def batch_arrays(n_scenes=1024, seed=0, pool=64, body_range=(8, 256), resolution
     params.resolution = resolution
     params.max_iterations = 100
     params.relative_tolerance = 1e-6
-    shapes = [_shape_arrays(*GEO.create_box(24.0, 1.0, 24.0), resolution, params.envelope, device)]
+    shapes = [_shape_arrays(*GEO.create_box(ground, 1.0, ground), resolution, params.envelope, device)]
     kind = [2]
     for s in rng.uniform(0.5, 2.0, pool):
         shapes.append(_shape_arrays(*GEO.create_box(s, s, s), resolution, params.envelope, device))
@@ -203,7 +203,7 @@ def batch_arrays(n_scenes=1024, seed=0, pool=64, body_range=(8, 256), resolution
         "shape_t_off": np.concatenate([[0], np.cumsum([len(s["T"]) for s in shapes])]).astype(np.int64),
         "shape_g_off": np.concatenate([[0], np.cumsum([len(s["grid"]) for s in shapes])]).astype(np.int64),
         "shape_grid_meta": np.array([s["meta"] for s in shapes]),
-        "shape_key": np.array(["pool%d:%d" % (seed, k) for k in range(len(shapes))]),
+        "shape_key": np.array(["pool%d:%d:%d:%g:%d" % (seed, pool, resolution, ground, k) for k in range(len(shapes))]),
     }
     from .world import PARAM_FIELDS
     pvec = np.array([float(getattr(params, f)) for f in PARAM_FIELDS])
