@@ -157,10 +157,11 @@ typedef struct rb_params {
                                      (values below 1 mean every sweep); the other rules test every sweep */
     int32_t precision;            /* RB_PRECISION_*; the FP32 modes need RB_TERMINATE_RESIDUAL_FIXED_R and a
                                      Gauss-Seidel scheme */
-    int32_t refine_iterations;    /* RB_PRECISION_FP32_REFINE: FP64 sweeps reserved after the FP32 phase (at least 1,
-                                     at most max_iterations).  The FP32 phase sweeps until its residual meets the
+    int32_t refine_iterations;    /* RB_PRECISION_FP32_REFINE: FP64 sweeps reserved after the FP32 phase (0 to
+                                     max_iterations).  The FP32 phase sweeps until its residual meets the
                                      tolerance, stalls below 1e-4, or max_iterations - refine_iterations sweeps
-                                     are done; the FP64 refinement then gets the sweeps left of max_iterations */
+                                     are done; the FP64 refinement then gets the sweeps left of max_iterations.
+                                     The residual of the result is always evaluated in FP64 */
     int32_t warm_start;           /* nonzero: start each contact's impulse from the previous step's solution for
                                      the same (body pair, side, triangle) found in rb_outputs.cache_*; the
                                      reference always starts from zero (contacts.py:53), so this is off for

@@ -28,6 +28,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 #include "rainbow_b200.h"
 #include "rb_device.cuh"
@@ -1176,7 +1177,7 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
         w_is_wjt_x = true;
         shown = res0;
         if (g.rank() == 0) st->fp32_sweeps = sweeps32;
-        if (res0 <= a.pr.residual_tolerance || a.pr.precision == RB_PRECISION_FP32) {
+        if (res0 <= a.pr.residual_tolerance || a.pr.precision == RB_PRECISION_FP32 || sweeps32 >= max_it) {
             for (int i = 4 * R.c0 + g.rank(); i < 4 * R.c1; i += g.size()) sol[i] = x[i];
             g.sync();
             const bool ok = res0 <= a.pr.residual_tolerance;
@@ -1189,7 +1190,7 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
             g.sync();
             return;
         }
-        loop_max = max(max_it - sweeps32, 1);   // the sweeps the FP32 phase left over
+        loop_max = max_it - sweeps32;   // the sweeps the FP32 phase left over
     }
     for (int it = 0; it < loop_max; ++it) {
         if (!w_is_wjt_x) scene_wjt(a, g, R, x, w);   // every sweep starts from w = WJT x (contacts.py:72)
@@ -1290,48 +1291,56 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
 }
 
 // ---------------------------------------------------------------------------------------------------------
-// FP32 phase of the FP32 precision modes: the scene's whole contact problem is copied into shared memory as
-// FP32 (J and WJT blocks, b, r, 1/diag, x, mu, body indices, the level order) and swept there, level by
-// level, with the fixed-r rule until the FP32 residual meets the tolerance or stops improving.  The FP64
-// solver then tests the iterate in FP64 and refines it.  Body accumulators are rebuilt from x at every
-// residual test (in the order of each body's contact list, so results are deterministic).
+// FP32 phase of the FP32 precision modes.  A scene's whole contact problem is copied into shared memory as
+// FP32 in a compact form and swept there, level by level (or colour by colour), with the fixed-r rule until
+// the FP32 residual meets the tolerance, stalls near FP32 rounding, or the sweep budget is spent; the FP64
+// solver then tests the iterate in FP64 and refines it with the sweeps left.
+//
+// Compact form.  A contact's Jacobian rows are [lin_lo | ang_lo | lin_hi | ang_hi] with lin_hi = -lin_lo
+// (the frame direction, zero on the torsion row) and W J^T = (m^-1 lin, I_w^-1 ang) per body, so a contact
+// stores per row q: lin_lo (3), ang_lo (3), ang_hi (3), b, 1/diag and x -- 12 floats, 48 per contact
+// (192 bytes; the torsion row's unused lin slot holds mu) -- and a body stores its accumulator w (6), m^-1,
+// a fixed flag and the world inverse inertia (6, symmetric): 16 floats.  The update of w after a contact
+// changes by dx is m^-1 sum_q lin_q dx_q (negated on the hi side) and I^-1 sum_q ang_q dx_q.
+//
+// Execution.  Four lanes share a contact (lane q computes row q's J w; the four z values meet by shuffles;
+// every lane applies the prox; the three sums of the update are reduced over the quad and each lane writes
+// one of the four 3-vectors).  A team -- one warp for scenes of up to kS32WarpSlab bytes, a 128-thread block
+// above -- takes scenes from a queue and synchronises between levels.  Three launches cover three size
+// classes (warp teams with small and large slabs, block teams) and run concurrently on separate streams.
 // ---------------------------------------------------------------------------------------------------------
-struct F32Scene {
-    float *J, *W, *b, *r, *dinv, *x, *mu, *w;
-    int16_t *lo, *hi;
-    uint16_t *order, *lptr;
-    uint8_t* fixed;
+constexpr int kS32Floats = 48;                       // floats per contact
+constexpr int kQueueFp32 = 5;                        // counters[5..7]: scene queues of the three size classes
+constexpr int kS32BodyFloats = 16;                   // floats per body
+constexpr int kFp32Block = 128;                      // threads per block of every FP32 launch
+constexpr int kFp32LargeSmem = 224 * 1024;           // slab of a block team (one scene per SM)
+constexpr int kS32SmallSlab = 28 * 1024;             // slab of a warp team, small class (8 scenes per SM)
+constexpr int kS32MidSlab = 56 * 1024;               // slab of a warp team, mid class (4 scenes per SM)
+// relative residual below which a stalled FP32 iteration is taken to have met FP32 rounding
+constexpr float kFp32Floor = 1e-4f;
+
+struct S32Scene {
+    float* c;          // kS32Floats per contact (row q at 12 q: lin[3], ang_lo[3], ang_hi[3], b, 1/diag, x)
+    float* body;       // kS32BodyFloats per body: w[6], m^-1, fixed, I^-1 (xx, xy, xz, yy, yz, zz), pad[2]
+    int16_t* lohi;     // scene-local body indices, 2 per contact
+    uint16_t* order;   // contacts by level
+    uint16_t* lptr;    // level starts (L + 1)
 };
-__host__ __device__ inline size_t f32_align(size_t v) { return (v + 15) & ~size_t(15); }
-__host__ __device__ inline size_t f32_bytes(int K, int nb) {
-    size_t o = 0;
-    o += f32_align(sizeof(float) * (size_t)K * 48) * 2;             // J, W
-    o += f32_align(sizeof(float) * (size_t)K * 4) * 4;              // b, r, dinv, x
-    o += f32_align(sizeof(float) * (size_t)K);                      // mu
-    o += f32_align(sizeof(float) * (size_t)nb * 6);                 // w
-    o += f32_align(sizeof(int16_t) * (size_t)K) * 2;                // lo, hi
-    o += f32_align(sizeof(uint16_t) * (size_t)K);                   // order
-    o += f32_align(sizeof(uint16_t) * (size_t)(K + 1));             // lptr
-    o += f32_align((size_t)nb);                                     // fixed
-    return o;
+__host__ __device__ inline size_t s32_align(size_t v) { return (v + 15) & ~size_t(15); }
+__host__ __device__ inline size_t s32_bytes(int K, int nb) {
+    return s32_align(sizeof(float) * (size_t)K * kS32Floats) + s32_align(sizeof(float) * (size_t)nb * kS32BodyFloats) +
+           s32_align(sizeof(int16_t) * 2 * (size_t)K) + s32_align(sizeof(uint16_t) * (size_t)K) +
+           s32_align(sizeof(uint16_t) * (size_t)(K + 1));
 }
-__device__ inline F32Scene f32_carve(char* base, int K, int nb) {
-    F32Scene f;
+__device__ inline S32Scene s32_carve(char* base, int K, int nb) {
+    S32Scene f;
     size_t o = 0;
-    auto take = [&](size_t bytes) { char* p = base + o; o += f32_align(bytes); return p; };
-    f.J = (float*)take(sizeof(float) * (size_t)K * 48);
-    f.W = (float*)take(sizeof(float) * (size_t)K * 48);
-    f.b = (float*)take(sizeof(float) * (size_t)K * 4);
-    f.r = (float*)take(sizeof(float) * (size_t)K * 4);
-    f.dinv = (float*)take(sizeof(float) * (size_t)K * 4);
-    f.x = (float*)take(sizeof(float) * (size_t)K * 4);
-    f.mu = (float*)take(sizeof(float) * (size_t)K);
-    f.w = (float*)take(sizeof(float) * (size_t)nb * 6);
-    f.lo = (int16_t*)take(sizeof(int16_t) * (size_t)K);
-    f.hi = (int16_t*)take(sizeof(int16_t) * (size_t)K);
+    auto take = [&](size_t bytes) { char* p = base + o; o += s32_align(bytes); return p; };
+    f.c = (float*)take(sizeof(float) * (size_t)K * kS32Floats);
+    f.body = (float*)take(sizeof(float) * (size_t)nb * kS32BodyFloats);
+    f.lohi = (int16_t*)take(sizeof(int16_t) * 2 * (size_t)K);
     f.order = (uint16_t*)take(sizeof(uint16_t) * (size_t)K);
     f.lptr = (uint16_t*)take(sizeof(uint16_t) * (size_t)(K + 1));
-    f.fixed = (uint8_t*)take((size_t)nb);
     return f;
 }
 
@@ -1344,54 +1353,125 @@ __device__ __forceinline__ void f32_prox(float zs, float zt, float ztau, float m
     o[0] = zs * scale; o[1] = zt * scale; o[2] = ztau * scale;
 }
 
-// w = WJT x from the shared copies (each body sums its contacts in ascending order)
-__device__ void f32_wjt(const StepArgs& a, const SceneRange& R, const F32Scene& f) {
-    const int nb = R.b1 - R.b0;
-    for (int bl = threadIdx.x; bl < nb; bl += blockDim.x) {
-        float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        if (!f.fixed[bl]) {
+// y = I^-1 t with I^-1 stored symmetric (xx, xy, xz, yy, yz, zz)
+__device__ __forceinline__ void s32_sym3(const float* I, const float* t, float* y) {
+    y[0] = fmaf(I[0], t[0], fmaf(I[1], t[1], I[2] * t[2]));
+    y[1] = fmaf(I[1], t[0], fmaf(I[3], t[1], I[4] * t[2]));
+    y[2] = fmaf(I[2], t[0], fmaf(I[4], t[1], I[5] * t[2]));
+}
+
+// J_q . [w_lo; w_hi] of row q (the torsion row has no linear part)
+__device__ __forceinline__ float s32_jw(const float* row, int q, const float* wl, const float* wh) {
+    float s = row[3] * wl[3];
+    s = fmaf(row[4], wl[4], s);
+    s = fmaf(row[5], wl[5], s);
+    s = fmaf(row[6], wh[3], s);
+    s = fmaf(row[7], wh[4], s);
+    s = fmaf(row[8], wh[5], s);
+    if (q < 3) {
+        s = fmaf(row[0], wl[0] - wh[0], s);
+        s = fmaf(row[1], wl[1] - wh[1], s);
+        s = fmaf(row[2], wl[2] - wh[2], s);
+    }
+    return s;
+}
+
+// copy scene R into the team's slab as FP32; returns the number of levels
+template <class G>
+__device__ int s32_load(const StepArgs& a, const G& g, const SceneRange& R, int s, const S32Scene& f, bool coloured) {
+    const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
+    const int L = coloured ? scene_colours(a, g, R, s) : scene_levels(a, g, R, s);
+    for (int i = g.rank(); i < 16 * K; i += g.size()) {   // (contact, row, part) with part 0: J lin+ang, 1: rest
+        const int kl = i >> 4, q = (i >> 2) & 3, part = i & 3;
+        const size_t k = (size_t)R.c0 + kl;
+        float* row = f.c + kS32Floats * kl + 12 * q;
+        const double* J = a.ws.J + 48 * k + 12 * q;
+        if (part == 0) {
+            row[0] = q < 3 ? (float)J[0] : (float)a.ws.mu[k];
+            row[1] = (float)J[1];
+            row[2] = (float)J[2];
+        } else if (part == 1) {
+            row[3] = (float)J[3]; row[4] = (float)J[4]; row[5] = (float)J[5];
+        } else if (part == 2) {
+            row[6] = (float)J[9]; row[7] = (float)J[10]; row[8] = (float)J[11];
+        } else {
+            row[9] = (float)a.ws.b[4 * k + q];
+            row[10] = (float)(1.0 / a.ws.diag[4 * k + q]);
+            row[11] = (float)a.ws.x[4 * k + q];
+        }
+    }
+    for (int kl = g.rank(); kl < K; kl += g.size()) {
+        const int k = R.c0 + kl;
+        f.lohi[2 * kl] = (int16_t)(a.ws.lohi[2 * k] - R.b0);
+        f.lohi[2 * kl + 1] = (int16_t)(a.ws.lohi[2 * k + 1] - R.b0);
+        f.order[kl] = (uint16_t)(a.ws.lev_order[R.c0 + kl] - R.c0);
+    }
+    for (int l = g.rank(); l <= L; l += g.size()) f.lptr[l] = (uint16_t)a.ws.lev_ptr[R.c0 + s + l];
+    for (int bl = g.rank(); bl < nb; bl += g.size()) {
+        const int b = R.b0 + bl;
+        float* B = f.body + kS32BodyFloats * bl;
+        const bool fx = a.bd.fixed[b] != 0;
+        const double* Wi = a.ws.Winv + 9 * (size_t)b;
+        B[6] = fx ? 0.0f : (float)(1.0 / a.bd.mass[b]);
+        B[7] = fx ? 1.0f : 0.0f;
+        B[8] = (float)Wi[0]; B[9] = (float)Wi[1]; B[10] = (float)Wi[2];
+        B[11] = (float)Wi[4]; B[12] = (float)Wi[5]; B[13] = (float)Wi[8];
+    }
+    g.sync();
+    return L;
+}
+
+// w = W J^T x (each body sums its contacts in ascending order), then the FP32 residual
+// ||x - prox(x - D^-1 (A x + b))||_inf / max(1, ||x||_inf)
+template <class G>
+__device__ float s32_residual(const StepArgs& a, const G& g, const SceneRange& R, const S32Scene& f) {
+    const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
+    for (int bl = g.rank(); bl < nb; bl += g.size()) {
+        float* B = f.body + kS32BodyFloats * bl;
+        float P[3] = {0.f, 0.f, 0.f}, T[3] = {0.f, 0.f, 0.f};
+        if (B[7] == 0.0f) {
             const int b = R.b0 + bl;
             for (int e = a.ws.bc_ptr[b]; e < a.ws.bc_ptr[b + 1]; ++e) {
                 const int code = a.ws.bc_list[e];
                 const int kl = (code >> 1) - R.c0, side = code & 1;
-                const float* Wk = f.W + 48 * kl + 6 * side;
-                const float* xk = f.x + 4 * kl;
-                for (int d = 0; d < 6; ++d)
-                    acc[d] = fmaf(Wk[36 + d], xk[3], fmaf(Wk[24 + d], xk[2], fmaf(Wk[12 + d], xk[1], fmaf(Wk[d], xk[0], acc[d]))));
+                const float* c = f.c + kS32Floats * kl;
+                for (int q = 0; q < 4; ++q) {
+                    const float* row = c + 12 * q;
+                    const float xq = row[11];
+                    if (q < 3) {
+                        const float sx = side ? -xq : xq;
+                        P[0] = fmaf(row[0], sx, P[0]); P[1] = fmaf(row[1], sx, P[1]); P[2] = fmaf(row[2], sx, P[2]);
+                    }
+                    const float* ang = row + (side ? 6 : 3);
+                    T[0] = fmaf(ang[0], xq, T[0]); T[1] = fmaf(ang[1], xq, T[1]); T[2] = fmaf(ang[2], xq, T[2]);
+                }
             }
         }
-        for (int d = 0; d < 6; ++d) f.w[6 * bl + d] = acc[d];
+        float om[3];
+        s32_sym3(B + 8, T, om);
+        B[0] = B[6] * P[0]; B[1] = B[6] * P[1]; B[2] = B[6] * P[2];
+        B[3] = om[0]; B[4] = om[1]; B[5] = om[2];
     }
-    __syncthreads();
-}
-
-__device__ __forceinline__ float f32_jw(const float* Jr, const float* wlo, const float* whi) {
-    float s = 0.0f;
-    for (int c = 0; c < 6; ++c) s = fmaf(Jr[c], wlo[c], s);
-    for (int c = 0; c < 6; ++c) s = fmaf(Jr[6 + c], whi[c], s);
-    return s;
-}
-
-// FP32 residual ||x - prox(x - D^-1 (A x + b))||_inf / max(1, ||x||_inf); rebuilds w first
-__device__ float f32_residual(const StepArgs& a, const SceneRange& R, const F32Scene& f, const BlockGroup& g) {
-    f32_wjt(a, R, f);
-    const int K = R.c1 - R.c0;
+    g.sync();
     float m = 0.0f, xm = 0.0f;
-    for (int kl = threadIdx.x; kl < K; kl += blockDim.x) {
-        const float* J = f.J + 48 * kl;
-        const float* wlo = f.w + 6 * f.lo[kl];
-        const float* whi = f.w + 6 * f.hi[kl];
-        float z[4];
-        for (int row = 0; row < 4; ++row)
-            z[row] = f.x[4 * kl + row] - f.dinv[4 * kl + row] * (f32_jw(J + 12 * row, wlo, whi) + f.b[4 * kl + row]);
+    for (int kl = g.rank(); kl < K; kl += g.size()) {
+        const float* c = f.c + kS32Floats * kl;
+        const float* wl = f.body + kS32BodyFloats * f.lohi[2 * kl];
+        const float* wh = f.body + kS32BodyFloats * f.lohi[2 * kl + 1];
+        float z[4], x[4];
+        for (int q = 0; q < 4; ++q) {
+            const float* row = c + 12 * q;
+            x[q] = row[11];
+            z[q] = x[q] - row[10] * (s32_jw(row, q, wl, wh) + row[9]);
+        }
         const float pn = fmaxf(z[0], 0.0f);
         float fr[3];
-        f32_prox(z[1], z[2], z[3], f.mu[kl], pn, fr);
-        const float d[4] = {f.x[4 * kl] - pn, f.x[4 * kl + 1] - fr[0], f.x[4 * kl + 2] - fr[1], f.x[4 * kl + 3] - fr[2]};
+        f32_prox(z[1], z[2], z[3], c[36], pn, fr);
+        const float d[4] = {x[0] - pn, x[1] - fr[0], x[2] - fr[1], x[3] - fr[2]};
         for (int i = 0; i < 4; ++i) {
             m = fmaxf(m, fabsf(d[i]));
             if (d[i] != d[i]) m = d[i];
-            xm = fmaxf(xm, fabsf(f.x[4 * kl + i]));
+            xm = fmaxf(xm, fabsf(x[i]));
         }
     }
     const double mres = g.max((double)m);
@@ -1399,99 +1479,126 @@ __device__ float f32_residual(const StepArgs& a, const SceneRange& R, const F32S
     return (float)(mres / (mx > 1.0 ? mx : 1.0));
 }
 
-constexpr int kFp32Block = 128;
-constexpr int kFp32LargeSmem = 200 * 1024;   // shared memory of the one-scene-per-SM FP32 solve
-// relative residual below which a stalled FP32 iteration is taken to have met FP32 rounding
-constexpr float kFp32Floor = 1e-4f;
+// one Gauss-Seidel sweep over the levels, four lanes per contact
+template <class G>
+__device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, float rscale) {
+    const int q = g.rank() & 3, slot = g.rank() >> 2, nslot = g.size() >> 2;
+    const int lane = threadIdx.x & 31, base = lane & ~3;
+    for (int l = 1; l <= L; ++l) {
+        const int start = f.lptr[l - 1], end = f.lptr[l];
+        // every lane of a quad runs the same trip count, so the quad's shuffles see all four lanes
+        for (int i0 = start; i0 < end; i0 += nslot) {
+            const int i = i0 + slot;
+            const bool on = i < end;
+            if (on) {
+                const unsigned qm = 0xfu << base;   // the quad's lanes share `on`
+                const int kl = f.order[i];
+                const int lo = f.lohi[2 * kl], hi = f.lohi[2 * kl + 1];
+                float* row = f.c + kS32Floats * kl + 12 * q;
+                float* Bl = f.body + kS32BodyFloats * lo;
+                float* Bh = f.body + kS32BodyFloats * hi;
+                const float xo = row[11];
+                const float z = xo - rscale * row[10] * (s32_jw(row, q, Bl, Bh) + row[9]);
+                float zz[4];
+                for (int j = 0; j < 4; ++j) zz[j] = __shfl_sync(qm, z, base | j);
+                const float mu = __shfl_sync(qm, row[0], base | 3);
+                const float xn = fmaxf(zz[0], 0.0f);
+                float fr[3];
+                f32_prox(zz[1], zz[2], zz[3], mu, xn, fr);
+                const float xq = q == 0 ? xn : (q == 1 ? fr[0] : (q == 2 ? fr[1] : fr[2]));
+                row[11] = xq;
+                const float dq = xq - xo;
+                // quad sums: P = sum_q lin_q dx_q, Tl = sum_q ang_lo_q dx_q, Th = sum_q ang_hi_q dx_q
+                float v[9];
+                for (int j = 0; j < 3; ++j) v[j] = q < 3 ? row[j] * dq : 0.0f;
+                for (int j = 0; j < 3; ++j) v[3 + j] = row[3 + j] * dq;
+                for (int j = 0; j < 3; ++j) v[6 + j] = row[6 + j] * dq;
+                for (int j = 0; j < 9; ++j) {
+                    v[j] += __shfl_xor_sync(qm, v[j], 1);
+                    v[j] += __shfl_xor_sync(qm, v[j], 2);
+                }
+                float* B = (q & 1) ? Bh : Bl;
+                if (B[7] == 0.0f) {
+                    if (q < 2) {          // linear: +m^-1 P on lo, -m^-1 P on hi
+                        const float sm = q ? -B[6] : B[6];
+                        B[0] = fmaf(sm, v[0], B[0]); B[1] = fmaf(sm, v[1], B[1]); B[2] = fmaf(sm, v[2], B[2]);
+                    } else {              // angular: I^-1 T
+                        const float t[3] = {q == 2 ? v[3] : v[6], q == 2 ? v[4] : v[7], q == 2 ? v[5] : v[8]};
+                        float om[3];
+                        s32_sym3(B + 8, t, om);
+                        B[3] += om[0]; B[4] += om[1]; B[5] += om[2];
+                    }
+                }
+            }
+        }
+        g.sync();
+    }
+}
 
-// scenes whose FP32 copy takes lo_bytes < bytes <= hi_bytes of shared memory
-__global__ void __launch_bounds__(kFp32Block) k_solve_fp32(const StepArgs a, size_t lo_bytes, size_t hi_bytes) {
+template <class G>
+__device__ __forceinline__ int team_next(const G& g, int* counter, int* slot) {
+    int s = 0;
+    if (g.rank() == 0) s = atomicAdd(counter, 1);
+    if (g.size() == 32) return __shfl_sync(0xffffffffu, s, 0);
+    if (g.rank() == 0) *slot = s;
+    __syncthreads();
+    s = *slot;
+    __syncthreads();
+    return s;
+}
+
+// FP32 phase for the scenes whose compact copy takes lo_bytes < bytes <= slab bytes; G = WarpGroup gives
+// every warp of the block its own slab and scene, G = BlockGroup one slab and scene per block
+template <class G>
+__global__ void __launch_bounds__(kFp32Block) k_solve_fp32(const StepArgs a, int queue, size_t lo_bytes, size_t slab) {
     extern __shared__ __align__(16) char f32_smem[];
     __shared__ double red[33];
     __shared__ int ired[33];
+    __shared__ int next_slot;
     if (a.ws.counters[kAbort]) return;
-    const BlockGroup g = {red, ired};
+    G g;
+    constexpr bool block_team = std::is_same_v<G, BlockGroup>;
+    if constexpr (block_team) { g.red = red; g.ired = ired; }
+    const int team = block_team ? 0 : (int)(threadIdx.x >> 5);
+    char* my_slab = f32_smem + (size_t)team * slab;
     const int max_it = a.pr.max_iterations;
     const int interval = a.pr.residual_interval > 1 ? a.pr.residual_interval : 1;
     const float tol = (float)a.pr.residual_tolerance;
-    // sweeps left to the FP64 refinement; the two phases together make at most max_iterations sweeps
-    const int reserve = a.pr.precision == RB_PRECISION_FP32_REFINE
-                      ? min(max(a.pr.refine_iterations, 1), max_it) : 0;
+    // sweeps reserved for the FP64 refinement
+    const int reserve = a.pr.precision == RB_PRECISION_FP32_REFINE ? min(max(a.pr.refine_iterations, 0), max_it) : 0;
     const int budget = max_it - reserve;
-    for (int s = blockIdx.x; s < a.bd.n_scenes; s += gridDim.x) {
+    double rs = a.pr.scheme == RB_SCHEME_RIGID_GS ? 1.0 : 0.1;   // the r of the scheme: r = rs / diag
+    if (a.pr.relaxation > 0.0) rs *= a.pr.relaxation;
+    const float rscale = (float)rs;
+    const bool coloured = a.pr.scheme == RB_SCHEME_COLOURED_GS || a.pr.ordering == RB_ORDER_COLOURED;
+    for (;;) {
+        const int s = team_next(g, a.ws.counters + queue, &next_slot);
+        if (s >= a.bd.n_scenes) break;
         const SceneRange R = scene_range(a, s);
         const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
-        if (K == 0 || K > 65535) continue;
-        const size_t bytes = f32_bytes(K, nb);
-        if (bytes <= lo_bytes || bytes > hi_bytes) continue;
-        const bool coloured = a.pr.scheme == RB_SCHEME_COLOURED_GS || a.pr.ordering == RB_ORDER_COLOURED;
-        const int L = coloured ? scene_colours(a, g, R, s) : scene_levels(a, g, R, s);
-        const F32Scene f = f32_carve(f32_smem, K, nb);
-        for (int i = threadIdx.x; i < 48 * K; i += blockDim.x) {
-            f.J[i] = (float)a.ws.J[48 * (size_t)R.c0 + i];
-            f.W[i] = (float)a.ws.WJT[48 * (size_t)R.c0 + i];
-        }
-        for (int i = threadIdx.x; i < 4 * K; i += blockDim.x) {
-            const size_t gi = 4 * (size_t)R.c0 + i;
-            f.b[i] = (float)a.ws.b[gi];
-            f.r[i] = (float)a.ws.r[gi];
-            f.dinv[i] = (float)(1.0 / a.ws.diag[gi]);
-            f.x[i] = (float)a.ws.x[gi];
-        }
-        for (int kl = threadIdx.x; kl < K; kl += blockDim.x) {
-            const int k = R.c0 + kl;
-            f.mu[kl] = (float)a.ws.mu[k];
-            f.lo[kl] = (int16_t)(a.ws.lohi[2 * k] - R.b0);
-            f.hi[kl] = (int16_t)(a.ws.lohi[2 * k + 1] - R.b0);
-            f.order[kl] = (uint16_t)(a.ws.lev_order[R.c0 + kl] - R.c0);
-        }
-        for (int l = threadIdx.x; l <= L; l += blockDim.x) f.lptr[l] = (uint16_t)a.ws.lev_ptr[R.c0 + s + l];
-        for (int bl = threadIdx.x; bl < nb; bl += blockDim.x) f.fixed[bl] = a.bd.fixed[R.b0 + bl];
-        __syncthreads();
-        float res = f32_residual(a, R, f, g);   // the warm-started iterate may already be good enough
+        if (K == 0 || K > 65535 || nb > 32767) continue;
+        const size_t bytes = s32_bytes(K, nb);
+        if (bytes <= lo_bytes || bytes > slab) continue;
+        const S32Scene f = s32_carve(my_slab, K, nb);
+        const int L = s32_load(a, g, R, s, f, coloured);
+        float res = s32_residual(a, g, R, f);   // the warm-started iterate may already be good enough
         float best = res;
         int sweeps = 0, stalls = 0;
         while (res > tol && sweeps < budget) {
-            for (int l = 1; l <= L; ++l) {
-                for (int i = f.lptr[l - 1] + threadIdx.x; i < f.lptr[l]; i += blockDim.x) {
-                    const int kl = f.order[i];
-                    const int lo = f.lo[kl], hi = f.hi[kl];
-                    const float* J = f.J + 48 * kl;
-                    float* wlo = f.w + 6 * lo;
-                    float* whi = f.w + 6 * hi;
-                    float xo[4], z[4];
-                    for (int row = 0; row < 4; ++row) {
-                        xo[row] = f.x[4 * kl + row];
-                        z[row] = xo[row] - f.r[4 * kl + row] * (f32_jw(J + 12 * row, wlo, whi) + f.b[4 * kl + row]);
-                    }
-                    const float xn = fmaxf(z[0], 0.0f);
-                    float fr[3];
-                    f32_prox(z[1], z[2], z[3], f.mu[kl], xn, fr);
-                    const float d[4] = {xn - xo[0], fr[0] - xo[1], fr[1] - xo[2], fr[2] - xo[3]};
-                    f.x[4 * kl] = xn; f.x[4 * kl + 1] = fr[0]; f.x[4 * kl + 2] = fr[1]; f.x[4 * kl + 3] = fr[2];
-                    const float* Wk = f.W + 48 * kl;
-                    for (int side = 0; side < 2; ++side) {
-                        if (f.fixed[side ? hi : lo]) continue;
-                        float* wb = side ? whi : wlo;
-                        const float* Ws = Wk + 6 * side;
-                        for (int dd = 0; dd < 6; ++dd)
-                            wb[dd] += fmaf(Ws[36 + dd], d[3], fmaf(Ws[24 + dd], d[2], fmaf(Ws[12 + dd], d[1], Ws[dd] * d[0])));
-                    }
-                }
-                __syncthreads();
-            }
+            s32_sweep(g, f, L, rscale);
             ++sweeps;
             if (sweeps % interval == 0 || sweeps == budget) {
-                res = f32_residual(a, R, f, g);
+                res = s32_residual(a, g, R, f);
                 // FP32 floor: hand over to FP64 once the residual, already small, stops improving.  Above
                 // the floor a pause is the Gauss-Seidel iteration itself (it is not monotone), so go on.
                 if (res < 0.95f * best) { best = res; stalls = 0; }
                 else if (best < kFp32Floor && ++stalls >= 3) break;
             }
         }
-        for (int i = threadIdx.x; i < 4 * K; i += blockDim.x) a.ws.x[4 * (size_t)R.c0 + i] = (double)f.x[i];
-        if (threadIdx.x == 0) a.ws.sweeps32[s] = sweeps;
-        __syncthreads();
+        for (int i = g.rank(); i < 4 * K; i += g.size())
+            a.ws.x[4 * (size_t)R.c0 + i] = (double)f.c[kS32Floats * (i >> 2) + 12 * (i & 3) + 11];
+        if (g.rank() == 0) a.ws.sweeps32[s] = sweeps;
+        g.sync();
     }
 }
 
@@ -1753,9 +1860,36 @@ int ensure_kernel_attributes() {
     const int block_max = 6 * (int)sizeof(double) * kSolveSmemBodies;
     e = cudaFuncSetAttribute(k_solve_warps, cudaFuncAttributeMaxDynamicSharedMemorySize, warp_max);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_solve_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, block_max);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_solve_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, kFp32LargeSmem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_solve_fp32<WarpGroup>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFp32LargeSmem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_solve_fp32<BlockGroup>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFp32LargeSmem);
     if (e != cudaSuccess) return fail(RB_ERR_CUDA, std::string("rb_step: cudaFuncSetAttribute: ") + cudaGetErrorString(e));
     g_attr_done[dev] = true;
+    return RB_OK;
+}
+
+// Side streams of the FP32 size classes, per host thread and device, made on the thread's first step on
+// the device (an uncaptured call).  Each step forks them from its stream with an event and joins them back,
+// which a stream capture records as parallel branches.
+struct SideStreams {
+    cudaStream_t s[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
+};
+thread_local SideStreams g_side[64];
+int side_streams(SideStreams** out) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return fail(RB_ERR_CUDA, "rb_step: no current device");
+    SideStreams& ss = g_side[dev];
+    if (!ss.fork) {
+        cudaError_t e = cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming);
+        for (int c = 0; c < 3 && e == cudaSuccess; ++c) {
+            e = cudaStreamCreateWithFlags(&ss.s[c], cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ss.join[c], cudaEventDisableTiming);
+        }
+        if (e != cudaSuccess) return fail(RB_ERR_CUDA, std::string("rb_step: side streams: ") + cudaGetErrorString(e));
+    }
+    *out = &ss;
     return RB_OK;
 }
 }  // namespace
@@ -1852,10 +1986,23 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     const int bg = bd->n_scenes < 148 * 16 ? bd->n_scenes : 148 * 16;
     k_sweeps32_init<<<blocks_for(bd->n_scenes, 256), 256, 0, st>>>(a); note_launch();
     if (pr->precision != RB_PRECISION_FP64) {
-        // FP32 phase in shared memory: small scenes several per SM, larger ones one per SM
-        const size_t small = 48 * 1024 - 1024, large = kFp32LargeSmem;
-        k_solve_fp32<<<bg, kFp32Block, small, st>>>(a, 0, small); note_launch();
-        k_solve_fp32<<<148, kFp32Block, large, st>>>(a, small, large); note_launch();
+        // FP32 phase in shared memory, three size classes side by side: warp teams with 28 KB slabs (8 scenes
+        // per SM), warp teams with 56 KB slabs (4 per SM), block teams with 224 KB (1 per SM)
+        SideStreams* ss = nullptr;
+        rc = side_streams(&ss);
+        if (rc != RB_OK) return rc;
+        cudaEventRecord(ss->fork, st);
+        for (int c = 0; c < 3; ++c) cudaStreamWaitEvent(ss->s[c], ss->fork, 0);
+        k_solve_fp32<WarpGroup><<<2 * 148, kFp32Block, 4 * (size_t)kS32SmallSlab, ss->s[0]>>>(
+            a, kQueueFp32, 0, kS32SmallSlab); note_launch();
+        k_solve_fp32<WarpGroup><<<148, kFp32Block, 4 * (size_t)kS32MidSlab, ss->s[1]>>>(
+            a, kQueueFp32 + 1, kS32SmallSlab, kS32MidSlab); note_launch();
+        k_solve_fp32<BlockGroup><<<148, kFp32Block, (size_t)kFp32LargeSmem, ss->s[2]>>>(
+            a, kQueueFp32 + 2, kS32MidSlab, kFp32LargeSmem); note_launch();
+        for (int c = 0; c < 3; ++c) {
+            cudaEventRecord(ss->join[c], ss->s[c]);
+            cudaStreamWaitEvent(st, ss->join[c], 0);
+        }
     }
     if (warp_bodies > 0) { k_solve_warps<<<wg, 32 * kSolveWarpsPerBlock, warp_smem, st>>>(a, 0, warp_bodies); note_launch(); }
     k_solve_blocks<<<bg, kSolveBlock, block_smem, st>>>(a, 0, warp_bodies, smem_bodies); note_launch();

@@ -35,7 +35,7 @@ def params_from_vector(vec):
 
 def make_rb_params(p, dt=None, scheme="rigid_gauss_seidel", termination="merit", residual_tolerance=1e-6,
                    profiling=False, warm_start=False, residual_interval=1, relaxation=1.0, precision="fp64",
-                   refine_iterations=20, ordering="serial"):
+                   refine_iterations=0, ordering="serial"):
     """rb_params from a Parameters-like mapping (types.py:356 field names).
 
     ordering="coloured" sweeps the Gauss-Seidel schemes colour by colour (the scheme
