@@ -1310,9 +1310,10 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
 // classes (warp teams with small and large slabs, block teams) and run concurrently on separate streams.
 // ---------------------------------------------------------------------------------------------------------
 constexpr int kS32Floats = 48;                       // floats per contact
-constexpr int kQueueFp32 = 5;                        // counters[5..7]: scene queues of the three size classes
+constexpr int kQueueFp32 = 5;                        // counters[5..8]: scene queues of the four size classes
 constexpr int kS32BodyFloats = 16;                   // floats per body
-constexpr int kFp32Block = 128;                      // threads per block of every FP32 launch
+constexpr int kFp32Block = 128;                      // threads per block of the FP32 launches
+constexpr int kFp32BlockMax = 256;                   // ... and of the launch for scenes beyond any slab
 constexpr int kFp32LargeSmem = 224 * 1024;           // slab of a block team (one scene per SM)
 constexpr int kS32SmallSlab = 28 * 1024;             // slab of a warp team, small class (8 scenes per SM)
 constexpr int kS32MidSlab = 56 * 1024;               // slab of a warp team, mid class (4 scenes per SM)
@@ -1327,16 +1328,18 @@ struct S32Scene {
     uint16_t* lptr;    // level starts (L + 1)
 };
 __host__ __device__ inline size_t s32_align(size_t v) { return (v + 15) & ~size_t(15); }
-__host__ __device__ inline size_t s32_bytes(int K, int nb) {
-    return s32_align(sizeof(float) * (size_t)K * kS32Floats) + s32_align(sizeof(float) * (size_t)nb * kS32BodyFloats) +
+// shared memory of a scene's FP32 copy; with contacts_in_l2 the contact rows live in global memory (L2)
+__host__ __device__ inline size_t s32_bytes(int K, int nb, bool contacts_in_l2 = false) {
+    return (contacts_in_l2 ? 0 : s32_align(sizeof(float) * (size_t)K * kS32Floats)) +
+           s32_align(sizeof(float) * (size_t)nb * kS32BodyFloats) +
            s32_align(sizeof(int16_t) * 2 * (size_t)K) + s32_align(sizeof(uint16_t) * (size_t)K) +
            s32_align(sizeof(uint16_t) * (size_t)(K + 1));
 }
-__device__ inline S32Scene s32_carve(char* base, int K, int nb) {
+__device__ inline S32Scene s32_carve(char* base, int K, int nb, float* c_global = nullptr) {
     S32Scene f;
     size_t o = 0;
     auto take = [&](size_t bytes) { char* p = base + o; o += s32_align(bytes); return p; };
-    f.c = (float*)take(sizeof(float) * (size_t)K * kS32Floats);
+    f.c = c_global ? c_global : (float*)take(sizeof(float) * (size_t)K * kS32Floats);
     f.body = (float*)take(sizeof(float) * (size_t)nb * kS32BodyFloats);
     f.lohi = (int16_t*)take(sizeof(int16_t) * 2 * (size_t)K);
     f.order = (uint16_t*)take(sizeof(uint16_t) * (size_t)K);
@@ -1548,9 +1551,11 @@ __device__ __forceinline__ int team_next(const G& g, int* counter, int* slot) {
 }
 
 // FP32 phase for the scenes whose compact copy takes lo_bytes < bytes <= slab bytes; G = WarpGroup gives
-// every warp of the block its own slab and scene, G = BlockGroup one slab and scene per block
-template <class G>
-__global__ void __launch_bounds__(kFp32Block) k_solve_fp32(const StepArgs a, int queue, size_t lo_bytes, size_t slab) {
+// every warp of the block its own slab and scene, G = BlockGroup one slab and scene per block.  kL2: the
+// scenes too large for any slab, with their contact rows in global memory (L2-resident) and the rest of
+// the copy in the slab.
+template <class G, bool kL2>
+__global__ void __launch_bounds__(kFp32BlockMax) k_solve_fp32(const StepArgs a, int queue, size_t lo_bytes, size_t slab) {
     extern __shared__ __align__(16) char f32_smem[];
     __shared__ double red[33];
     __shared__ int ired[33];
@@ -1577,9 +1582,13 @@ __global__ void __launch_bounds__(kFp32Block) k_solve_fp32(const StepArgs a, int
         const SceneRange R = scene_range(a, s);
         const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
         if (K == 0 || K > 65535 || nb > 32767) continue;
-        const size_t bytes = s32_bytes(K, nb);
-        if (bytes <= lo_bytes || bytes > slab) continue;
-        const S32Scene f = s32_carve(my_slab, K, nb);
+        if (kL2) {   // the scenes no slab holds whole, and whose bodies and level order fit one
+            if (s32_bytes(K, nb) <= lo_bytes || s32_bytes(K, nb, true) > slab) continue;
+        } else {
+            const size_t bytes = s32_bytes(K, nb);
+            if (bytes <= lo_bytes || bytes > slab) continue;
+        }
+        const S32Scene f = s32_carve(my_slab, K, nb, kL2 ? a.ws.c32 + kS32Floats * (size_t)R.c0 : nullptr);
         const int L = s32_load(a, g, R, s, f, coloured);
         float res = s32_residual(a, g, R, f);   // the warm-started iterate may already be good enough
         float best = res;
@@ -1861,9 +1870,11 @@ int ensure_kernel_attributes() {
     e = cudaFuncSetAttribute(k_solve_warps, cudaFuncAttributeMaxDynamicSharedMemorySize, warp_max);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_solve_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, block_max);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_solve_fp32<WarpGroup>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFp32LargeSmem);
+        e = cudaFuncSetAttribute(k_solve_fp32<WarpGroup, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFp32LargeSmem);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_solve_fp32<BlockGroup>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFp32LargeSmem);
+        e = cudaFuncSetAttribute(k_solve_fp32<BlockGroup, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFp32LargeSmem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_solve_fp32<BlockGroup, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFp32LargeSmem);
     if (e != cudaSuccess) return fail(RB_ERR_CUDA, std::string("rb_step: cudaFuncSetAttribute: ") + cudaGetErrorString(e));
     g_attr_done[dev] = true;
     return RB_OK;
@@ -1872,9 +1883,10 @@ int ensure_kernel_attributes() {
 // Side streams of the FP32 size classes, per host thread and device, made on the thread's first step on
 // the device (an uncaptured call).  Each step forks them from its stream with an event and joins them back,
 // which a stream capture records as parallel branches.
+constexpr int kSideStreams = 4;
 struct SideStreams {
-    cudaStream_t s[3] = {nullptr, nullptr, nullptr};
-    cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
+    cudaStream_t s[kSideStreams] = {};
+    cudaEvent_t fork = nullptr, join[kSideStreams] = {};
 };
 thread_local SideStreams g_side[64];
 int side_streams(SideStreams** out) {
@@ -1883,7 +1895,7 @@ int side_streams(SideStreams** out) {
     SideStreams& ss = g_side[dev];
     if (!ss.fork) {
         cudaError_t e = cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming);
-        for (int c = 0; c < 3 && e == cudaSuccess; ++c) {
+        for (int c = 0; c < kSideStreams && e == cudaSuccess; ++c) {
             e = cudaStreamCreateWithFlags(&ss.s[c], cudaStreamNonBlocking);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ss.join[c], cudaEventDisableTiming);
         }
@@ -1986,20 +1998,23 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     const int bg = bd->n_scenes < 148 * 16 ? bd->n_scenes : 148 * 16;
     k_sweeps32_init<<<blocks_for(bd->n_scenes, 256), 256, 0, st>>>(a); note_launch();
     if (pr->precision != RB_PRECISION_FP64) {
-        // FP32 phase in shared memory, three size classes side by side: warp teams with 28 KB slabs (8 scenes
-        // per SM), warp teams with 56 KB slabs (4 per SM), block teams with 224 KB (1 per SM)
+        // FP32 phase, four size classes side by side: warp teams with 28 KB slabs (8 scenes per SM), warp
+        // teams with 56 KB slabs (4 per SM), block teams with 224 KB (1 per SM), and 256-thread block teams
+        // for the scenes beyond that, whose contact rows stay in L2
         SideStreams* ss = nullptr;
         rc = side_streams(&ss);
         if (rc != RB_OK) return rc;
         cudaEventRecord(ss->fork, st);
-        for (int c = 0; c < 3; ++c) cudaStreamWaitEvent(ss->s[c], ss->fork, 0);
-        k_solve_fp32<WarpGroup><<<2 * 148, kFp32Block, 4 * (size_t)kS32SmallSlab, ss->s[0]>>>(
-            a, kQueueFp32, 0, kS32SmallSlab); note_launch();
-        k_solve_fp32<WarpGroup><<<148, kFp32Block, 4 * (size_t)kS32MidSlab, ss->s[1]>>>(
-            a, kQueueFp32 + 1, kS32SmallSlab, kS32MidSlab); note_launch();
-        k_solve_fp32<BlockGroup><<<148, kFp32Block, (size_t)kFp32LargeSmem, ss->s[2]>>>(
+        for (int c = 0; c < kSideStreams; ++c) cudaStreamWaitEvent(ss->s[c], ss->fork, 0);
+        k_solve_fp32<BlockGroup, true><<<148, kFp32BlockMax, (size_t)kFp32LargeSmem, ss->s[3]>>>(
+            a, kQueueFp32 + 3, kFp32LargeSmem, kFp32LargeSmem); note_launch();
+        k_solve_fp32<BlockGroup, false><<<148, kFp32Block, (size_t)kFp32LargeSmem, ss->s[2]>>>(
             a, kQueueFp32 + 2, kS32MidSlab, kFp32LargeSmem); note_launch();
-        for (int c = 0; c < 3; ++c) {
+        k_solve_fp32<WarpGroup, false><<<148, kFp32Block, 4 * (size_t)kS32MidSlab, ss->s[1]>>>(
+            a, kQueueFp32 + 1, kS32SmallSlab, kS32MidSlab); note_launch();
+        k_solve_fp32<WarpGroup, false><<<2 * 148, kFp32Block, 4 * (size_t)kS32SmallSlab, ss->s[0]>>>(
+            a, kQueueFp32, 0, kS32SmallSlab); note_launch();
+        for (int c = 0; c < kSideStreams; ++c) {
             cudaEventRecord(ss->join[c], ss->s[c]);
             cudaStreamWaitEvent(st, ss->join[c], 0);
         }
