@@ -1321,28 +1321,28 @@ constexpr int kS32MidSlab = 56 * 1024;               // slab of a warp team, mid
 constexpr float kFp32Floor = 1e-4f;
 
 struct S32Scene {
-    float* c;          // kS32Floats per contact (row q at 12 q: lin[3], ang_lo[3], ang_hi[3], b, 1/diag, x)
+    float* c;          // kS32Floats per contact, in level order (row q at 12 q: lin[3], ang_lo[3], ang_hi[3],
+                       // b, 1/diag, x; the torsion row's lin[0] holds mu)
     float* body;       // kS32BodyFloats per body: w[6], m^-1, fixed, I^-1 (xx, xy, xz, yy, yz, zz), pad[2]
-    int16_t* lohi;     // scene-local body indices, 2 per contact
-    uint16_t* order;   // contacts by level
+    uint32_t* lohi;    // per contact in level order: scene-local lo | hi << 16
+    uint16_t* pos;     // level-order position of each contact (scene-local contact index -> position)
     uint16_t* lptr;    // level starts (L + 1)
 };
 __host__ __device__ inline size_t s32_align(size_t v) { return (v + 15) & ~size_t(15); }
 // shared memory of a scene's FP32 copy; with contacts_in_l2 the contact rows live in global memory (L2)
 __host__ __device__ inline size_t s32_bytes(int K, int nb, bool contacts_in_l2 = false) {
     return (contacts_in_l2 ? 0 : s32_align(sizeof(float) * (size_t)K * kS32Floats)) +
-           s32_align(sizeof(float) * (size_t)nb * kS32BodyFloats) +
-           s32_align(sizeof(int16_t) * 2 * (size_t)K) + s32_align(sizeof(uint16_t) * (size_t)K) +
-           s32_align(sizeof(uint16_t) * (size_t)(K + 1));
+           s32_align(sizeof(float) * (size_t)nb * kS32BodyFloats) + s32_align(sizeof(uint32_t) * (size_t)K) +
+           s32_align(sizeof(uint16_t) * (size_t)K) + s32_align(sizeof(uint16_t) * (size_t)(K + 1));
 }
-__device__ inline S32Scene s32_carve(char* base, int K, int nb, float* c_global = nullptr) {
+__device__ __forceinline__ S32Scene s32_carve(char* base, int K, int nb, float* c_global = nullptr) {
     S32Scene f;
     size_t o = 0;
     auto take = [&](size_t bytes) { char* p = base + o; o += s32_align(bytes); return p; };
     f.c = c_global ? c_global : (float*)take(sizeof(float) * (size_t)K * kS32Floats);
     f.body = (float*)take(sizeof(float) * (size_t)nb * kS32BodyFloats);
-    f.lohi = (int16_t*)take(sizeof(int16_t) * 2 * (size_t)K);
-    f.order = (uint16_t*)take(sizeof(uint16_t) * (size_t)K);
+    f.lohi = (uint32_t*)take(sizeof(uint32_t) * (size_t)K);
+    f.pos = (uint16_t*)take(sizeof(uint16_t) * (size_t)K);
     f.lptr = (uint16_t*)take(sizeof(uint16_t) * (size_t)(K + 1));
     return f;
 }
@@ -1379,15 +1379,17 @@ __device__ __forceinline__ float s32_jw(const float* row, int q, const float* wl
     return s;
 }
 
-// copy scene R into the team's slab as FP32; returns the number of levels
+// copy scene R into the team's slab as FP32, contacts in level order; returns the number of levels
 template <class G>
-__device__ int s32_load(const StepArgs& a, const G& g, const SceneRange& R, int s, const S32Scene& f, bool coloured) {
+__device__ __forceinline__ int s32_load(const StepArgs& a, const G& g, const SceneRange& R, int s, const S32Scene& f,
+                                        bool coloured) {
     const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
     const int L = coloured ? scene_colours(a, g, R, s) : scene_levels(a, g, R, s);
-    for (int i = g.rank(); i < 16 * K; i += g.size()) {   // (contact, row, part) with part 0: J lin+ang, 1: rest
-        const int kl = i >> 4, q = (i >> 2) & 3, part = i & 3;
-        const size_t k = (size_t)R.c0 + kl;
-        float* row = f.c + kS32Floats * kl + 12 * q;
+    const int* order = a.ws.lev_order + R.c0;
+    for (int t = g.rank(); t < 16 * K; t += g.size()) {   // (position, row, part)
+        const int i = t >> 4, q = (t >> 2) & 3, part = t & 3;
+        const size_t k = (size_t)order[i];
+        float* row = f.c + kS32Floats * i + 12 * q;
         const double* J = a.ws.J + 48 * k + 12 * q;
         if (part == 0) {
             row[0] = q < 3 ? (float)J[0] : (float)a.ws.mu[k];
@@ -1403,11 +1405,10 @@ __device__ int s32_load(const StepArgs& a, const G& g, const SceneRange& R, int 
             row[11] = (float)a.ws.x[4 * k + q];
         }
     }
-    for (int kl = g.rank(); kl < K; kl += g.size()) {
-        const int k = R.c0 + kl;
-        f.lohi[2 * kl] = (int16_t)(a.ws.lohi[2 * k] - R.b0);
-        f.lohi[2 * kl + 1] = (int16_t)(a.ws.lohi[2 * k + 1] - R.b0);
-        f.order[kl] = (uint16_t)(a.ws.lev_order[R.c0 + kl] - R.c0);
+    for (int i = g.rank(); i < K; i += g.size()) {
+        const int k = order[i];
+        f.pos[k - R.c0] = (uint16_t)i;
+        f.lohi[i] = (uint32_t)(a.ws.lohi[2 * k] - R.b0) | ((uint32_t)(a.ws.lohi[2 * k + 1] - R.b0) << 16);
     }
     for (int l = g.rank(); l <= L; l += g.size()) f.lptr[l] = (uint16_t)a.ws.lev_ptr[R.c0 + s + l];
     for (int bl = g.rank(); bl < nb; bl += g.size()) {
@@ -1427,7 +1428,7 @@ __device__ int s32_load(const StepArgs& a, const G& g, const SceneRange& R, int 
 // w = W J^T x (each body sums its contacts in ascending order), then the FP32 residual
 // ||x - prox(x - D^-1 (A x + b))||_inf / max(1, ||x||_inf)
 template <class G>
-__device__ float s32_residual(const StepArgs& a, const G& g, const SceneRange& R, const S32Scene& f) {
+__device__ __forceinline__ float s32_residual(const StepArgs& a, const G& g, const SceneRange& R, const S32Scene& f) {
     const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
     for (int bl = g.rank(); bl < nb; bl += g.size()) {
         float* B = f.body + kS32BodyFloats * bl;
@@ -1436,8 +1437,8 @@ __device__ float s32_residual(const StepArgs& a, const G& g, const SceneRange& R
             const int b = R.b0 + bl;
             for (int e = a.ws.bc_ptr[b]; e < a.ws.bc_ptr[b + 1]; ++e) {
                 const int code = a.ws.bc_list[e];
-                const int kl = (code >> 1) - R.c0, side = code & 1;
-                const float* c = f.c + kS32Floats * kl;
+                const int side = code & 1;
+                const float* c = f.c + kS32Floats * f.pos[(code >> 1) - R.c0];
                 for (int q = 0; q < 4; ++q) {
                     const float* row = c + 12 * q;
                     const float xq = row[11];
@@ -1457,10 +1458,11 @@ __device__ float s32_residual(const StepArgs& a, const G& g, const SceneRange& R
     }
     g.sync();
     float m = 0.0f, xm = 0.0f;
-    for (int kl = g.rank(); kl < K; kl += g.size()) {
-        const float* c = f.c + kS32Floats * kl;
-        const float* wl = f.body + kS32BodyFloats * f.lohi[2 * kl];
-        const float* wh = f.body + kS32BodyFloats * f.lohi[2 * kl + 1];
+    for (int i = g.rank(); i < K; i += g.size()) {
+        const float* c = f.c + kS32Floats * i;
+        const uint32_t lh = f.lohi[i];
+        const float* wl = f.body + kS32BodyFloats * (int)(lh & 0xffffu);
+        const float* wh = f.body + kS32BodyFloats * (int)(lh >> 16);
         float z[4], x[4];
         for (int q = 0; q < 4; ++q) {
             const float* row = c + 12 * q;
@@ -1471,10 +1473,10 @@ __device__ float s32_residual(const StepArgs& a, const G& g, const SceneRange& R
         float fr[3];
         f32_prox(z[1], z[2], z[3], c[36], pn, fr);
         const float d[4] = {x[0] - pn, x[1] - fr[0], x[2] - fr[1], x[3] - fr[2]};
-        for (int i = 0; i < 4; ++i) {
-            m = fmaxf(m, fabsf(d[i]));
-            if (d[i] != d[i]) m = d[i];
-            xm = fmaxf(xm, fabsf(x[i]));
+        for (int t = 0; t < 4; ++t) {
+            m = fmaxf(m, fabsf(d[t]));
+            if (d[t] != d[t]) m = d[t];
+            xm = fmaxf(xm, fabsf(x[t]));
         }
     }
     const double mres = g.max((double)m);
@@ -1482,59 +1484,59 @@ __device__ float s32_residual(const StepArgs& a, const G& g, const SceneRange& R
     return (float)(mres / (mx > 1.0 ? mx : 1.0));
 }
 
-// one Gauss-Seidel sweep over the levels, four lanes per contact
+// One Gauss-Seidel sweep over the levels, four lanes per contact.  Lane q computes row q of J w; the z of
+// the four rows meet by shuffles and every lane applies the prox; lane q then forms one 3-vector of the
+// update from the four rows' columns it owns (lin for q = 0, 1; ang_lo for 2; ang_hi for 3) and applies
+// +m^-1, -m^-1, I_lo^-1 or I_hi^-1 to it.  Every lane runs the same instructions (lane-dependent offsets).
 template <class G>
 __device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, float rscale) {
     const int q = g.rank() & 3, slot = g.rank() >> 2, nslot = g.size() >> 2;
-    const int lane = threadIdx.x & 31, base = lane & ~3;
+    const int base = (threadIdx.x & 31) & ~3;
+    const unsigned qm = 0xfu << base;
+    const int off = q < 2 ? 0 : (q == 2 ? 3 : 6);   // the update columns this lane sums
+    int start = f.lptr[0], end = f.lptr[1];
     for (int l = 1; l <= L; ++l) {
-        const int start = f.lptr[l - 1], end = f.lptr[l];
+        const int next_end = l < L ? f.lptr[l + 1] : end;
         // every lane of a quad runs the same trip count, so the quad's shuffles see all four lanes
         for (int i0 = start; i0 < end; i0 += nslot) {
             const int i = i0 + slot;
-            const bool on = i < end;
-            if (on) {
-                const unsigned qm = 0xfu << base;   // the quad's lanes share `on`
-                const int kl = f.order[i];
-                const int lo = f.lohi[2 * kl], hi = f.lohi[2 * kl + 1];
-                float* row = f.c + kS32Floats * kl + 12 * q;
-                float* Bl = f.body + kS32BodyFloats * lo;
-                float* Bh = f.body + kS32BodyFloats * hi;
-                const float xo = row[11];
-                const float z = xo - rscale * row[10] * (s32_jw(row, q, Bl, Bh) + row[9]);
+            if (i < end) {
+                float* C = f.c + kS32Floats * i;
+                const uint32_t lh = f.lohi[i];
+                float* Bl = f.body + kS32BodyFloats * (int)(lh & 0xffffu);
+                float* Bh = f.body + kS32BodyFloats * (int)(lh >> 16);
+                const float* row = C + 12 * q;
+                float v[4][3], xo[4];
+                for (int j = 0; j < 4; ++j) {
+                    v[j][0] = C[12 * j + off]; v[j][1] = C[12 * j + off + 1]; v[j][2] = C[12 * j + off + 2];
+                    xo[j] = C[12 * j + 11];
+                }
+                const float mu = C[36];
+                const float z = xo[q] - rscale * row[10] * (s32_jw(row, q, Bl, Bh) + row[9]);
                 float zz[4];
                 for (int j = 0; j < 4; ++j) zz[j] = __shfl_sync(qm, z, base | j);
-                const float mu = __shfl_sync(qm, row[0], base | 3);
                 const float xn = fmaxf(zz[0], 0.0f);
                 float fr[3];
                 f32_prox(zz[1], zz[2], zz[3], mu, xn, fr);
-                const float xq = q == 0 ? xn : (q == 1 ? fr[0] : (q == 2 ? fr[1] : fr[2]));
-                row[11] = xq;
-                const float dq = xq - xo;
-                // quad sums: P = sum_q lin_q dx_q, Tl = sum_q ang_lo_q dx_q, Th = sum_q ang_hi_q dx_q
-                float v[9];
-                for (int j = 0; j < 3; ++j) v[j] = q < 3 ? row[j] * dq : 0.0f;
-                for (int j = 0; j < 3; ++j) v[3 + j] = row[3 + j] * dq;
-                for (int j = 0; j < 3; ++j) v[6 + j] = row[6 + j] * dq;
-                for (int j = 0; j < 9; ++j) {
-                    v[j] += __shfl_xor_sync(qm, v[j], 1);
-                    v[j] += __shfl_xor_sync(qm, v[j], 2);
-                }
+                const float d[4] = {xn - xo[0], fr[0] - xo[1], fr[1] - xo[2], fr[2] - xo[3]};
+                C[12 * q + 11] = q == 0 ? xn : (q == 1 ? fr[0] : (q == 2 ? fr[1] : fr[2]));
+                const float d3 = q < 2 ? 0.0f : d[3];   // the torsion row has no linear columns
+                float S[3];
+                for (int c = 0; c < 3; ++c)
+                    S[c] = fmaf(v[3][c], d3, fmaf(v[2][c], d[2], fmaf(v[1][c], d[1], v[0][c] * d[0])));
                 float* B = (q & 1) ? Bh : Bl;
-                if (B[7] == 0.0f) {
-                    if (q < 2) {          // linear: +m^-1 P on lo, -m^-1 P on hi
-                        const float sm = q ? -B[6] : B[6];
-                        B[0] = fmaf(sm, v[0], B[0]); B[1] = fmaf(sm, v[1], B[1]); B[2] = fmaf(sm, v[2], B[2]);
-                    } else {              // angular: I^-1 T
-                        const float t[3] = {q == 2 ? v[3] : v[6], q == 2 ? v[4] : v[7], q == 2 ? v[5] : v[8]};
-                        float om[3];
-                        s32_sym3(B + 8, t, om);
-                        B[3] += om[0]; B[4] += om[1]; B[5] += om[2];
-                    }
-                }
+                const float m = (q == 1) ? -B[6] : B[6];
+                const float I[6] = {q < 2 ? m : B[8], q < 2 ? 0.0f : B[9], q < 2 ? 0.0f : B[10],
+                                    q < 2 ? m : B[11], q < 2 ? 0.0f : B[12], q < 2 ? m : B[13]};
+                float dw[3];
+                s32_sym3(I, S, dw);
+                float* t = B + (q < 2 ? 0 : 3);
+                if (B[7] == 0.0f) { t[0] += dw[0]; t[1] += dw[1]; t[2] += dw[2]; }
             }
         }
         g.sync();
+        start = end;
+        end = next_end;
     }
 }
 
@@ -1555,7 +1557,7 @@ __device__ __forceinline__ int team_next(const G& g, int* counter, int* slot) {
 // scenes too large for any slab, with their contact rows in global memory (L2-resident) and the rest of
 // the copy in the slab.
 template <class G, bool kL2>
-__global__ void __launch_bounds__(kFp32BlockMax) k_solve_fp32(const StepArgs a, int queue, size_t lo_bytes, size_t slab) {
+__global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs a, int queue, size_t lo_bytes, size_t slab) {
     extern __shared__ __align__(16) char f32_smem[];
     __shared__ double red[33];
     __shared__ int ired[33];
@@ -1604,8 +1606,10 @@ __global__ void __launch_bounds__(kFp32BlockMax) k_solve_fp32(const StepArgs a, 
                 else if (best < kFp32Floor && ++stalls >= 3) break;
             }
         }
-        for (int i = g.rank(); i < 4 * K; i += g.size())
-            a.ws.x[4 * (size_t)R.c0 + i] = (double)f.c[kS32Floats * (i >> 2) + 12 * (i & 3) + 11];
+        for (int t = g.rank(); t < 4 * K; t += g.size()) {   // back to contact order
+            const int i = t >> 2, q = t & 3;
+            a.ws.x[4 * (size_t)a.ws.lev_order[R.c0 + i] + q] = (double)f.c[kS32Floats * i + 12 * q + 11];
+        }
         if (g.rank() == 0) a.ws.sweeps32[s] = sweeps;
         g.sync();
     }
