@@ -300,7 +300,15 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device(dev))
     from rainbow_b200 import engine_io, world as W
     from rainbow_b200.stepper import GpuStepper
-    arrays, params, cfg, engine = build_workload(args.workload, dev, args.scenes)
+    from rainbow_b200.sharding import max_over_ranks, partition_scenes, sum_over_ranks
+    if world_size > 1 and args.workload == "batch1024":
+        # weak scaling: world_size x --scenes scenes, split by body count so every GPU holds --scenes of them
+        arrays, params, cfg, engine = build_workload(args.workload, dev, args.scenes * world_size)
+        parts = partition_scenes([len(a["body_mass"]) for a in arrays], world_size)
+        arrays = [arrays[i] for i in parts[rank]]
+        cfg.update({"scenes_per_gpu": len(arrays), "scenes": args.scenes * world_size})
+    else:
+        arrays, params, cfg, engine = build_workload(args.workload, dev, args.scenes)
     max_it = int(params.max_iterations)
     world = W.DeviceWorld(arrays, device=dev, max_iterations=max(max_it, LONG_SWEEPS))
     kw = dict(scheme=args.scheme, termination=args.termination, residual_tolerance=args.tolerance,
@@ -393,13 +401,10 @@ def run_ours(args):
         dist.barrier()
     status = int(world.t_status[0].item())
     after = world.stats()
-    total_ms = float(times.sum())
-    if world_size > 1:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(float(times.sum()), dev)       # the slowest rank's device time
     n_scenes = world.n_scenes
-    value = world_size * n_scenes * args.steps / (total_ms / 1000.0)
+    all_scenes = int(sum_over_ranks(n_scenes, dev))
+    value = all_scenes * args.steps / (total_ms / 1000.0)
     residuals = np.array([s.residual for s in after if s.n_contacts > 0])
     iters = np.array([s.iterations + 1 if s.exitcode == 3 else max_it for s in after if s.n_contacts > 0])
     ncont = np.array([s.n_contacts for s in after])
@@ -409,7 +414,7 @@ def run_ours(args):
 
     # plain one-scene-per-launch FP64 baseline (same scheme, same tolerance, same starting states)
     plain = None
-    if n_scenes > 1 and args.plain_scenes > 0:
+    if n_scenes > 1 and args.plain_scenes > 0 and rank == 0:
         x0r, u0r = x0.reshape(-1, 7), u0.reshape(-1, 6)
         pts, gts = [], []
         for s in range(min(args.plain_scenes, n_scenes)):
@@ -465,11 +470,8 @@ def run_ours(args):
                 st = world.t_stats.cpu()
             el = time.perf_counter() - t0
             d2h = 13 * 8 * world.n_bodies + st.numel()
-        if world_size > 1:
-            t = torch.tensor([el], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
-        e2e = {"value": world_size * n_scenes * args.steps / el, "unit": "scene-steps/s",
+        el = max_over_ranks(el, dev)
+        e2e = {"value": all_scenes * args.steps / el, "unit": "scene-steps/s",
                "h2d_bytes_per_step": 13 * 8 * world.n_bodies, "d2h_bytes_per_step": int(d2h),
                "api": "GpuStepper.step via engine" if engine is not None else "DeviceWorld set_state/launch/state"}
 
@@ -500,7 +502,7 @@ def run_ours(args):
     achieved = nbytes / dt_s / 1e9 if dt_s > 0 else 0.0
 
     serving_rep = None
-    if args.serve_seconds > 0 and args.workload == "batch1024":
+    if args.serve_seconds > 0 and args.workload == "batch1024" and world_size == 1:
         serving_rep = run_serving(args, dev, dict(warm_start=warm, precision=prec, **kw), max_it)
 
     cpu = None
@@ -513,7 +515,9 @@ def run_ours(args):
                 "precision": prec, "warm_start": warm, "residual_interval": kw["residual_interval"], "pre_roll_steps": args.pre_roll, "contacts_per_step": int(K),
                 "sweeps_per_step_contacts": int(sweeps), "l2": "256 MB buffer written between timed steps",
                 "launch": "each timed step replays one CUDA graph of the whole rb_step",
-                "parallelism": "replicas" if world_size > 1 else "single"})
+                "parallelism": ("scenes partitioned over %d GPUs, no collective on the step" % world_size
+                                if world_size > 1 and args.workload == "batch1024"
+                                else "replicas" if world_size > 1 else "single")})
     line = {
         "metric": "scene-steps/s", "value": value, "unit": "scene-steps/s", "n_gpus": world_size,
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,

@@ -1161,7 +1161,10 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
     const WView w = {on_chip ? w_smem : a.ws.w + 6 * R.b0, R.b0};
     const bool coloured = !post && !jacobi &&
                           (scheme == RB_SCHEME_COLOURED_GS || a.pr.ordering == RB_ORDER_COLOURED);
-    const int L = jacobi ? 0 : (coloured ? scene_colours(a, g, R, s) : scene_levels(a, g, R, s));
+    // FP32 modes: the scene's FP32 phase left its iterate in x and its level order in lev_order / lev_ptr
+    const int sweeps32 = (!post && a.pr.precision != RB_PRECISION_FP64) ? a.ws.sweeps32[s] : -1;
+    const int L = jacobi ? 0 : sweeps32 >= 0 ? a.ws.nlev[s]
+                : (coloured ? scene_colours(a, g, R, s) : scene_levels(a, g, R, s));
     if (!post && g.rank() == 0) st->n_levels = L;
     const bool by_residual = !post && a.pr.termination != RB_TERMINATE_MERIT;
     const bool fixed_r = !post && a.pr.termination == RB_TERMINATE_RESIDUAL_FIXED_R;
@@ -1169,8 +1172,7 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
     double last = INFINITY, global_last = INFINITY, shown = 0.0;
     int iterations = max_it, exitcode = 0;
     bool w_is_wjt_x = false;   // w already holds WJT x for the current x (left by the residual pass)
-    // FP32 modes: the scene's FP32 phase left its iterate in x; test it in FP64, then refine in FP64
-    const int sweeps32 = (!post && a.pr.precision != RB_PRECISION_FP64) ? a.ws.sweeps32[s] : -1;
+    // FP32 modes: test the FP32 iterate in FP64, then refine it in FP64 with the sweeps left
     int loop_max = max_it;
     if (sweeps32 >= 0) {
         const double res0 = scene_residual(a, g, R, x, w);
@@ -1592,6 +1594,7 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
         }
         const S32Scene f = s32_carve(my_slab, K, nb, kL2 ? a.ws.c32 + kS32Floats * (size_t)R.c0 : nullptr);
         const int L = s32_load(a, g, R, s, f, coloured);
+        if (g.rank() == 0) a.ws.nlev[s] = L;
         float res = s32_residual(a, g, R, f);   // the warm-started iterate may already be good enough
         float best = res;
         int sweeps = 0, stalls = 0;
