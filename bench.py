@@ -35,6 +35,7 @@ sys.path.insert(0, ROOT)
 
 
 
+PROFILED_SOLVE_DRAM_BYTES = 44_989_440   # FP32 solve kernels of one batch1024 step (ncu, cold caches)
 LONG_SWEEPS = 4000   # iteration cap of the converged reference solve the error figures are measured against
 
 
@@ -44,7 +45,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batch1024", choices=["batch1024", "mixed4096", "boxes64"])
+    ap.add_argument("--workload", default="batch1024", choices=["batch1024", "mixed4096", "boxes64", "tower32"],
+                    help="tower32: the precision stress comparison (FP64 / FP32 + FP64 refinement / FP32)")
     ap.add_argument("--scheme", default="rigid_gauss_seidel")
     ap.add_argument("--termination", default="residual_fixed_r", choices=["residual_fixed_r", "residual", "merit"])
     ap.add_argument("--scenes", type=int, default=1024, help="scenes of the batch1024 workload")
@@ -478,6 +480,8 @@ def run_ours(args):
     # roofline of the dominant phase from the profiled step (event times on the launching stream)
     K = sum(s.n_contacts for s in stats)
     sweeps = sum(s.n_contacts * ((s.iterations + 1) if 0 <= s.iterations < max_it else max_it) for s in stats)
+    sweeps32 = sum(s.n_contacts * min(max(s.fp32_sweeps, 0), max_it) for s in stats)   # of those, in FP32
+    sweeps64 = max(0, sweeps - sweeps32)
     cand = sum(s.n_candidates for s in stats)
     lookups = sum(s.n_grid_lookups for s in stats)
     npairs = sum(s.n_pairs for s in stats)
@@ -486,9 +490,10 @@ def run_ours(args):
         "contact_search": (phases[2], cand * (72 + 64) + lookups * 64,
                            "per candidate triangle: 3 world vertices (72 B) + result record (64 B); 8 grid values "
                            "(64 B) per signed distance lookup, lookups counted on the device"),
-        "solve": (phases[4], sweeps * 137 * 8 + resid_passes * 106 * 8,
-                  "per contact per sweep: J 48 + WJT 48 + b 4 + r 4 + mu 1 + x 8 + body w 24 doubles (1096 B); "
-                  "residual pass: J 48 + WJT 48 + b 4 + x 4 + mu 1 + w 1 doubles"),
+        "solve": (phases[4], sweeps64 * 137 * 8 + sweeps32 * 137 * 4 + resid_passes * 106 * 8,
+                  "per contact per sweep: J 48 + WJT 48 + b 4 + r 4 + mu 1 + x 8 + body w 24 values, 8 B each in "
+                  "FP64 sweeps (1096 B) and 4 B in FP32 sweeps (548 B); residual pass: J 48 + WJT 48 + b 4 + x 4 "
+                  "+ mu 1 + w 1 doubles"),
         "pairs_and_candidates": (phases[1], npairs * 2 * 48 + cand * 8,
                                  "per body pair: 2 boxes (96 B); per candidate 8 B"),
     }
@@ -499,6 +504,10 @@ def run_ours(args):
         peaks = {}
     peak = float(peaks.get("hbm_gbs", 6650.0))
     dt_s, nbytes, model = alg[dom]
+    # DRAM bytes of the solve phase's kernels per step, from the ncu capture summarised in
+    # profiles/k_solve_fp32_batch1024.md (the FP32 copies live in shared memory, so DRAM sees the copy-in only)
+    traffic = PROFILED_SOLVE_DRAM_BYTES if (dom == "solve" and args.workload == "batch1024"
+                                             and prec != "fp64") else None
     achieved = nbytes / dt_s / 1e9 if dt_s > 0 else 0.0
 
     serving_rep = None
@@ -536,7 +545,7 @@ def run_ours(args):
                      "levels_per_scene_p50_max": [float(np.percentile(levels, 50)), int(levels.max())]
                      if len(levels) else None},
         "roofline": {"bound": "hbm", "kernel_phase": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "algorithmic_bytes": int(nbytes),
+                     "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": int(nbytes),
                      "bytes_model": model, "phase_ms": dt_s * 1000.0,
                      "peak_source": "of measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "of fallback 6650 GB/s"},
         "phases_ms": {k: v * 1000.0 for k, v in zip(["bodies_bvh", "pairs_candidates", "contact_search", "dedup",
@@ -554,8 +563,54 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_tower(args):
+    """32-high box tower, masses alternating 1 and 1000, mu 0.6, dt 0.005, --steps steps (500 by the
+    configuration) in each precision; residual and position drift against the FP64 run per step."""
+    import torch
+    from rainbow_b200 import engine_io, scenes, world as W
+    arrays = engine_io.scene_arrays(scenes.box_tower(32, device="cuda:0"))
+    params = W.params_from_vector(arrays["params"])
+    out = {}
+    for mode in ("fp64", "fp32_refine", "fp32"):
+        w = W.DeviceWorld(arrays, max_iterations=100)
+        rp = W.make_rb_params(params, precision=mode, termination="residual_fixed_r", residual_tolerance=1e-6,
+                              residual_interval=4, warm_start=True)
+        xs, res, ms = [], [], []
+        stream = torch.cuda.current_stream()
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            w.step(rp)
+            e1.record(stream)
+            xs.append(w.state()[0][:, :3].copy())
+            res.append(w.stats()[0].residual)
+            ms.append(e0.elapsed_time(e1))
+        out[mode] = (np.array(xs), np.array(res), np.array(ms))
+    x64 = out["fp64"][0]
+    every = max(1, args.steps // 20)
+    report = {}
+    for mode, (xs, res, ms) in out.items():
+        drift = np.abs(xs - x64).max(axis=(1, 2))
+        report[mode] = {"ms_per_step": float(ms.mean()), "residual_median": float(np.median(res)),
+                        "residual_max": float(res.max()),
+                        "per_step": [{"step": k + 1, "residual": float(res[k]), "drift_m": float(drift[k])}
+                                     for k in range(every - 1, args.steps, every)]}
+    line = {"metric": "scene-steps/s", "value": 1000.0 / report["fp32_refine"]["ms_per_step"],
+            "unit": "scene-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": 0,
+            "ms_per_step": report["fp32_refine"]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "box_tower_32_mass_ratio_1e3", "bodies": 33, "dt": 0.005, "mu": 0.6,
+                       "termination": "residual_fixed_r", "tolerance": 1e-6, "max_iterations": 100},
+            "precision": report}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload == "tower32":
+        if int(os.environ.get("RANK", "0")) == 0:
+            run_tower(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
