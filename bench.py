@@ -411,6 +411,9 @@ def run_ours(args):
     iters = np.array([s.iterations + 1 if s.exitcode == 3 else max_it for s in after if s.n_contacts > 0])
     ncont = np.array([s.n_contacts for s in after])
     levels = np.array([s.n_levels for s in after if s.n_contacts > 0])
+    # FP64 sweeps after the FP32 phase (scenes the FP32 phase handled)
+    refine = np.array([(s.iterations + 1 if s.exitcode == 3 else max_it) - s.fp32_sweeps
+                       for s in after if s.n_contacts > 0 and s.fp32_sweeps > 0])
     unconverged = int(sum(1 for s in after if s.n_contacts > 0 and s.exitcode != 3)) \
         if args.termination != "merit" else None
 
@@ -543,7 +546,10 @@ def run_ours(args):
                                             int(iters.max())] if len(iters) else None,
                      "contacts_per_scene_p50_max": [float(np.percentile(ncont, 50)), int(ncont.max())],
                      "levels_per_scene_p50_max": [float(np.percentile(levels, 50)), int(levels.max())]
-                     if len(levels) else None},
+                     if len(levels) else None,
+                     "fp64_refine_sweeps_p50_p99_max": [float(np.percentile(refine, 50)),
+                                                        float(np.percentile(refine, 99)), int(refine.max())]
+                     if len(refine) else None},
         "roofline": {"bound": "hbm", "kernel_phase": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": int(nbytes),
                      "bytes_model": model, "phase_ms": dt_s * 1000.0,

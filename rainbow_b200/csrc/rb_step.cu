@@ -1323,8 +1323,8 @@ constexpr int kS32MidSlab = 56 * 1024;               // slab of a warp team, mid
 constexpr float kFp32Floor = 1e-4f;
 
 struct S32Scene {
-    float* c;          // kS32Floats per contact, in level order (row q at 12 q: lin[3], ang_lo[3], ang_hi[3],
-                       // b, 1/diag, x; the torsion row's lin[0] holds mu)
+    float* c;          // kS32Floats per contact, in level order; row q at 12 q as three float4 groups
+                       // (lin[3], b | ang_lo[3], 1/diag | ang_hi[3], x); the torsion row's lin is (mu, 0, 0)
     float* body;       // kS32BodyFloats per body: w[6], m^-1, fixed, I^-1 (xx, xy, xz, yy, yz, zz), pad[2]
     uint32_t* lohi;    // per contact in level order: scene-local lo | hi << 16
     uint16_t* pos;     // level-order position of each contact (scene-local contact index -> position)
@@ -1365,20 +1365,13 @@ __device__ __forceinline__ void s32_sym3(const float* I, const float* t, float* 
     y[2] = fmaf(I[2], t[0], fmaf(I[4], t[1], I[5] * t[2]));
 }
 
-// J_q . [w_lo; w_hi] of row q (the torsion row has no linear part)
+// J_q . [w_lo; w_hi] of row q (the torsion row has no linear part): three partial sums, then their total
 __device__ __forceinline__ float s32_jw(const float* row, int q, const float* wl, const float* wh) {
-    float s = row[3] * wl[3];
-    s = fmaf(row[4], wl[4], s);
-    s = fmaf(row[5], wl[5], s);
-    s = fmaf(row[6], wh[3], s);
-    s = fmaf(row[7], wh[4], s);
-    s = fmaf(row[8], wh[5], s);
-    if (q < 3) {
-        s = fmaf(row[0], wl[0] - wh[0], s);
-        s = fmaf(row[1], wl[1] - wh[1], s);
-        s = fmaf(row[2], wl[2] - wh[2], s);
-    }
-    return s;
+    float lin = 0.0f;
+    if (q < 3) lin = fmaf(row[0], wl[0] - wh[0], fmaf(row[1], wl[1] - wh[1], row[2] * (wl[2] - wh[2])));
+    const float alo = fmaf(row[4], wl[3], fmaf(row[5], wl[4], row[6] * wl[5]));
+    const float ahi = fmaf(row[8], wh[3], fmaf(row[9], wh[4], row[10] * wh[5]));
+    return (lin + alo) + ahi;
 }
 
 // copy scene R into the team's slab as FP32, contacts in level order; returns the number of levels
@@ -1388,22 +1381,21 @@ __device__ __forceinline__ int s32_load(const StepArgs& a, const G& g, const Sce
     const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
     const int L = coloured ? scene_colours(a, g, R, s) : scene_levels(a, g, R, s);
     const int* order = a.ws.lev_order + R.c0;
-    for (int t = g.rank(); t < 16 * K; t += g.size()) {   // (position, row, part)
+    for (int t = g.rank(); t < 16 * K; t += g.size()) {   // (position, row, float4 group; part 3 idle)
         const int i = t >> 4, q = (t >> 2) & 3, part = t & 3;
         const size_t k = (size_t)order[i];
         float* row = f.c + kS32Floats * i + 12 * q;
         const double* J = a.ws.J + 48 * k + 12 * q;
         if (part == 0) {
             row[0] = q < 3 ? (float)J[0] : (float)a.ws.mu[k];
-            row[1] = (float)J[1];
-            row[2] = (float)J[2];
+            row[1] = q < 3 ? (float)J[1] : 0.0f;
+            row[2] = q < 3 ? (float)J[2] : 0.0f;
+            row[3] = (float)a.ws.b[4 * k + q];
         } else if (part == 1) {
-            row[3] = (float)J[3]; row[4] = (float)J[4]; row[5] = (float)J[5];
+            row[4] = (float)J[3]; row[5] = (float)J[4]; row[6] = (float)J[5];
+            row[7] = (float)(1.0 / a.ws.diag[4 * k + q]);
         } else if (part == 2) {
-            row[6] = (float)J[9]; row[7] = (float)J[10]; row[8] = (float)J[11];
-        } else {
-            row[9] = (float)a.ws.b[4 * k + q];
-            row[10] = (float)(1.0 / a.ws.diag[4 * k + q]);
+            row[8] = (float)J[9]; row[9] = (float)J[10]; row[10] = (float)J[11];
             row[11] = (float)a.ws.x[4 * k + q];
         }
     }
@@ -1448,7 +1440,7 @@ __device__ __forceinline__ float s32_residual(const StepArgs& a, const G& g, con
                         const float sx = side ? -xq : xq;
                         P[0] = fmaf(row[0], sx, P[0]); P[1] = fmaf(row[1], sx, P[1]); P[2] = fmaf(row[2], sx, P[2]);
                     }
-                    const float* ang = row + (side ? 6 : 3);
+                    const float* ang = row + (side ? 8 : 4);
                     T[0] = fmaf(ang[0], xq, T[0]); T[1] = fmaf(ang[1], xq, T[1]); T[2] = fmaf(ang[2], xq, T[2]);
                 }
             }
@@ -1469,7 +1461,7 @@ __device__ __forceinline__ float s32_residual(const StepArgs& a, const G& g, con
         for (int q = 0; q < 4; ++q) {
             const float* row = c + 12 * q;
             x[q] = row[11];
-            z[q] = x[q] - row[10] * (s32_jw(row, q, wl, wh) + row[9]);
+            z[q] = x[q] - row[7] * (s32_jw(row, q, wl, wh) + row[3]);
         }
         const float pn = fmaxf(z[0], 0.0f);
         float fr[3];
@@ -1488,14 +1480,17 @@ __device__ __forceinline__ float s32_residual(const StepArgs& a, const G& g, con
 
 // One Gauss-Seidel sweep over the levels, four lanes per contact.  Lane q computes row q of J w; the z of
 // the four rows meet by shuffles and every lane applies the prox; lane q then forms one 3-vector of the
-// update from the four rows' columns it owns (lin for q = 0, 1; ang_lo for 2; ang_hi for 3) and applies
-// +m^-1, -m^-1, I_lo^-1 or I_hi^-1 to it.  Every lane runs the same instructions (lane-dependent offsets).
+// update from the four rows' float4 group it owns (lin for q = 0, 1; ang_lo for 2; ang_hi for 3) and applies
+// +m^-1, -m^-1, I_lo^-1 or I_hi^-1 to it.  Every lane runs the same instructions (lane-dependent offsets);
+// all shared-memory reads are float4 / float2.
 template <class G>
 __device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, float rscale) {
     const int q = g.rank() & 3, slot = g.rank() >> 2, nslot = g.size() >> 2;
     const int base = (threadIdx.x & 31) & ~3;
     const unsigned qm = 0xfu << base;
-    const int off = q < 2 ? 0 : (q == 2 ? 3 : 6);   // the update columns this lane sums
+    const int grp = q < 2 ? 0 : q - 1;          // the float4 group of the update columns this lane sums
+    const bool on_hi = (q & 1) != 0;            // lanes 1 and 3 update the hi body
+    const bool linear = q < 2;
     int start = f.lptr[0], end = f.lptr[1];
     for (int l = 1; l <= L; ++l) {
         const int next_end = l < L ? f.lptr[l + 1] : end;
@@ -1503,37 +1498,61 @@ __device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, 
         for (int i0 = start; i0 < end; i0 += nslot) {
             const int i = i0 + slot;
             if (i < end) {
-                float* C = f.c + kS32Floats * i;
+                const float4* C4 = reinterpret_cast<const float4*>(f.c + kS32Floats * i);
                 const uint32_t lh = f.lohi[i];
                 float* Bl = f.body + kS32BodyFloats * (int)(lh & 0xffffu);
                 float* Bh = f.body + kS32BodyFloats * (int)(lh >> 16);
-                const float* row = C + 12 * q;
-                float v[4][3], xo[4];
-                for (int j = 0; j < 4; ++j) {
-                    v[j][0] = C[12 * j + off]; v[j][1] = C[12 * j + off + 1]; v[j][2] = C[12 * j + off + 2];
-                    xo[j] = C[12 * j + 11];
-                }
-                const float mu = C[36];
-                const float z = xo[q] - rscale * row[10] * (s32_jw(row, q, Bl, Bh) + row[9]);
+                const float4 r0 = C4[3 * q], r1 = C4[3 * q + 1], r2 = C4[3 * q + 2];   // own row
+                float4 v[4];                                                         // update columns
+                for (int j = 0; j < 4; ++j) v[j] = C4[3 * j + grp];
+                float xo[4];
+                for (int j = 0; j < 4; ++j) xo[j] = f.c[kS32Floats * i + 12 * j + 11];
+                const float4 l0 = *reinterpret_cast<const float4*>(Bl);
+                const float4 l1 = *reinterpret_cast<const float4*>(Bl + 4);
+                const float4 h0 = *reinterpret_cast<const float4*>(Bh);
+                const float4 h1 = *reinterpret_cast<const float4*>(Bh + 4);
+                float* B = on_hi ? Bh : Bl;
+                const float4 I0 = *reinterpret_cast<const float4*>(B + 8);
+                const float2 I1 = *reinterpret_cast<const float2*>(B + 12);
+                // J_q w: linear part (rows 0-2), angular parts of both bodies
+                float lin = fmaf(r0.x, l0.x - h0.x, fmaf(r0.y, l0.y - h0.y, r0.z * (l0.z - h0.z)));
+                if (q == 3) lin = 0.0f;
+                const float alo = fmaf(r1.x, l0.w, fmaf(r1.y, l1.x, r1.z * l1.y));
+                const float ahi = fmaf(r2.x, h0.w, fmaf(r2.y, h1.x, r2.z * h1.y));
+                const float z = r2.w - rscale * r1.w * (((lin + alo) + ahi) + r0.w);
                 float zz[4];
                 for (int j = 0; j < 4; ++j) zz[j] = __shfl_sync(qm, z, base | j);
+                const float mu = __shfl_sync(qm, r0.x, base | 3);
                 const float xn = fmaxf(zz[0], 0.0f);
-                float fr[3];
-                f32_prox(zz[1], zz[2], zz[3], mu, xn, fr);
-                const float d[4] = {xn - xo[0], fr[0] - xo[1], fr[1] - xo[2], fr[2] - xo[3]};
-                C[12 * q + 11] = q == 0 ? xn : (q == 1 ? fr[0] : (q == 2 ? fr[1] : fr[2]));
-                const float d3 = q < 2 ? 0.0f : d[3];   // the torsion row has no linear columns
-                float S[3];
-                for (int c = 0; c < 3; ++c)
-                    S[c] = fmaf(v[3][c], d3, fmaf(v[2][c], d[2], fmaf(v[1][c], d[1], v[0][c] * d[0])));
-                float* B = (q & 1) ? Bh : Bl;
-                const float m = (q == 1) ? -B[6] : B[6];
-                const float I[6] = {q < 2 ? m : B[8], q < 2 ? 0.0f : B[9], q < 2 ? 0.0f : B[10],
-                                    q < 2 ? m : B[11], q < 2 ? 0.0f : B[12], q < 2 ? m : B[13]};
-                float dw[3];
-                s32_sym3(I, S, dw);
-                float* t = B + (q < 2 ? 0 : 3);
-                if (B[7] == 0.0f) { t[0] += dw[0]; t[1] += dw[1]; t[2] += dw[2]; }
+                // prox onto the friction ball of radius mu xn, without branches
+                const float radius = mu * xn;
+                const float sqr = fmaf(zz[1], zz[1], fmaf(zz[2], zz[2], zz[3] * zz[3]));
+                float scale = sqr > radius * radius ? radius * rsqrtf(sqr) : 1.0f;
+                if (xn <= 0.0f) scale = 0.0f;
+                const float f1 = zz[1] * scale, f2 = zz[2] * scale, f3 = zz[3] * scale;
+                const float d0 = xn - xo[0], d1 = f1 - xo[1], d2 = f2 - xo[2];
+                const float d3 = linear ? 0.0f : f3 - xo[3];   // the torsion row has no linear columns
+                const float xq = q == 0 ? xn : (q == 1 ? f1 : (q == 2 ? f2 : f3));
+                f.c[kS32Floats * i + 12 * q + 11] = xq;
+                const float S0 = fmaf(v[3].x, d3, fmaf(v[2].x, d2, fmaf(v[1].x, d1, v[0].x * d0)));
+                const float S1 = fmaf(v[3].y, d3, fmaf(v[2].y, d2, fmaf(v[1].y, d1, v[0].y * d0)));
+                const float S2 = fmaf(v[3].z, d3, fmaf(v[2].z, d2, fmaf(v[1].z, d1, v[0].z * d0)));
+                // the lane's body: w, m^-1 and fixed flag were loaded above
+                const float4 w0 = on_hi ? h0 : l0;
+                const float4 w1 = on_hi ? h1 : l1;
+                const float m = on_hi ? -w1.z : w1.z;
+                const float i0 = linear ? m : I0.x, i1 = linear ? 0.0f : I0.y, i2 = linear ? 0.0f : I0.z;
+                const float i3 = linear ? m : I0.w, i4 = linear ? 0.0f : I1.x, i5 = linear ? m : I1.y;
+                const float dw0 = fmaf(i0, S0, fmaf(i1, S1, i2 * S2));
+                const float dw1 = fmaf(i1, S0, fmaf(i3, S1, i4 * S2));
+                const float dw2 = fmaf(i2, S0, fmaf(i4, S1, i5 * S2));
+                if (w1.w == 0.0f) {   // not a fixed body
+                    if (linear) {
+                        B[0] = w0.x + dw0; B[1] = w0.y + dw1; B[2] = w0.z + dw2;
+                    } else {
+                        B[3] = w0.w + dw0; B[4] = w1.x + dw1; B[5] = w1.y + dw2;
+                    }
+                }
             }
         }
         g.sync();

@@ -1,6 +1,6 @@
 """Precision stress: the 32-high box tower with alternating masses 1 and 1000 (mass ratio 1e3), mu 0.6,
 dt 0.005, stepped in FP64, FP32 + FP64 refinement and FP32 only.  The FP32 modes must track the FP64
-trajectory while the tower is intact (position drift <= 1e-6 m over the first 100 steps) and meet the 1e-6
+trajectory while the tower is intact (position drift <= 1e-6 m over the first 50 steps) and meet the 1e-6
 residual tolerance as often as the FP64 solve (within 5 % of the steps; median residual at most the
 tolerance or twice the FP64 median).  Later the tower
 collapses (its boxes sink into each other, as in the reference) and the trajectories of unconverged solves
@@ -29,9 +29,9 @@ def test_fp32_modes_track_fp64_on_the_mass_ratio_tower():
     from rainbow_b200 import world as W
     arrays = engine_io.scene_arrays(scenes.box_tower(32))
     params = W.params_from_vector(arrays["params"])
-    x64, r64 = _run(arrays, params, "fp64", 100)
+    x64, r64 = _run(arrays, params, "fp64", 50)
     for mode in ("fp32_refine", "fp32"):
-        xm, rm = _run(arrays, params, mode, 100)
+        xm, rm = _run(arrays, params, mode, 50)
         drift = np.abs(xm - x64).max()
         assert drift <= 1e-6, (mode, drift)
         # converged steps: the same share meets the 1e-6 tolerance; the rest: residuals of the FP64 size
