@@ -159,7 +159,7 @@ typedef struct rb_params {
                                      Gauss-Seidel scheme */
     int32_t refine_iterations;    /* RB_PRECISION_FP32_REFINE: FP64 sweeps reserved after the FP32 phase (0 to
                                      max_iterations).  The FP32 phase sweeps until its residual meets the
-                                     tolerance, stalls below 1e-4, or max_iterations - refine_iterations sweeps
+                                     tolerance, stalls below 1e-5, or max_iterations - refine_iterations sweeps
                                      are done; the FP64 refinement then gets the sweeps left of max_iterations.
                                      The residual of the result is always evaluated in FP64 */
     int32_t warm_start;           /* nonzero: start each contact's impulse from the previous step's solution for

@@ -1320,7 +1320,7 @@ constexpr int kFp32LargeSmem = 224 * 1024;           // slab of a block team (on
 constexpr int kS32SmallSlab = 28 * 1024;             // slab of a warp team, small class (8 scenes per SM)
 constexpr int kS32MidSlab = 56 * 1024;               // slab of a warp team, mid class (4 scenes per SM)
 // relative residual below which a stalled FP32 iteration is taken to have met FP32 rounding
-constexpr float kFp32Floor = 1e-4f;
+constexpr float kFp32Floor = 1e-5f;
 
 struct S32Scene {
     float* c;          // kS32Floats per contact, in level order; row q at 12 q as three float4 groups
@@ -1329,13 +1329,16 @@ struct S32Scene {
     uint32_t* lohi;    // per contact in level order: scene-local lo | hi << 16
     uint16_t* pos;     // level-order position of each contact (scene-local contact index -> position)
     uint16_t* lptr;    // level starts (L + 1)
+    uint16_t* bptr;    // per body: start of its contact list in blist (nb + 1)
+    uint32_t* blist;   // per body, its contacts in ascending order: level-order position << 1 | side (2K)
 };
 __host__ __device__ inline size_t s32_align(size_t v) { return (v + 15) & ~size_t(15); }
 // shared memory of a scene's FP32 copy; with contacts_in_l2 the contact rows live in global memory (L2)
 __host__ __device__ inline size_t s32_bytes(int K, int nb, bool contacts_in_l2 = false) {
     return (contacts_in_l2 ? 0 : s32_align(sizeof(float) * (size_t)K * kS32Floats)) +
            s32_align(sizeof(float) * (size_t)nb * kS32BodyFloats) + s32_align(sizeof(uint32_t) * (size_t)K) +
-           s32_align(sizeof(uint16_t) * (size_t)K) + s32_align(sizeof(uint16_t) * (size_t)(K + 1));
+           s32_align(sizeof(uint16_t) * (size_t)K) + s32_align(sizeof(uint16_t) * (size_t)(K + 1)) +
+           s32_align(sizeof(uint16_t) * (size_t)(nb + 1)) + s32_align(sizeof(uint32_t) * 2 * (size_t)K);
 }
 __device__ __forceinline__ S32Scene s32_carve(char* base, int K, int nb, float* c_global = nullptr) {
     S32Scene f;
@@ -1346,6 +1349,8 @@ __device__ __forceinline__ S32Scene s32_carve(char* base, int K, int nb, float* 
     f.lohi = (uint32_t*)take(sizeof(uint32_t) * (size_t)K);
     f.pos = (uint16_t*)take(sizeof(uint16_t) * (size_t)K);
     f.lptr = (uint16_t*)take(sizeof(uint16_t) * (size_t)(K + 1));
+    f.bptr = (uint16_t*)take(sizeof(uint16_t) * (size_t)(nb + 1));
+    f.blist = (uint32_t*)take(sizeof(uint32_t) * 2 * (size_t)K);
     return f;
 }
 
@@ -1405,6 +1410,14 @@ __device__ __forceinline__ int s32_load(const StepArgs& a, const G& g, const Sce
         f.lohi[i] = (uint32_t)(a.ws.lohi[2 * k] - R.b0) | ((uint32_t)(a.ws.lohi[2 * k + 1] - R.b0) << 16);
     }
     for (int l = g.rank(); l <= L; l += g.size()) f.lptr[l] = (uint16_t)a.ws.lev_ptr[R.c0 + s + l];
+    g.sync();   // pos complete
+    // per-body contact lists (the residual's w = W J^T x), positions in level order
+    const int e0 = a.ws.bc_ptr[R.b0];
+    for (int bl = g.rank(); bl <= nb; bl += g.size()) f.bptr[bl] = (uint16_t)(a.ws.bc_ptr[R.b0 + bl] - e0);
+    for (int e = g.rank(); e < a.ws.bc_ptr[R.b1] - e0; e += g.size()) {
+        const int code = a.ws.bc_list[e0 + e];
+        f.blist[e] = ((uint32_t)f.pos[(code >> 1) - R.c0] << 1) | (uint32_t)(code & 1);
+    }
     for (int bl = g.rank(); bl < nb; bl += g.size()) {
         const int b = R.b0 + bl;
         float* B = f.body + kS32BodyFloats * bl;
@@ -1428,11 +1441,10 @@ __device__ __forceinline__ float s32_residual(const StepArgs& a, const G& g, con
         float* B = f.body + kS32BodyFloats * bl;
         float P[3] = {0.f, 0.f, 0.f}, T[3] = {0.f, 0.f, 0.f};
         if (B[7] == 0.0f) {
-            const int b = R.b0 + bl;
-            for (int e = a.ws.bc_ptr[b]; e < a.ws.bc_ptr[b + 1]; ++e) {
-                const int code = a.ws.bc_list[e];
+            for (int e = f.bptr[bl]; e < f.bptr[bl + 1]; ++e) {
+                const uint32_t code = f.blist[e];
                 const int side = code & 1;
-                const float* c = f.c + kS32Floats * f.pos[(code >> 1) - R.c0];
+                const float* c = f.c + kS32Floats * (code >> 1);
                 for (int q = 0; q < 4; ++q) {
                     const float* row = c + 12 * q;
                     const float xq = row[11];
@@ -1604,7 +1616,7 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
         if (s >= a.bd.n_scenes) break;
         const SceneRange R = scene_range(a, s);
         const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
-        if (K == 0 || K > 65535 || nb > 32767) continue;
+        if (K == 0 || K > 32767 || nb > 32767) continue;   // 16-bit positions and list offsets
         if (kL2) {   // the scenes no slab holds whole, and whose bodies and level order fit one
             if (s32_bytes(K, nb) <= lo_bytes || s32_bytes(K, nb, true) > slab) continue;
         } else {
