@@ -1321,6 +1321,7 @@ constexpr int kS32SmallSlab = 28 * 1024;             // slab of a warp team, sma
 constexpr int kS32MidSlab = 56 * 1024;               // slab of a warp team, mid class (4 scenes per SM)
 // relative residual below which a stalled FP32 iteration is taken to have met FP32 rounding
 constexpr float kFp32Floor = 1e-5f;
+constexpr int kS32Corrections = 3;   // FP64 defect corrections of one scene's FP32 problem per step
 
 struct S32Scene {
     float* c;          // kS32Floats per contact, in level order; row q at 12 q as three float4 groups
@@ -1573,6 +1574,70 @@ __device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, 
     }
 }
 
+// FP64 check of the FP32 iterate and defect correction of the FP32 problem.  With x the current FP32 iterate,
+// evaluates A x + b in FP64 (J, W J^T and b of the FP64 problem, w in the scene's global FP64 accumulators)
+// and in FP32 (the shared copy), adds the difference to the FP32 b, and returns the FP64 residual
+// ||x - prox(x - D^-1 (A x + b))||_inf / max(1, ||x||_inf).  The FP32 sweeps that follow then converge to the
+// FP64 problem's solution: at the current x the corrected FP32 problem has the FP64 problem's residual.  The
+// FP32 w must hold W J^T x for this x (the residual test just before rebuilt it).
+template <class G>
+__device__ __forceinline__ double s32_correct(const StepArgs& a, const G& g, const SceneRange& R, const S32Scene& f) {
+    const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
+    const int* order = a.ws.lev_order + R.c0;
+    double* w64 = a.ws.w + 6 * (size_t)R.b0;   // the scene's FP64 accumulators, unused until the FP64 solve
+    for (int bl = g.rank(); bl < nb; bl += g.size()) {
+        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (f.body[kS32BodyFloats * bl + 7] == 0.0f) {
+            for (int e = f.bptr[bl]; e < f.bptr[bl + 1]; ++e) {
+                const uint32_t code = f.blist[e];
+                const int i = (int)(code >> 1), side = (int)(code & 1);
+                const double* Wk = a.ws.WJT + 48 * (size_t)order[i] + 6 * side;
+                for (int q = 0; q < 4; ++q) {
+                    const double xq = (double)f.c[kS32Floats * i + 12 * q + 11];
+                    for (int d = 0; d < 6; ++d) acc[d] = fma(Wk[12 * q + d], xq, acc[d]);
+                }
+            }
+        }
+        for (int d = 0; d < 6; ++d) w64[6 * bl + d] = acc[d];
+    }
+    g.sync();
+    double m = 0.0, xm = 0.0;
+    for (int i = g.rank(); i < K; i += g.size()) {
+        const size_t k = (size_t)order[i];
+        const uint32_t lh = f.lohi[i];
+        const int lo = (int)(lh & 0xffffu), hi = (int)(lh >> 16);
+        const double* wl = w64 + 6 * lo;
+        const double* wh = w64 + 6 * hi;
+        const float* wl32 = f.body + kS32BodyFloats * lo;
+        const float* wh32 = f.body + kS32BodyFloats * hi;
+        double z[4], x[4];
+        for (int q = 0; q < 4; ++q) {
+            const double* J = a.ws.J + 48 * k + 12 * q;
+            double v64 = a.ws.b[4 * k + q];
+            for (int c = 0; c < 6; ++c) v64 = fma(J[c], wl[c], v64);
+            for (int c = 0; c < 6; ++c) v64 = fma(J[6 + c], wh[c], v64);
+            float* row = f.c + kS32Floats * i + 12 * q;
+            const float v32 = s32_jw(row, q, wl32, wh32) + row[3];
+            row[3] += (float)(v64 - (double)v32);
+            x[q] = (double)row[11];
+            z[q] = x[q] - v64 / a.ws.diag[4 * k + q];
+        }
+        const double pn = z[0] > 0.0 ? z[0] : 0.0;
+        double fr[3];
+        prox_sphere(z[1], z[2], z[3], a.ws.mu[k], pn, fr);
+        const double d[4] = {x[0] - pn, x[1] - fr[0], x[2] - fr[1], x[3] - fr[2]};
+        for (int t = 0; t < 4; ++t) {
+            m = fmax(m, fabs(d[t]));
+            if (d[t] != d[t]) m = d[t];
+            xm = fmax(xm, fabs(x[t]));
+        }
+    }
+    const double mres = g.max(m);
+    const double mx = g.max(xm);
+    g.sync();
+    return mres / (mx > 1.0 ? mx : 1.0);
+}
+
 template <class G>
 __device__ __forceinline__ int team_next(const G& g, int* counter, int* slot) {
     int s = 0;
@@ -1628,17 +1693,29 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
         if (g.rank() == 0) a.ws.nlev[s] = L;
         float res = s32_residual(a, g, R, f);   // the warm-started iterate may already be good enough
         float best = res;
-        int sweeps = 0, stalls = 0;
-        while (res > tol && sweeps < budget) {
-            s32_sweep(g, f, L, rscale);
-            ++sweeps;
-            if (sweeps % interval == 0 || sweeps == budget) {
-                res = s32_residual(a, g, R, f);
-                // FP32 floor: hand over to FP64 once the residual, already small, stops improving.  Above
-                // the floor a pause is the Gauss-Seidel iteration itself (it is not monotone), so go on.
-                if (res < 0.95f * best) { best = res; stalls = 0; }
-                else if (best < kFp32Floor && ++stalls >= 3) break;
+        int sweeps = 0, stalls = 0, corrections = 0;
+        for (;;) {
+            while (res > tol && sweeps < budget) {
+                s32_sweep(g, f, L, rscale);
+                ++sweeps;
+                if (sweeps % interval == 0 || sweeps == budget) {
+                    res = s32_residual(a, g, R, f);
+                    // FP32 floor: hand over once the residual, already small, stops improving.  Above the
+                    // floor a pause is the Gauss-Seidel iteration itself (it is not monotone), so go on.
+                    if (res < 0.95f * best) { best = res; stalls = 0; }
+                    else if (best < kFp32Floor && ++stalls >= 3) break;
+                }
             }
+            // FP32 + refinement: test in FP64; if the FP32 answer misses the tolerance in FP64, correct the FP32
+            // problem's b by the FP64 defect and sweep on in FP32 (a few times at most)
+            if (a.pr.precision != RB_PRECISION_FP32_REFINE || sweeps >= budget || corrections >= kS32Corrections)
+                break;
+            const double r64 = s32_correct(a, g, R, f);
+            ++corrections;
+            if (r64 <= a.pr.residual_tolerance) break;
+            res = s32_residual(a, g, R, f);
+            best = res;
+            stalls = 0;
         }
         for (int t = g.rank(); t < 4 * K; t += g.size()) {   // back to contact order
             const int i = t >> 2, q = t & 3;
