@@ -1334,24 +1334,26 @@ struct S32Scene {
     uint32_t* blist;   // per body, its contacts in ascending order: level-order position << 1 | side (2K)
 };
 __host__ __device__ inline size_t s32_align(size_t v) { return (v + 15) & ~size_t(15); }
-// shared memory of a scene's FP32 copy; with contacts_in_l2 the contact rows live in global memory (L2)
-__host__ __device__ inline size_t s32_bytes(int K, int nb, bool contacts_in_l2 = false) {
-    return (contacts_in_l2 ? 0 : s32_align(sizeof(float) * (size_t)K * kS32Floats)) +
+// shared memory of a scene's FP32 copy; with in_l2 the contact rows, the level-order positions and the
+// per-body contact lists live in global memory (L2) and only the bodies, body indices and level and list
+// starts stay on chip
+__host__ __device__ inline size_t s32_bytes(int K, int nb, bool in_l2 = false) {
+    return (in_l2 ? 0 : s32_align(sizeof(float) * (size_t)K * kS32Floats) + s32_align(sizeof(uint16_t) * (size_t)K) +
+                        s32_align(sizeof(uint32_t) * 2 * (size_t)K)) +
            s32_align(sizeof(float) * (size_t)nb * kS32BodyFloats) + s32_align(sizeof(uint32_t) * (size_t)K) +
-           s32_align(sizeof(uint16_t) * (size_t)K) + s32_align(sizeof(uint16_t) * (size_t)(K + 1)) +
-           s32_align(sizeof(uint16_t) * (size_t)(nb + 1)) + s32_align(sizeof(uint32_t) * 2 * (size_t)K);
+           s32_align(sizeof(uint16_t) * (size_t)(K + 1)) + s32_align(sizeof(uint16_t) * (size_t)(nb + 1));
 }
-__device__ __forceinline__ S32Scene s32_carve(char* base, int K, int nb, float* c_global = nullptr) {
+__device__ __forceinline__ S32Scene s32_carve(char* base, int K, int nb, const StepArgs* l2 = nullptr, int c0 = 0) {
     S32Scene f;
     size_t o = 0;
     auto take = [&](size_t bytes) { char* p = base + o; o += s32_align(bytes); return p; };
-    f.c = c_global ? c_global : (float*)take(sizeof(float) * (size_t)K * kS32Floats);
+    f.c = l2 ? l2->ws.c32 + kS32Floats * (size_t)c0 : (float*)take(sizeof(float) * (size_t)K * kS32Floats);
     f.body = (float*)take(sizeof(float) * (size_t)nb * kS32BodyFloats);
     f.lohi = (uint32_t*)take(sizeof(uint32_t) * (size_t)K);
-    f.pos = (uint16_t*)take(sizeof(uint16_t) * (size_t)K);
+    f.pos = l2 ? l2->ws.pos32 + c0 : (uint16_t*)take(sizeof(uint16_t) * (size_t)K);
     f.lptr = (uint16_t*)take(sizeof(uint16_t) * (size_t)(K + 1));
     f.bptr = (uint16_t*)take(sizeof(uint16_t) * (size_t)(nb + 1));
-    f.blist = (uint32_t*)take(sizeof(uint32_t) * 2 * (size_t)K);
+    f.blist = l2 ? l2->ws.blist32 + 2 * (size_t)c0 : (uint32_t*)take(sizeof(uint32_t) * 2 * (size_t)K);
     return f;
 }
 
@@ -1496,7 +1498,7 @@ __device__ __forceinline__ float s32_residual(const StepArgs& a, const G& g, con
 // update from the four rows' float4 group it owns (lin for q = 0, 1; ang_lo for 2; ang_hi for 3) and applies
 // +m^-1, -m^-1, I_lo^-1 or I_hi^-1 to it.  Every lane runs the same instructions (lane-dependent offsets);
 // all shared-memory reads are float4 / float2.
-template <class G>
+template <class G, bool kL2>
 __device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, float rscale) {
     const int q = g.rank() & 3, slot = g.rank() >> 2, nslot = g.size() >> 2;
     const int base = (threadIdx.x & 31) & ~3;
@@ -1507,6 +1509,12 @@ __device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, 
     int start = f.lptr[0], end = f.lptr[1];
     for (int l = 1; l <= L; ++l) {
         const int next_end = l < L ? f.lptr[l + 1] : end;
+        if (kL2) {   // rows in L2: pull the next level's rows (contiguous in level order) into L1 meanwhile
+            const char* p0 = reinterpret_cast<const char*>(f.c + kS32Floats * (size_t)end);
+            const int lines = (int)(((size_t)(next_end - end) * kS32Floats * sizeof(float) + 127) / 128);
+            for (int t = g.rank(); t < lines; t += g.size())
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(p0 + 128 * (size_t)t));
+        }
         // every lane of a quad runs the same trip count, so the quad's shuffles see all four lanes
         for (int i0 = start; i0 < end; i0 += nslot) {
             const int i = i0 + slot;
@@ -1688,7 +1696,7 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
             const size_t bytes = s32_bytes(K, nb);
             if (bytes <= lo_bytes || bytes > slab) continue;
         }
-        const S32Scene f = s32_carve(my_slab, K, nb, kL2 ? a.ws.c32 + kS32Floats * (size_t)R.c0 : nullptr);
+        const S32Scene f = s32_carve(my_slab, K, nb, kL2 ? &a : nullptr, R.c0);
         const int L = s32_load(a, g, R, s, f, coloured);
         if (g.rank() == 0) a.ws.nlev[s] = L;
         float res = s32_residual(a, g, R, f);   // the warm-started iterate may already be good enough
@@ -1696,7 +1704,7 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
         int sweeps = 0, stalls = 0, corrections = 0;
         for (;;) {
             while (res > tol && sweeps < budget) {
-                s32_sweep(g, f, L, rscale);
+                s32_sweep<G, kL2>(g, f, L, rscale);
                 ++sweeps;
                 if (sweeps % interval == 0 || sweeps == budget) {
                     res = s32_residual(a, g, R, f);

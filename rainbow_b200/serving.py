@@ -393,18 +393,24 @@ class Server:
         now = time.perf_counter()
         for r in admitted:
             r.admitted = now
+        relayout_s = 0.0
         if admitted or len(staying) != len(self.active):
+            t1 = time.perf_counter()
             if staying or admitted:
                 self._relayout(staying, admitted)
             else:
                 self.batch, self.active = None, []
+            relayout_s = time.perf_counter() - t1
         if not self.active:
             return []
         stream = torch.cuda.current_stream(self.device)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        caps0 = (self.batch.caps.pair_capacity, self.batch.caps.item_capacity, self.batch.caps.contact_capacity)
         e0.record(stream)
         status = self.batch.step(self.rp)
         e1.record(stream)
+        grown = caps0 != (self.batch.caps.pair_capacity, self.batch.caps.item_capacity,
+                          self.batch.caps.contact_capacity)
         if status & N.STATUS_NONFINITE:
             raise N.NativeError("the step produced a non-finite body state")
         done = []
@@ -421,7 +427,8 @@ class Server:
             r.tick_device.append(dev_ms)
         self.ticks.append({"wall_s": wall, "device_ms": dev_ms, "scenes": len(self.active),
                            "bodies": self.batch.n_bodies, "admitted": len(admitted), "finished": len(done),
-                           "queued": len(self.queue)})
+                           "queued": len(self.queue), "grown": grown,
+                           "relayout_s": relayout_s})
         self.finished.extend(done)
         return done
 
