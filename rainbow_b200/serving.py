@@ -179,21 +179,28 @@ class ServingBatch(W.DeviceWorld):
     ``prev`` (the batch this one replaces) and ``body_map`` (old body -> new body or -1) carry the staying
     scenes' state and warm-start cache; bodies beyond the carried ones start from their block's initial state."""
 
-    def __init__(self, library, blocks, device, caps, max_iterations, prev=None, body_map=None, n_kept=0):
+    def __init__(self, library, blocks, device, caps, max_iterations, prev=None, body_map=None, n_kept=0,
+                 pool=None):
+        t0 = time.perf_counter()
+        # device buffers reused from batch to batch (grow-only), so a re-layout allocates nothing in the
+        # steady state; the warm-start cache alternates between two slots (the old one feeds rb_repack)
+        self.pool = pool if pool is not None else {}
+        self.cache_slot = 1 - prev.cache_slot if prev is not None else 0
         self.lib = N.load()
         self.device = torch.device(device)
         self.n_scenes = len(blocks)
         library.sync()
         P = pack_blocks(blocks, library)
+        t1 = time.perf_counter()
         dev = self.device
         T = {k: torch.from_numpy(np.ascontiguousarray(P[k])).to(dev, dt) for k, dt in _BODY_TENSORS.items()}
         nbod = P["n_bodies"]
         for k, n in (("body_v0", nbod + 1), ("body_t0", nbod + 1), ("body_c0", nbod + 1),
                      ("vert_body", P["n_body_vertices"]), ("tri_body", P["n_body_triangles"]),
                      ("clu_body", P["n_clusters"])):
-            T[k] = torch.empty(max(1, n), dtype=torch.int32, device=dev)
-        T["x"] = torch.empty(7 * nbod, dtype=torch.float64, device=dev)
-        T["u"] = torch.empty(6 * nbod, dtype=torch.float64, device=dev)
+            T[k] = self._pooled(k, max(1, n), torch.int32)
+        T["x"] = self._pooled("x%d" % self.cache_slot, 7 * nbod, torch.float64)   # the old state feeds rb_repack
+        T["u"] = self._pooled("u%d" % self.cache_slot, 6 * nbod, torch.float64)
         self.tensors = T
         self.t_x, self.t_u = T["x"], T["u"]
         self.packed = P
@@ -221,7 +228,9 @@ class ServingBatch(W.DeviceWorld):
         self.caps = N.RbCaps()
         self.caps.max_iterations = max(1, int(max_iterations))
         self.caps.pair_capacity, self.caps.item_capacity, self.caps.contact_capacity = caps
-        W.DeviceWorld._alloc(self)
+        t2 = time.perf_counter()
+        self._alloc()
+        t3 = time.perf_counter()
         # state: carried rows of the staying bodies, initial rows of the new ones
         if prev is not None and n_kept > 0:
             tmap = torch.from_numpy(np.ascontiguousarray(body_map, np.int32)).to(dev)
@@ -243,6 +252,53 @@ class ServingBatch(W.DeviceWorld):
             hu = torch.from_numpy(np.ascontiguousarray(np.concatenate([b.u0 for b in new]).reshape(-1)))
             self.t_x[7 * kept_bodies:].copy_(hx.pin_memory(), non_blocking=True)
             self.t_u[6 * kept_bodies:].copy_(hu.pin_memory(), non_blocking=True)
+        # host seconds of the re-layout: packing, uploads and topology, work-list allocation, state carry
+        self.relayout_times = (t1 - t0, t2 - t1, t3 - t2, time.perf_counter() - t3)
+
+    def _pooled(self, name, n, dtype):
+        t = self.pool.get(name)
+        if t is None or t.numel() < n:
+            t = torch.empty(int(1.25 * n) + 1024, dtype=dtype, device=self.device)
+            self.pool[name] = t
+        return t[:n]
+
+    def _alloc(self):
+        """DeviceWorld._alloc with the server's pooled buffers (outputs are written by every step, so the
+        reused buffers need no clearing)."""
+        K = self.caps.contact_capacity
+        self.t_cids = self._pooled("cids", 2 * K, torch.int32)
+        self.t_cp = self._pooled("cp", 3 * K, torch.float64)
+        self.t_cn = self._pooled("cn", 3 * K, torch.float64)
+        self.t_cg = self._pooled("cg", K, torch.float64)
+        self.t_csol = self._pooled("csol", 4 * K, torch.float64)
+        self.t_stats = torch.zeros(self.n_scenes * ctypes.sizeof(N.RbSceneStats), dtype=torch.uint8,
+                                   device=self.device)
+        self.t_resid = self._pooled("resid", self.n_scenes * self.caps.max_iterations, torch.float64)
+        self.t_status = torch.zeros(8, dtype=torch.int32, device=self.device)
+        old_key, old_sol = getattr(self, "t_cache_key", None), getattr(self, "t_cache_sol", None)
+        key = self._pooled("cache_key%d" % self.cache_slot, 2 * K, torch.int64)
+        sol = self._pooled("cache_sol%d" % self.cache_slot, 4 * K, torch.float64)
+        if old_key is not None and old_key.data_ptr() != key.data_ptr():   # grown within this batch
+            n = min(old_key.numel(), key.numel()) // 2
+            key[:2 * n].copy_(old_key[:2 * n])
+            sol[:4 * n].copy_(old_sol[:4 * n])
+        self.t_cache_key, self.t_cache_sol = key, sol
+        if not hasattr(self, "t_cache_count"):
+            self.t_cache_count = torch.zeros(1, dtype=torch.int32, device=self.device)
+        out = N.RbOutputs()
+        out.contact_ids, out.contact_p, out.contact_n = self.t_cids.data_ptr(), self.t_cp.data_ptr(), self.t_cn.data_ptr()
+        out.contact_g, out.contact_sol = self.t_cg.data_ptr(), self.t_csol.data_ptr()
+        out.stats, out.residuals = self.t_stats.data_ptr(), self.t_resid.data_ptr()
+        out.status, out.n_contacts_total = self.t_status.data_ptr(), self.t_status.data_ptr() + 4
+        out.needed = self.t_status.data_ptr() + 8
+        out.cache_key, out.cache_sol = self.t_cache_key.data_ptr(), self.t_cache_sol.data_ptr()
+        out.cache_count = self.t_cache_count.data_ptr()
+        self.rb_outputs = out
+        nbytes = ctypes.c_size_t(0)
+        N.check(self.lib.rb_workspace_bytes(ctypes.byref(self.rb_bodies), ctypes.byref(self.caps), ctypes.byref(nbytes)),
+                "rb_workspace_bytes")
+        self.workspace_bytes = int(nbytes.value)
+        self.t_ws = self._pooled("ws", self.workspace_bytes, torch.uint8)
 
     def scene_state(self, s):
         """(x, u) rows of scene s on the host."""
@@ -285,6 +341,7 @@ class Server:
         self.max_active_bodies = max_active_bodies
         self.caps_per_body = list(caps_per_body)
         self.library = ShapeLibrary(device)
+        self.pool = {}
         self.queue = deque()
         self.active = []
         self.batch = None
@@ -377,7 +434,8 @@ class Server:
                                                                          prev.caps.item_capacity,
                                                                          prev.caps.contact_capacity)))
         batch = ServingBatch(self.library, [r.block for r in scenes], self.device, caps, self.max_iterations,
-                             prev=prev, body_map=body_map, n_kept=len(staying) if prev is not None else 0)
+                             prev=prev, body_map=body_map, n_kept=len(staying) if prev is not None else 0,
+                             pool=self.pool)
         for i, r in enumerate(scenes):
             r.slot = i
         self.batch = batch
@@ -428,7 +486,8 @@ class Server:
         self.ticks.append({"wall_s": wall, "device_ms": dev_ms, "scenes": len(self.active),
                            "bodies": self.batch.n_bodies, "admitted": len(admitted), "finished": len(done),
                            "queued": len(self.queue), "grown": grown,
-                           "relayout_s": relayout_s})
+                           "relayout_s": relayout_s,
+                           "relayout_parts_s": self.batch.relayout_times if relayout_s else None})
         self.finished.extend(done)
         return done
 
