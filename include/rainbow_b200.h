@@ -167,6 +167,13 @@ typedef struct rb_params {
                                      reference always starts from zero (contacts.py:53), so this is off for
                                      parity runs */
     int32_t ordering;             /* RB_ORDER_*: contact visiting order of the Gauss-Seidel schemes */
+    /* launch shapes (0 = built-in value); they change speed only, never results */
+    int32_t fp32_small_slab;      /* bytes of a warp team's slab in the FP32 solve's small class (28672);
+                                     multiple of 16, 4096 .. fp32_mid_slab - 16 */
+    int32_t fp32_mid_slab;        /* bytes of a warp team's slab in the mid class (57344), at most 57344 */
+    int32_t mid_blocks;           /* blocks of the triangle-candidate search (2368) */
+    int32_t narrow_blocks;        /* blocks of the Frank-Wolfe contact search (1184) */
+    int32_t narrow_threads;       /* threads per contact-search block: 64, 128 or 256 (256) */
 } rb_params;
 
 /* Per-scene results of one step. */

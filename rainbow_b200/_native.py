@@ -64,6 +64,8 @@ class RbParams(ctypes.Structure):
         ("termination", _i32), ("residual_tolerance", ctypes.c_double), ("profiling", _i32),
         ("relaxation", ctypes.c_double), ("residual_interval", _i32), ("precision", _i32),
         ("refine_iterations", _i32), ("warm_start", _i32), ("ordering", _i32),
+        ("fp32_small_slab", _i32), ("fp32_mid_slab", _i32), ("mid_blocks", _i32), ("narrow_blocks", _i32),
+        ("narrow_threads", _i32),
     ]
 
 

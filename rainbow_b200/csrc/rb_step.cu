@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <algorithm>
 #include <atomic>
 #include <cstring>
 #include <mutex>
@@ -2041,6 +2042,17 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
         return fail(RB_ERR_UNSUPPORTED, "rb_step: unknown solver scheme");
     if (pr->ordering != RB_ORDER_SERIAL && pr->ordering != RB_ORDER_COLOURED)
         return fail(RB_ERR_ARG, "rb_step: unknown contact ordering");
+    // launch shapes
+    const int small_slab = pr->fp32_small_slab > 0 ? pr->fp32_small_slab : kS32SmallSlab;
+    const int mid_slab = pr->fp32_mid_slab > 0 ? pr->fp32_mid_slab : kS32MidSlab;
+    const int mid_blocks = pr->mid_blocks > 0 ? pr->mid_blocks : 148 * 16;
+    const int narrow_blocks = pr->narrow_blocks > 0 ? pr->narrow_blocks : 148 * 8;
+    const int narrow_threads = pr->narrow_threads > 0 ? pr->narrow_threads : 256;
+    if (small_slab % 16 || mid_slab % 16 || small_slab < 4096 || small_slab >= mid_slab || mid_slab > kS32MidSlab)
+        return fail(RB_ERR_ARG, "rb_step: FP32 slabs must be multiples of 16 with 4096 <= small < mid <= 57344");
+    if (mid_blocks > 65535 || narrow_blocks > 65535 ||
+        (narrow_threads != 64 && narrow_threads != 128 && narrow_threads != 256))
+        return fail(RB_ERR_ARG, "rb_step: launch shape out of range");
     if (pr->max_iterations < 0 || pr->max_iterations > caps->max_iterations)
         return fail(RB_ERR_ARG, "rb_step: max_iterations exceeds rb_caps.max_iterations");
     if (!(pr->dt > 0.0)) return fail(RB_ERR_ARG, "rb_step: dt must be positive");
@@ -2089,12 +2101,12 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     {
         const int max_clusters = (sh->max_shape_triangles + 31) / 32;
         const size_t mid_smem = (size_t)kWarpsPerBlock * 3 * sizeof(uint32_t) * (max_clusters > 0 ? max_clusters : 1);
-        k_mid<<<148 * 16, kBlock, mid_smem, st>>>(a, max_clusters > 0 ? max_clusters : 1); note_launch();
+        k_mid<<<mid_blocks, kBlock, mid_smem, st>>>(a, max_clusters > 0 ? max_clusters : 1); note_launch();
     }
     k_check<<<1, 1, 0, st>>>(a.ws.counters, kNItems, caps->item_capacity, RB_STATUS_ITEM_OVERFLOW, out->status); note_launch();
     prof_mark(prof, 2, st);
     // narrow phase
-    k_narrow<<<G, 256, 0, st>>>(a); note_launch();
+    k_narrow<<<narrow_blocks, narrow_threads, 0, st>>>(a); note_launch();
     prof_mark(prof, 3, st);
     // reduction and compaction
     k_dedup<false><<<G, kBlock, 0, st>>>(a); note_launch();
@@ -2132,11 +2144,14 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
         k_solve_fp32<BlockGroup, true><<<148, kFp32BlockMax, (size_t)kFp32LargeSmem, ss->s[3]>>>(
             a, kQueueFp32 + 3, kFp32LargeSmem, kFp32LargeSmem); note_launch();
         k_solve_fp32<BlockGroup, false><<<148, kFp32Block, (size_t)kFp32LargeSmem, ss->s[2]>>>(
-            a, kQueueFp32 + 2, kS32MidSlab, kFp32LargeSmem); note_launch();
-        k_solve_fp32<WarpGroup, false><<<148, kFp32Block, 4 * (size_t)kS32MidSlab, ss->s[1]>>>(
-            a, kQueueFp32 + 1, kS32SmallSlab, kS32MidSlab); note_launch();
-        k_solve_fp32<WarpGroup, false><<<2 * 148, kFp32Block, 4 * (size_t)kS32SmallSlab, ss->s[0]>>>(
-            a, kQueueFp32, 0, kS32SmallSlab); note_launch();
+            a, kQueueFp32 + 2, mid_slab, kFp32LargeSmem); note_launch();
+        // blocks per SM that the shared memory (227 KB) and the threads (2048) allow
+        const int small_per_sm = std::min(16, (227 * 1024) / (4 * small_slab));
+        const int mid_per_sm = std::max(1, std::min(16, (227 * 1024) / (4 * mid_slab)));
+        k_solve_fp32<WarpGroup, false><<<148 * mid_per_sm, kFp32Block, 4 * (size_t)mid_slab, ss->s[1]>>>(
+            a, kQueueFp32 + 1, small_slab, mid_slab); note_launch();
+        k_solve_fp32<WarpGroup, false><<<148 * small_per_sm, kFp32Block, 4 * (size_t)small_slab, ss->s[0]>>>(
+            a, kQueueFp32, 0, small_slab); note_launch();
         for (int c = 0; c < kSideStreams; ++c) {
             cudaEventRecord(ss->join[c], ss->s[c]);
             cudaStreamWaitEvent(st, ss->join[c], 0);
