@@ -180,7 +180,7 @@ class ServingBatch(W.DeviceWorld):
     scenes' state and warm-start cache; bodies beyond the carried ones start from their block's initial state."""
 
     def __init__(self, library, blocks, device, caps, max_iterations, prev=None, body_map=None, n_kept=0,
-                 pool=None):
+                 pool=None, packed=None):
         t0 = time.perf_counter()
         # device buffers reused from batch to batch (grow-only), so a re-layout allocates nothing in the
         # steady state; the warm-start cache alternates between two slots (the old one feeds rb_repack)
@@ -190,7 +190,7 @@ class ServingBatch(W.DeviceWorld):
         self.device = torch.device(device)
         self.n_scenes = len(blocks)
         library.sync()
-        P = pack_blocks(blocks, library)
+        P = packed if packed is not None else pack_blocks(blocks, library)
         t1 = time.perf_counter()
         dev = self.device
         T = {k: torch.from_numpy(np.ascontiguousarray(P[k])).to(dev, dt) for k, dt in _BODY_TENSORS.items()}
@@ -342,6 +342,7 @@ class Server:
         self.caps_per_body = list(caps_per_body)
         self.library = ShapeLibrary(device)
         self.pool = {}
+        self._next = None          # the next tick's plan, made while the current step runs
         self.queue = deque()
         self.active = []
         self.batch = None
@@ -359,8 +360,9 @@ class Server:
         return uid
 
     def idle(self):
-        """True when nothing is queued and every resident scene has finished its horizon."""
-        return not self.queue and all(r.done >= r.horizon for r in self.active)
+        """True when nothing is queued or planned and every resident scene has finished its horizon."""
+        planned = self._next is not None and bool(self._next[1])
+        return not self.queue and not planned and all(r.done >= r.horizon for r in self.active)
 
     def _bytes_for(self, n_bodies, n_scenes, nv, nt, nc):
         """Device bytes of a batch of this size: workspace, outputs, cache and body arrays."""
@@ -414,7 +416,7 @@ class Server:
                 counts[k] += cnt[k]
         return admitted
 
-    def _relayout(self, staying, admitted):
+    def _relayout(self, staying, admitted, packed=None):
         """New batch of staying + admitted scenes, carrying the staying scenes' state and cache."""
         prev = self.batch
         body_map = None
@@ -435,27 +437,42 @@ class Server:
                                                                          prev.caps.contact_capacity)))
         batch = ServingBatch(self.library, [r.block for r in scenes], self.device, caps, self.max_iterations,
                              prev=prev, body_map=body_map, n_kept=len(staying) if prev is not None else 0,
-                             pool=self.pool)
+                             pool=self.pool, packed=packed)
         for i, r in enumerate(scenes):
             r.slot = i
         self.batch = batch
         self.active = scenes
 
     # ---------------------------------------------------------------------------------------------------------
-    def tick(self):
-        """Admit, re-lay out if the membership changed, step every resident scene once, retire the finished.
-        Returns the requests finished in this tick."""
-        t0 = time.perf_counter()
-        staying = [r for r in self.active if r.done < r.horizon]
+    def _plan(self, staying):
+        """Membership of the next tick: the staying scenes plus the queued ones admitted now, and, when it
+        differs from the current one, the host arrays of its layout."""
         admitted = self._admit(staying)
         now = time.perf_counter()
         for r in admitted:
             r.admitted = now
+        changed = bool(admitted) or len(staying) != len(self.active)
+        packed = None
+        if changed and (staying or admitted):
+            self.library.sync()
+            packed = pack_blocks([r.block for r in staying + admitted], self.library)
+        return staying, admitted, changed, packed
+
+    def tick(self):
+        """Re-lay out if the membership changed, step every resident scene once, retire the finished.
+
+        The next tick's admissions and host-side packing are done while this tick's step runs on the GPU, so
+        the host work of continuous batching overlaps the device work.  Returns the requests finished in
+        this tick."""
+        t0 = time.perf_counter()
+        plan = self._next if self._next is not None else self._plan([r for r in self.active if r.done < r.horizon])
+        self._next = None
+        staying, admitted, changed, packed = plan
         relayout_s = 0.0
-        if admitted or len(staying) != len(self.active):
+        if changed:
             t1 = time.perf_counter()
             if staying or admitted:
-                self._relayout(staying, admitted)
+                self._relayout(staying, admitted, packed)
             else:
                 self.batch, self.active = None, []
             relayout_s = time.perf_counter() - t1
@@ -464,9 +481,17 @@ class Server:
         stream = torch.cuda.current_stream(self.device)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         caps0 = (self.batch.caps.pair_capacity, self.batch.caps.item_capacity, self.batch.caps.contact_capacity)
+        self.batch.t_status.zero_()
         e0.record(stream)
-        status = self.batch.step(self.rp)
+        self.batch.launch(self.rp)
         e1.record(stream)
+        # meanwhile on the host: who stays after this step, who joins, and the next layout's arrays
+        self._next = self._plan([r for r in self.active if r.done + 1 < r.horizon])
+        status = int(self.batch.t_status[0].item())   # waits for the step
+        if status & (N.STATUS_PAIR_OVERFLOW | N.STATUS_ITEM_OVERFLOW | N.STATUS_CONTACT_OVERFLOW):
+            self.batch._grow(status)                  # the step left the state alone: grow and repeat it
+            status = self.batch.step(self.rp)
+            e1.record(stream)
         grown = caps0 != (self.batch.caps.pair_capacity, self.batch.caps.item_capacity,
                           self.batch.caps.contact_capacity)
         if status & N.STATUS_NONFINITE:
