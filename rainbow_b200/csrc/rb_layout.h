@@ -62,6 +62,7 @@ struct Workspace {
     int32_t* cpred;      // 2K  previous contact on the same (non-fixed) body, per side, or -1
     int32_t* sweeps32;   // S   FP32 sweeps done per scene (-1: the scene is solved in FP64 only)
     int32_t* nlev;       // S   levels (or colours) the FP32 phase found for the scene
+    double* eterm;       // 2N  kinetic and potential energy of each body (profiled steps)
     // scans and counters
     int32_t* scan_tmp;   // kScanBlocks + 1
     int32_t* counters;   // 16
@@ -97,7 +98,7 @@ inline size_t layout(Workspace* ws, char* base, int64_t N, int64_t NV, int64_t N
     take(w->ckey, 2 * K);
     take(w->lev_of, K); take(w->lev_order, K); take(w->lev_ptr, K + S + 1); take(w->lev_cur, K + S + 1);
     take(w->cpred, 2 * K);
-    take(w->sweeps32, S); take(w->nlev, S);
+    take(w->sweeps32, S); take(w->nlev, S); take(w->eterm, 2 * N);
     take(w->scan_tmp, kScanBlocks + 1); take(w->counters, 16);
     return off;
 }

@@ -1862,28 +1862,51 @@ __global__ void k_scene_summary(const StepArgs a) {
             for (int i = 0; i < 3; ++i) G[i] = G[i] + fp[1 + i] * fp[0];
             has_gravity = 1;
         }
+    // the per-body terms come from k_body_energy; summed here in body order (state_storage.py:188-237)
     double kinetic = 0.0, potential = 0.0;
     for (int b = R.b0; b < R.b1; ++b) {
         if (a.bd.fixed[b]) continue;
-        const double* xb = a.bd.x + 7 * b;
-        double Rm[9], Iw[9], Ib[3] = {a.bd.inertia[3 * b], a.bd.inertia[3 * b + 1], a.bd.inertia[3 * b + 2]};
-        quat_to_matrix(xb + 3, Rm);
-        update_inertia_tensor(Rm, Ib, Iw);
-        const double m = a.bd.mass[b];
-        if (has_gravity) {
-            const d3 Gv = d3{G[0], G[1], G[2]};
-            const double ln = norm3_np(Gv);
-            const d3 up = d3{G[0] / ln, G[1] / ln, G[2] / ln};
-            const double g = norm3_np(Gv);
-            const double h = dot3_np(up, ld3(xb));
-            potential += m * g * h;
-        }
-        const d3 v = ld3(a.bd.u + 6 * b), w = ld3(a.bd.u + 6 * b + 3);
-        const double wIw = dot3_np(w, gemv3_np(Iw, w));
-        kinetic += 0.5 * (m * dot3_np(v, v) + wIw);
+        if (has_gravity) potential += a.ws.eterm[2 * (size_t)b + 1];
+        kinetic += a.ws.eterm[2 * (size_t)b];
     }
     st->kinetic_energy = kinetic;
     st->potential_energy = potential;
+}
+
+// per-body energy terms of a profiled step (StateStorage.compute_total_energy, state_storage.py:188-237):
+// 0.5 (m v.v + w.(I_w w)) and m g (up . r) with the scene's summed gravity
+__global__ void k_body_energy(const StepArgs a) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= a.bd.n_bodies || a.ws.counters[kAbort]) return;
+    double* out = a.ws.eterm + 2 * (size_t)b;
+    if (a.bd.fixed[b]) { out[0] = 0.0; out[1] = 0.0; return; }
+    const int s = scene_of(a.bd.scene_start, a.bd.n_scenes, b);
+    double G[3] = {0.0, 0.0, 0.0};
+    int has_gravity = 0;
+    for (int f = a.bd.scene_force_start[s]; f < a.bd.scene_force_start[s + 1]; ++f)
+        if (a.bd.force_kind[f] == 0) {
+            const double* fp = a.bd.force_params + 4 * f;
+            for (int i = 0; i < 3; ++i) G[i] = G[i] + fp[1 + i] * fp[0];
+            has_gravity = 1;
+        }
+    const double* xb = a.bd.x + 7 * b;
+    double Rm[9], Iw[9], Ib[3] = {a.bd.inertia[3 * b], a.bd.inertia[3 * b + 1], a.bd.inertia[3 * b + 2]};
+    quat_to_matrix(xb + 3, Rm);
+    update_inertia_tensor(Rm, Ib, Iw);
+    const double m = a.bd.mass[b];
+    double pot = 0.0;
+    if (has_gravity) {
+        const d3 Gv = d3{G[0], G[1], G[2]};
+        const double ln = norm3_np(Gv);
+        const d3 up = d3{G[0] / ln, G[1] / ln, G[2] / ln};
+        const double g = norm3_np(Gv);
+        const double h = dot3_np(up, ld3(xb));
+        pot = m * g * h;
+    }
+    const d3 v = ld3(a.bd.u + 6 * b), w = ld3(a.bd.u + 6 * b + 3);
+    const double wIw = dot3_np(w, gemv3_np(Iw, w));
+    out[0] = 0.5 * (m * dot3_np(v, v) + wIw);
+    out[1] = pot;
 }
 
 // keep this step's contact keys and impulses for the next step's warm start
@@ -2167,6 +2190,7 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
         k_solve_blocks<<<bg, kSolveBlock, block_smem, st>>>(a, 1, warp_bodies, smem_bodies); note_launch();
         k_post_apply<<<blocks_for(N, 128), 128, 0, st>>>(a); note_launch();
     }
+    if (prof) { k_body_energy<<<blocks_for(N, 128), 128, 0, st>>>(a); note_launch(); }
     k_scene_summary<<<blocks_for(bd->n_scenes, 64), 64, 0, st>>>(a); note_launch();
     k_cache_store<<<G, 256, 0, st>>>(a); note_launch();
     k_finish<<<1, 1, 0, st>>>(a); note_launch();
