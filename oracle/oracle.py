@@ -49,6 +49,7 @@ class OScene(ctypes.Structure):
         ("n_bodies", ctypes.c_int32), ("body_shape", _i32), ("mass", _d), ("inertia", _d), ("fixed", _u8),
         ("material", _i32), ("n_forces", ctypes.c_int32), ("force_kind", _i32), ("force_params", _d),
         ("body_force_order", _i32), ("n_materials", ctypes.c_int32), ("material_mu", _d), ("material_eps", _d),
+        ("n_hinges", ctypes.c_int32), ("hinge_bodies", _i32), ("hinge_frames", _d),
     ]
 
 
@@ -62,6 +63,7 @@ class OStepOut(ctypes.Structure):
         ("ids", _i32), ("p", _d), ("n", _d), ("g", _d), ("b", _d), ("diag", _d), ("sol", _d),
         ("residuals", _d), ("delta_u_ext", _d),
         ("kinetic", ctypes.c_double), ("potential", ctypes.c_double), ("max_penetration", ctypes.c_double),
+        ("hinge_b", _d), ("hinge_diag", _d), ("hinge_sol", _d),
     ]
 
 
@@ -240,6 +242,12 @@ class OracleScene:
         s.n_materials = int(len(a["material_epsilon"]))
         s.material_mu = _ptr(keep(a["material_mu"], np.float64), _d)
         s.material_eps = _ptr(keep(a["material_epsilon"], np.float64), _d)
+        hb = np.asarray(a["hinge_bodies"], np.int32).reshape(-1, 2) if "hinge_bodies" in a else np.zeros((0, 2))
+        self.n_hinges = int(len(hb))
+        s.n_hinges = self.n_hinges
+        s.hinge_bodies = _ptr(keep(hb if len(hb) else np.zeros((1, 2)), np.int32), _i32)
+        hf = np.asarray(a["hinge_frames"], np.float64).reshape(-1, 12) if self.n_hinges else np.zeros((1, 12))
+        s.hinge_frames = _ptr(keep(hf, np.float64), _d)
         self.params = np.ascontiguousarray(a["params"], dtype=np.float64).copy()
         self.r = np.ascontiguousarray(a["body_r"], dtype=np.float64).copy()
         self.q = np.ascontiguousarray(a["body_q"], dtype=np.float64).copy()
@@ -264,6 +272,10 @@ class OracleScene:
         bufs = dict(ids=np.zeros((cap, 2), np.int32), p=np.zeros((cap, 3)), n=np.zeros((cap, 3)), g=np.zeros(cap),
                     b=np.zeros(4 * cap), diag=np.zeros(4 * cap), sol=np.zeros(4 * cap),
                     residuals=np.full(max(1, max_it), np.inf), delta_u_ext=np.zeros(6 * self.n_bodies))
+        H = max(1, self.n_hinges)
+        bufs.update(hinge_b=np.zeros(5 * H), hinge_diag=np.zeros(5 * H), hinge_sol=np.zeros(5 * H))
+        for k in ("hinge_b", "hinge_diag", "hinge_sol"):
+            setattr(out, k, _ptr(bufs[k], _d))
         out.ids = _ptr(bufs["ids"], _i32)
         for k in ("p", "n", "g", "b", "diag", "sol", "residuals", "delta_u_ext"):
             setattr(out, k, _ptr(bufs[k], _d))
@@ -278,6 +290,9 @@ class OracleScene:
             raise RuntimeError("ContactPoint.init() was called with non-unit size normal")
         if rc == 1:
             raise RuntimeError("oracle contact capacity %d exceeded (%d contacts)" % (cap, out.n_contacts))
+        if rc == 4:
+            raise NotImplementedError("hinge joints are solved with the reference stepper's rule only "
+                                      "(rigid Gauss-Seidel, merit termination, serial order)")
         K = out.n_contacts
         return dict(
             n_contacts=K, ids=bufs["ids"][:K].copy(), p=bufs["p"][:K].copy(), n=bufs["n"][:K].copy(),
@@ -288,5 +303,7 @@ class OracleScene:
             n_overlap_pairs=out.n_overlap_pairs, n_leaf_overlaps=out.n_leaf_overlaps,
             n_candidates=out.n_candidates, n_colours=out.n_colours, kinetic=out.kinetic, potential=out.potential,
             max_penetration=out.max_penetration,
+            hinge_b=bufs["hinge_b"][:5 * self.n_hinges].copy(), hinge_diag=bufs["hinge_diag"][:5 * self.n_hinges].copy(),
+            hinge_sol=bufs["hinge_sol"][:5 * self.n_hinges].copy(),
             x=np.concatenate([self.r, self.q], axis=1).ravel(), u=np.concatenate([self.v, self.w], axis=1).ravel(),
         )

@@ -247,6 +247,9 @@ typedef struct {
     int32_t n_materials;
     const double* material_mu;                    /* M x M x 3 */
     const double* material_eps;                   /* M x M */
+    int32_t n_hinges;                             /* engine.hinges in Hinge.idx order */
+    const int32_t* hinge_bodies;                  /* 2 per hinge: parent, child */
+    const double* hinge_frames;                   /* 12 per hinge: arm_p, arm_c, axis_p, axis_c (body frames) */
 } OScene;
 
 /* Parameter vector order (Parameters fields, types.py:356-418) */
@@ -278,6 +281,7 @@ typedef struct {
     double* residuals;           /* max_iterations */
     double* delta_u_ext;         /* 6 per body */
     double kinetic, potential, max_penetration;
+    double* hinge_b; double* hinge_diag; double* hinge_sol;   /* 5 per hinge (NULL: not recorded) */
 } OStepOut;
 
 typedef struct { double lo[3], hi[3]; } AABB;
@@ -794,6 +798,177 @@ int rbo_colour_contacts(int K, int N, const int32_t* ids, const uint8_t* fixed, 
 /* complementarity residual: max | x - prox(x - D^-1 (A x + b)) |_inf / max(1, |x|_inf) with D = diag(A).
    Every solver of the reference scales the prox argument by a positive multiple of D^-1 (r = 1/diag,
    0.1/diag, and uniform factors of them), so all of them share this map's zeros as their fixed points. */
+/* ------------------------------------------------------------------------------------------------------ */
+/* Hinge joints (constraints/hinges.py): 5 rows per hinge, solved in the same Gauss-Seidel loop as the      */
+/* contacts (gauss_seidel_solver.py:14), each problem with its own w, r-factors and merit                  */
+/* ------------------------------------------------------------------------------------------------------ */
+typedef struct {
+    int H, N;
+    double* J;      /* H x 5 x 12: [body lo: v(3) w(3) | body hi: v(3) w(3)] */
+    int32_t* lohi;  /* H x 2 body indices in ascending order */
+    double* WJT;    /* H x 5 x 12 */
+    uint8_t* has_w; /* H x 2 */
+    int32_t* body_ptr; int32_t* body_list;
+} HProblem;
+
+/* hinges.py:95-180 _compute_jacobian_matrix and the W J^T product of hinges.py:37 */
+static void hinge_build(HProblem* P, const OScene* sc, const double* q, const double* Winv) {
+    const int H = sc->n_hinges, N = sc->n_bodies;
+    P->H = H; P->N = N;
+    P->J = (double*)calloc((size_t)60 * (H ? H : 1), sizeof(double));
+    P->WJT = (double*)calloc((size_t)60 * (H ? H : 1), sizeof(double));
+    P->lohi = (int32_t*)malloc(sizeof(int32_t) * 2 * (H ? H : 1));
+    P->has_w = (uint8_t*)malloc(2 * (H ? H : 1));
+    P->body_ptr = (int32_t*)calloc((size_t)N + 1, sizeof(int32_t));
+    P->body_list = (int32_t*)malloc(sizeof(int32_t) * 2 * (H ? H : 1));
+    /* the reference fills preallocated 5x3 blocks; rows 3-4 of the linear blocks stay 0 */
+    double JAv[5][3] = {{0}}, JAw[5][3] = {{0}}, JBv[5][3] = {{0}}, JBw[5][3] = {{0}};
+    for (int k = 0; k < H; ++k) {
+        const int A = sc->hinge_bodies[2 * k], B = sc->hinge_bodies[2 * k + 1];
+        const double* f = sc->hinge_frames + 12 * k;
+        double ap[3], ac[3], np_[3], t[3], bb[3], nn[3];
+        quat_rotate(q + 4 * A, f, ap);
+        quat_rotate(q + 4 * B, f + 3, ac);
+        quat_rotate(q + 4 * A, f + 6, np_);
+        make_orthonormal_vectors(np_, t, bb, nn);
+        /* JA_v[0:3] = I, JA_w[0:3] = -star(arm_p), JA_w[3] = t, JA_w[4] = b; JB_v[0:3] = -I,
+           JB_w[0:3] = star(arm_c), JB_w[3] = -t, JB_w[4] = -b  (star(v) = [[0,-v2,v1],[v2,0,-v0],[-v1,v0,0]]) */
+        const double sp[3][3] = {{0.0, -ap[2], ap[1]}, {ap[2], 0.0, -ap[0]}, {-ap[1], ap[0], 0.0}};
+        const double sc3[3][3] = {{0.0, -ac[2], ac[1]}, {ac[2], 0.0, -ac[0]}, {-ac[1], ac[0], 0.0}};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                JAv[i][j] = i == j ? 1.0 : 0.0;
+                JAw[i][j] = -sp[i][j];
+                JBv[i][j] = -(i == j ? 1.0 : 0.0);
+                JBw[i][j] = sc3[i][j];
+            }
+        for (int j = 0; j < 3; ++j) {
+            JAw[3][j] = t[j]; JAw[4][j] = bb[j];
+            JBw[3][j] = -t[j]; JBw[4][j] = -bb[j];
+        }
+        const int lo = A < B ? A : B, hi = A < B ? B : A;
+        P->lohi[2 * k] = lo; P->lohi[2 * k + 1] = hi;
+        for (int row = 0; row < 5; ++row) {
+            double* Jr = P->J + 60 * k + 12 * row;
+            double* sideA = Jr + (A == lo ? 0 : 6);
+            double* sideB = Jr + (B == lo ? 0 : 6);
+            for (int a = 0; a < 3; ++a) {
+                sideA[a] = JAv[row][a]; sideA[3 + a] = JAw[row][a];
+                sideB[a] = JBv[row][a]; sideB[3 + a] = JBw[row][a];
+            }
+        }
+        for (int side = 0; side < 2; ++side) {
+            const int b = P->lohi[2 * k + side];
+            P->has_w[2 * k + side] = sc->fixed[b] ? 0 : 1;
+            P->body_ptr[b + 1] += 1;
+            if (sc->fixed[b]) continue;
+            const double m = 1.0 / sc->mass[b];
+            const double* Wi = Winv + 9 * b;
+            for (int row = 0; row < 5; ++row) {
+                const double* Jr = P->J + 60 * k + 12 * row + 6 * side;
+                double* Wr = P->WJT + 60 * k + 12 * row + 6 * side;
+                for (int i = 0; i < 3; ++i) {
+                    double s2 = 0.0;
+                    s2 += (i == 0 ? m : 0.0) * Jr[0];
+                    s2 += (i == 1 ? m : 0.0) * Jr[1];
+                    s2 += (i == 2 ? m : 0.0) * Jr[2];
+                    Wr[i] = s2;
+                    double u = 0.0;
+                    u += Wi[3 * i + 0] * Jr[3];
+                    u += Wi[3 * i + 1] * Jr[4];
+                    u += Wi[3 * i + 2] * Jr[5];
+                    Wr[3 + i] = u;
+                }
+            }
+        }
+    }
+    for (int b = 0; b < N; ++b) P->body_ptr[b + 1] += P->body_ptr[b];
+    int32_t* fill = (int32_t*)calloc((size_t)N, sizeof(int32_t));
+    for (int k = 0; k < H; ++k)
+        for (int side = 0; side < 2; ++side) {
+            int b = P->lohi[2 * k + side];
+            P->body_list[P->body_ptr[b] + fill[b]++] = k;
+        }
+    free(fill);
+}
+
+static void hinge_free(HProblem* P) {
+    free(P->J); free(P->WJT); free(P->lohi); free(P->has_w); free(P->body_ptr); free(P->body_list);
+}
+
+static inline double hrow_dot(const HProblem* P, int k, int row, const double* w) {
+    const double* Jr = P->J + 60 * k + 12 * row;
+    const int lo = P->lohi[2 * k], hi = P->lohi[2 * k + 1];
+    double s = 0.0;
+    for (int c = 0; c < 6; ++c) s += Jr[c] * w[6 * lo + c];
+    for (int c = 0; c < 6; ++c) s += Jr[6 + c] * w[6 * hi + c];
+    return s;
+}
+
+static void hinge_wjt_dot(const HProblem* P, const double* x, double* y) {
+    for (int b = 0; b < P->N; ++b)
+        for (int d = 0; d < 6; ++d) {
+            double s = 0.0;
+            for (int e = P->body_ptr[b]; e < P->body_ptr[b + 1]; ++e) {
+                int k = P->body_list[e];
+                int side = (P->lohi[2 * k] == b) ? 0 : 1;
+                if (!P->has_w[2 * k + side]) continue;
+                for (int row = 0; row < 5; ++row) s += P->WJT[60 * k + 12 * row + 6 * side + d] * x[5 * k + row];
+            }
+            y[6 * b + d] = s;
+        }
+}
+
+/* hinges.py:188-218 _compute_error_vector (pre-stabilisation only) */
+static void hinge_error(const OScene* sc, const double* params, double dt, const double* r, const double* q,
+                        double* g) {
+    const int H = sc->n_hinges;
+    for (int i = 0; i < 5 * H; ++i) g[i] = 0.0;
+    if (params[P_USE_PRE] == 0.0) return;
+    for (int k = 0; k < H; ++k) {
+        const int A = sc->hinge_bodies[2 * k], B = sc->hinge_bodies[2 * k + 1];
+        const double* f = sc->hinge_frames + 12 * k;
+        double rp[3], rc[3], np_[3], t[3], bb[3], nn[3], nc[3], u[3];
+        quat_rotate(q + 4 * A, f, rp);
+        quat_rotate(q + 4 * B, f + 3, rc);
+        for (int i = 0; i < 3; ++i) { rp[i] = rp[i] + r[3 * A + i]; rc[i] = rc[i] + r[3 * B + i]; }
+        quat_rotate(q + 4 * A, f + 6, np_);
+        make_orthonormal_vectors(np_, t, bb, nn);
+        quat_rotate(q + 4 * B, f + 9, nc);
+        cross_np(nn, nc, u);
+        for (int i = 0; i < 3; ++i) g[5 * k + i] = rc[i] - rp[i];
+        g[5 * k + 3] = dot3_np(t, u);
+        g[5 * k + 4] = dot3_np(bb, u);
+    }
+    const double rate = params[P_GAP_REDUCTION] / dt;
+    for (int i = 0; i < 5 * H; ++i) g[i] = g[i] * rate;
+}
+
+/* hinges.py:57-90 Hinges.sweep: x_b -= r_b (J w + b)_b, then w += WJT[:, b] dx */
+static void hinge_sweep(const HProblem* P, const double* r, const double* b, double* x, double* w) {
+    hinge_wjt_dot(P, x, w);
+    for (int k = 0; k < P->H; ++k) {
+        double xb[5], delta[5], jw[5];
+        for (int i = 0; i < 5; ++i) jw[i] = hrow_dot(P, k, i, w);
+        for (int i = 0; i < 5; ++i) {
+            xb[i] = x[5 * k + i];
+            delta[i] = xb[i];
+            xb[i] = xb[i] - r[5 * k + i] * (jw[i] + b[5 * k + i]);
+            x[5 * k + i] = xb[i];
+            delta[i] = xb[i] - delta[i];
+        }
+        for (int side = 0; side < 2; ++side) {
+            if (!P->has_w[2 * k + side]) continue;
+            const int bb = P->lohi[2 * k + side];
+            for (int d = 0; d < 6; ++d) {
+                double s = 0.0;
+                for (int row = 0; row < 5; ++row) s += P->WJT[60 * k + 12 * row + 6 * side + d] * delta[row];
+                w[6 * bb + d] = w[6 * bb + d] + s;
+            }
+        }
+    }
+}
+
 static const double* g_residual_diag = NULL;
 static int g_residual_interval = 1;   /* tol_mode 2: residual tested every this many sweeps */
 static double g_relaxation = 1.0;     /* tol_mode 2: r = relaxation / diag */
@@ -881,6 +1056,47 @@ static void solve_rigid(const Problem* P, const double* params, double* r, const
                 for (int i = 0; i < n; ++i) r[i] = params[P_NU_INCREASE] * r[i];
             last_merit = merit;
             global_merit = global_merit > merit ? global_merit : merit;
+        }
+        if (residuals) residuals[it] = global_merit;
+        if (global_merit < params[P_ABS_TOL]) { *iterations = it; *exitcode = 1; break; }
+        if (fabs(global_merit - global_last) < params[P_REL_TOL] * global_last) { *iterations = it; *exitcode = 2; break; }
+        global_last = global_merit;
+    }
+    free(w);
+}
+
+/* gauss_seidel_solver.py:14 solve over the problem list [contacts (when any), hinges]: every iteration
+   sweeps each problem in turn and accepts or rolls back its iterate against that problem's own last merit;
+   the convergence tests use the largest merit of the iteration */
+static void solve_problems(const Problem* P, double* r, const double* b, const double* mu, double* x, double* sol,
+                           const HProblem* HP, double* hr, const double* hb, double* hx, double* hsol,
+                           const double* params, double* residuals, int* iterations, int* exitcode) {
+    const int max_it = (int)params[P_MAX_ITER];
+    const int N = HP->N;
+    double* w = (double*)malloc(sizeof(double) * 6 * (N ? N : 1));
+    double last[2] = {INFINITY, INFINITY}, global_last = INFINITY;
+    *iterations = max_it; *exitcode = 0;
+    for (int it = 0; it < max_it; ++it) {
+        double global_merit = 0.0;
+        for (int prob = (P ? 0 : 1); prob < 2; ++prob) {
+            double* xx = prob ? hx : x;
+            double* ss = prob ? hsol : sol;
+            double* rr = prob ? hr : r;
+            const int n = prob ? 5 * HP->H : 4 * P->K;
+            if (prob) hinge_sweep(HP, hr, hb, hx, w);
+            else sweep_gs(P, r, b, mu, x, w, 0, NULL);
+            const double merit = merit_inf(xx, ss, n);
+            if (merit > last[prob]) {
+                for (int i = 0; i < n; ++i) rr[i] = params[P_NU_REDUCE] * rr[i];
+                memcpy(xx, ss, sizeof(double) * n);
+                global_merit = global_merit > last[prob] ? global_merit : last[prob];
+            } else {
+                memcpy(ss, xx, sizeof(double) * n);
+                if (last[prob] - merit < params[P_TOO_SMALL])
+                    for (int i = 0; i < n; ++i) rr[i] = params[P_NU_INCREASE] * rr[i];
+                last[prob] = merit;
+                global_merit = global_merit > merit ? global_merit : merit;
+            }
         }
         if (residuals) residuals[it] = global_merit;
         if (global_merit < params[P_ABS_TOL]) { *iterations = it; *exitcode = 1; break; }
@@ -1059,6 +1275,12 @@ int rbo_step(const OScene* sc, const double* params, double dt, double* r, doubl
     if (out->delta_u_ext) memcpy(out->delta_u_ext, dux, sizeof(double) * 6 * N);
     for (int i = 0; i < 6 * N; ++i) du[i] = dt * dux[i];
 
+    const int H = sc->n_hinges;
+    /* hinges are solved by the reference stepper's own Gauss-Seidel rule only */
+    if (H > 0 && (out->scheme != S_RIGID_GS || tol_mode != 0 || g_ordering != 0)) {
+        free(dux); free(Winv); free(u); free(du);
+        return 4;
+    }
     ContactList cl = {0, 0, NULL, NULL, NULL, NULL};
     run_collision_detection(sc, params, r, q, &cl, out);
     const int K = cl.n;
@@ -1069,6 +1291,42 @@ int rbo_step(const OScene* sc, const double* params, double dt, double* r, doubl
     Problem P;
     memset(&P, 0, sizeof(P));
     double *b = NULL, *diag = NULL, *rr = NULL, *x = NULL, *sol = NULL, *mu = NULL;
+    /* hinges.py:28-50 Hinges.initialize */
+    HProblem HP;
+    memset(&HP, 0, sizeof(HP));
+    double *hb = NULL, *hdiag = NULL, *hr = NULL, *hx = NULL, *hsol = NULL;
+    if (H > 0) {
+        hinge_build(&HP, sc, q, Winv);
+        hb = (double*)malloc(sizeof(double) * 5 * H);
+        hdiag = (double*)malloc(sizeof(double) * 5 * H);
+        hr = (double*)malloc(sizeof(double) * 5 * H);
+        hx = (double*)calloc((size_t)5 * H, sizeof(double));
+        hsol = (double*)calloc((size_t)5 * H, sizeof(double));
+        double* g = (double*)malloc(sizeof(double) * 5 * H);
+        double* dtd = (double*)malloc(sizeof(double) * 6 * N);
+        for (int i = 0; i < 6 * N; ++i) dtd[i] = dt * dux[i];
+        hinge_error(sc, params, dt, r, q, g);
+        for (int k = 0; k < H; ++k)
+            for (int i = 0; i < 5; ++i)
+                hb[5 * k + i] = (hrow_dot(&HP, k, i, u) + hrow_dot(&HP, k, i, dtd)) + g[5 * k + i];
+        /* diag = sum(J .* WJT^T, axis=1), zero entries replaced by 1; r = 1 / diag */
+        for (int k = 0; k < H; ++k)
+            for (int row = 0; row < 5; ++row) {
+                const double* Jr = HP.J + 60 * k + 12 * row;
+                const double* Wr = HP.WJT + 60 * k + 12 * row;
+                double prods[12];
+                int m = 0;
+                for (int c = 0; c < 12; ++c) {
+                    if (!HP.has_w[2 * k + c / 6]) continue;
+                    const double prod = Jr[c] * Wr[c];
+                    if (prod != 0.0) prods[m++] = prod;
+                }
+                const double sd = np_reduce_sum(prods, m);
+                hdiag[5 * k + row] = sd == 0.0 ? 1.0 : sd;
+            }
+        for (int i = 0; i < 5 * H; ++i) hr[i] = 1.0 / hdiag[i];
+        free(g); free(dtd);
+    }
     if (K > 0) {
         problem_build(&P, sc, &cl, r, Winv);
         b = (double*)malloc(sizeof(double) * 4 * K);
@@ -1130,7 +1388,9 @@ int rbo_step(const OScene* sc, const double* params, double dt, double* r, doubl
             free(colour); free(cptr);
             out->n_colours = nc;
         }
-        if (out->scheme == S_RIGID_GS)
+        if (H > 0)
+            solve_problems(&P, rr, b, mu, x, sol, &HP, hr, hb, hx, hsol, params, out->residuals, &iters, &exitc);
+        else if (out->scheme == S_RIGID_GS)
             solve_rigid(&P, params, rr, b, mu, x, sol, out->residuals, &iters, &exitc, 0, tol_mode, tol, clist);
         else
             solve_interface(&P, params, out->scheme, diag, b, mu, x, sol, out->residuals, &iters, &exitc, clist,
@@ -1142,6 +1402,22 @@ int rbo_step(const OScene* sc, const double* params, double dt, double* r, doubl
         wjt_dot(&P, sol, dc);
         for (int i = 0; i < 6 * N; ++i) du[i] = du[i] + dc[i];
         free(dc);
+    } else if (H > 0) {
+        int iters = 0, exitc = 0;
+        solve_problems(NULL, NULL, NULL, NULL, NULL, NULL, &HP, hr, hb, hx, hsol, params, out->residuals, &iters,
+                       &exitc);
+        out->iterations = iters; out->exitcode = exitc;
+    }
+    if (H > 0) {   /* hinges.py:52 finalize_solution, added after the contacts' (steppers.py:84-85) */
+        double* dh = (double*)malloc(sizeof(double) * 6 * N);
+        hinge_wjt_dot(&HP, hsol, dh);
+        for (int i = 0; i < 6 * N; ++i) du[i] = du[i] + dh[i];
+        free(dh);
+        if (out->hinge_b) memcpy(out->hinge_b, hb, sizeof(double) * 5 * H);
+        if (out->hinge_diag) memcpy(out->hinge_diag, hdiag, sizeof(double) * 5 * H);
+        if (out->hinge_sol) memcpy(out->hinge_sol, hsol, sizeof(double) * 5 * H);
+        hinge_free(&HP);
+        free(hb); free(hdiag); free(hr); free(hx); free(hsol);
     }
     /* state_storage.py:239 velocity_update, :251 position_update */
     for (int i = 0; i < 6 * N; ++i) u[i] = u[i] + du[i];

@@ -172,6 +172,54 @@ def scene_flags(res, seed):
     return engine
 
 
+def scene_hinge_chain(links, res, stab=False, tilt=0.0, ledge=False):
+    """Cubes rotated 45 degrees about z, side by side along x, joined by hinges at the midpoints between
+    neighbours; the first link is fixed and gravity pulls the rest down, so the chain swings about the hinge
+    axes (world z, turned by `tilt` about x).  With `ledge` a fixed box under the outer links catches them,
+    so hinges and contacts are solved together."""
+    engine = API.create_engine()
+    engine.params.resolution = res
+    engine.params.use_pre_stabilization = stab
+    API.create_surfaces_interaction(engine, "m", "m", 0.0, V3.make(0.4, 0.4, 0.4))
+    V, T = create_box(1.0, 1.0, 1.0)
+    API.create_shape(engine, "cube", API.create_mesh(V, T))
+    API.create_gravity_force(engine, "gravity", 9.81, V3.j())
+    diameter = np.sqrt(2.0)
+    margin = 0.1 * diameter / 2.0
+    names = []
+    for k in range(links):
+        name = "link%d" % k
+        names.append(name)
+        API.create_rigid_body(engine, name)
+        API.connect_shape(engine, name, "cube")
+        API.set_position(engine, name, V3.make(k * (diameter + margin), 0.0, 0.0), True)
+        API.set_orientation(engine, name, Q.Rz(np.pi / 4), True)
+        API.set_mass_properties(engine, name, 1.0)
+        API.set_body_material(engine, name, "m")
+        if k == 0:
+            API.set_body_type(engine, name, "fixed")
+        else:
+            API.connect_force(engine, name, "gravity")
+    if ledge:
+        V, T = create_box(6.0, 1.0, 2.0)
+        API.create_shape(engine, "ledge_shape", API.create_mesh(V, T))
+        API.create_rigid_body(engine, "ledge")
+        API.connect_shape(engine, "ledge", "ledge_shape")
+        API.set_position(engine, "ledge", V3.make(2.0 * (diameter + margin) + 1.5, -1.3, 0.0), True)
+        API.set_orientation(engine, "ledge", Q.identity(), True)
+        API.set_body_type(engine, "ledge", "fixed")
+        API.set_mass_properties(engine, "ledge", 1.0)
+        API.set_body_material(engine, "ledge", "m")
+    axis = Q.rotate(Q.Rx(tilt), V3.k())
+    for k in range(links - 1):
+        hinge = names[k] + "_" + names[k + 1]
+        API.create_hinge(engine, hinge)
+        o = (API.get_position(engine, names[k]) + API.get_position(engine, names[k + 1])) / 2.0
+        API.set_hinge(engine=engine, hinge_name=hinge, parent_name=names[k], child_name=names[k + 1], origin=o,
+                      axis=axis, mode="world")
+    return engine
+
+
 # ---------------------------------------------------------------------------------------------------------------
 # serialisation
 # ---------------------------------------------------------------------------------------------------------------
@@ -247,6 +295,11 @@ def scene_arrays(engine):
     out["material_epsilon"] = eps
     out["params"] = np.array([float(getattr(engine.params, f)) for f in PARAM_FIELDS])
     out["param_names"] = np.array(PARAM_FIELDS)
+    hinges = sorted(engine.hinges.values(), key=lambda h: h.idx)
+    assert [h.idx for h in hinges] == list(range(len(hinges)))
+    out["hinge_bodies"] = np.array([[h.parent.idx, h.child.idx] for h in hinges], dtype=np.int32).reshape(-1, 2)
+    out["hinge_frames"] = np.array([np.concatenate([h.arm_p, h.arm_c, h.axis_p, h.axis_c]) for h in hinges],
+                                   dtype=np.float64).reshape(-1, 12)
     return out
 
 
@@ -276,12 +329,28 @@ class Recorder:
             if rec.delta_u_ext is None:
                 rec.delta_u_ext = state.delta_u_ext.copy()
 
+        orig_h_init = PROBLEMS.Hinges.initialize
+        orig_h_finalize = PROBLEMS.Hinges.finalize_solution
+
+        def h_initialize(problem, dt, state, engine):
+            orig_h_init(problem, dt, state, engine)
+            rec.hinge_b = problem.b.copy()
+            rec.hinge_diag = problem.diag.copy()
+
+        def h_finalize(problem):
+            out = orig_h_finalize(problem)
+            rec.hinge_sol = problem.sol.copy()
+            return out
+
         PROBLEMS.Contacts.initialize = initialize
         PROBLEMS.Contacts.finalize_solution = finalize
+        PROBLEMS.Hinges.initialize = h_initialize
+        PROBLEMS.Hinges.finalize_solution = h_finalize
         STORAGE.StateStorage.copy_from_engine = copy_from_engine
 
     def reset(self):
         self.b = self.diag = self.mu = self.sol = self.delta_u_ext = None
+        self.hinge_b = self.hinge_diag = self.hinge_sol = None
 
 
 def run_fixture(name, engine, steps):
@@ -289,7 +358,7 @@ def run_fixture(name, engine, steps):
     data = scene_arrays(engine)
     per_step = {k: [] for k in ["contacts_ids", "contacts_p", "contacts_n", "contacts_g", "b", "diag", "sol",
                                 "iterations", "exitcode", "residuals", "x", "u", "delta_u_ext", "dt",
-                                "post_iterations", "post_exitcode"]}
+                                "post_iterations", "post_exitcode", "hinge_b", "hinge_diag", "hinge_sol"]}
     t0 = time.perf_counter()
     for s in range(steps):
         rec.reset()
@@ -306,6 +375,10 @@ def run_fixture(name, engine, steps):
         per_step["b"].append(rec.b if K else np.zeros(0))
         per_step["diag"].append(rec.diag if K else np.zeros(0))
         per_step["sol"].append(rec.sol if K else np.zeros(0))
+        H = len(engine.hinges)
+        per_step["hinge_b"].append(rec.hinge_b if H else np.zeros(0))
+        per_step["hinge_diag"].append(rec.hinge_diag if H else np.zeros(0))
+        per_step["hinge_sol"].append(rec.hinge_sol if H else np.zeros(0))
         per_step["iterations"].append(log.get("iterations", -1))
         per_step["exitcode"].append(log.get("exitcode", -1))
         per_step["residuals"].append(np.asarray(log.get("residuals", np.zeros(0)), dtype=np.float64))
@@ -369,6 +442,8 @@ FIXTURES = {
     "spheres": lambda: (scene_spheres(16, seed=3), 8),
     "tower6": lambda: (scene_tower(6, 16), 20),
     "flags": lambda: (scene_flags(16, seed=5), 10),
+    "hinges": lambda: (scene_hinge_chain(5, 16, ledge=True), 30),
+    "hinges_stab": lambda: (scene_hinge_chain(4, 16, stab=True, tilt=0.3), 25),
 }
 
 

@@ -54,3 +54,25 @@ def test_oracle_proximal_contact_schemes(oracle_lib, scheme):
     np.testing.assert_array_equal(o["sol"], d["sol_" + scheme])
     assert o["iterations"] == d["iterations_" + scheme]
     assert o["exitcode"] == d["exitcode_" + scheme]
+
+
+@pytest.mark.parametrize("name", ["hinges", "hinges_stab"])
+def test_oracle_hinges_match_reference_step_by_step(oracle_lib, name):
+    """Hinge chains (constraints/hinges.py), one with contacts against a ledge and one with pre-stabilisation:
+    the hinge problem's b, Delassus diagonal and solution, the solver statistics and the state, bit for bit."""
+    d = load_fixture(name)
+    sc = oracle_lib.OracleScene(d)
+    N = sc.n_bodies
+    for s in range(int(d["steps"])):
+        if s > 0:
+            x = d["step_x"][s - 1].reshape(N, 7)
+            u = d["step_u"][s - 1].reshape(N, 6)
+            sc.r[:], sc.q[:], sc.v[:], sc.w[:] = x[:, :3], x[:, 3:], u[:, :3], u[:, 3:]
+        o = sc.step(dt=float(d["step_dt"][s]))
+        np.testing.assert_array_equal(o["ids"], step_slice(d, "contacts_ids", s), err_msg="step %d contact ids" % s)
+        for key, ref in (("b", "b"), ("diag", "diag"), ("sol", "sol"), ("hinge_b", "hinge_b"),
+                         ("hinge_diag", "hinge_diag"), ("hinge_sol", "hinge_sol")):
+            np.testing.assert_array_equal(o[key].ravel(), step_slice(d, ref, s).ravel(), err_msg="step %d %s" % (s, key))
+        assert (o["iterations"], o["exitcode"]) == (d["step_iterations"][s], d["step_exitcode"][s]), s
+        np.testing.assert_array_equal(o["x"], d["step_x"][s], err_msg="step %d x" % s)
+        np.testing.assert_array_equal(o["u"], d["step_u"][s], err_msg="step %d u" % s)
