@@ -118,6 +118,15 @@ typedef struct rb_bodies {
     /* state, read at the start and written at the end of a step (state_storage.py:43-68 layout) */
     double* x;                    /* 7 per body: r[3], q[4] */
     double* u;                    /* 6 per body: v[3], w[3] */
+    /* hinge joints (types.py:304 Hinge, constraints/hinges.py); scene s owns hinges scene_hinge_start[s] ..
+       scene_hinge_start[s+1]-1 in Hinge.idx order.  They are solved with the reference stepper's rule only
+       (RB_SCHEME_RIGID_GS, RB_TERMINATE_MERIT, RB_ORDER_SERIAL, RB_PRECISION_FP64); other settings are
+       rejected with RB_ERR_UNSUPPORTED for batches that hold hinges */
+    int32_t n_hinges;
+    const int32_t* scene_hinge_start; /* n_scenes+1 (may be NULL when n_hinges == 0) */
+    const int32_t* hinge_bodies;  /* 2 per hinge: parent, child (global body indices) */
+    const double* hinge_frames;   /* 12 per hinge: arm_p[3], arm_c[3], axis_p[3], axis_c[3] in the parent's and
+                                     the child's body frames (Hinge.arm_p, .arm_c, .axis_p, .axis_c) */
 } rb_bodies;
 
 /* Capacities of the per-step work lists.  Exceeding one sets a status bit; the step then leaves x and u
@@ -217,6 +226,7 @@ typedef struct rb_outputs {
     int64_t* cache_key;           /* 2 per contact */
     double* cache_sol;            /* 4 per contact */
     int32_t* cache_count;         /* 1 int32 */
+    double* hinge_sol;            /* 5 per hinge: the hinge problem's solution (hinges.py:52), or NULL */
 } rb_outputs;
 
 /* Library ABI version (RB_ABI_VERSION). */

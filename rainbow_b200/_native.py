@@ -45,6 +45,7 @@ class RbBodies(ctypes.Structure):
         ("n_body_vertices", _i32), ("n_body_triangles", _i32), ("n_clusters", _i32), ("max_scene_bodies", _i32),
         ("body_v0", _vp), ("body_t0", _vp), ("body_c0", _vp), ("vert_body", _vp), ("tri_body", _vp),
         ("clu_body", _vp), ("x", _vp), ("u", _vp),
+        ("n_hinges", _i32), ("scene_hinge_start", _vp), ("hinge_bodies", _vp), ("hinge_frames", _vp),
     ]
 
 
@@ -83,7 +84,7 @@ class RbOutputs(ctypes.Structure):
     _fields_ = [("contact_ids", _vp), ("contact_p", _vp), ("contact_n", _vp), ("contact_g", _vp),
                 ("contact_sol", _vp), ("stats", _vp), ("residuals", _vp), ("status", _vp),
                 ("n_contacts_total", _vp), ("needed", _vp), ("cache_key", _vp), ("cache_sol", _vp),
-                ("cache_count", _vp)]
+                ("cache_count", _vp), ("hinge_sol", _vp)]
 
 
 # exported symbols and their ctypes signatures: every function declared in include/rainbow_b200.h

@@ -14,7 +14,7 @@ import numpy as np
 
 from . import geometry as GEO
 from .stepper import GpuStepper
-from .types import Damping, Engine, Gravity, RigidBody, Shape, SurfacesInteraction
+from .types import Damping, Engine, Gravity, Hinge, RigidBody, Shape, SurfacesInteraction
 
 create_box = GEO.create_box
 create_sphere = GEO.create_sphere
@@ -35,6 +35,49 @@ def create_rigid_body(engine, body_name):
     body = RigidBody(body_name)
     body.idx = len(engine.bodies)
     engine.bodies[body_name] = body
+
+
+def create_hinge(engine, hinge_name):
+    """api.py:71"""
+    if hinge_name in engine.hinges:
+        raise RuntimeError("create_hinge() hinge already exist with that name")
+    hinge = Hinge(hinge_name)
+    hinge.idx = len(engine.hinges)
+    engine.hinges[hinge_name] = hinge
+
+
+def set_hinge(engine, hinge_name, parent_name, child_name, origin, axis, mode="world"):
+    """api.py:86: joint origin and axis given in world coordinates, in the parent's body frame ("body") or in
+    the parent's model frame ("model"); stored as each body's arm (origin in its body frame) and axis (the
+    joint frame's z axis in its body frame), as Hinge.set_parent_socket / set_child_socket do (types.py:330)."""
+    if hinge_name not in engine.hinges:
+        raise RuntimeError("set_hinge() no such rigid body exist with that name")
+    hinge = engine.hinges[hinge_name]
+    if parent_name not in engine.bodies or child_name not in engine.bodies:
+        raise RuntimeError("set_hinge() no such rigid body exist with that name")
+    parent, child = engine.bodies[parent_name], engine.bodies[child_name]
+    origin = np.asarray(origin, dtype=np.float64)
+    axis = np.asarray(axis, dtype=np.float64)
+    if mode == "world":
+        o_world, s_world = origin.copy(), axis.copy()
+    elif mode == "body":
+        o_world = GEO.quat_rotate(parent.q, origin) + parent.r
+        s_world = GEO.quat_rotate(parent.q, axis)
+    elif mode == "model":
+        o_body = GEO.quat_rotate(GEO.quat_conj(parent.shape.q), origin - parent.shape.r)
+        s_body = GEO.quat_rotate(GEO.quat_conj(parent.shape.q), axis)
+        o_world = GEO.quat_rotate(parent.q, o_body) + parent.r
+        s_world = GEO.quat_rotate(parent.q, s_body)
+    else:
+        raise ValueError(f"set_hinge() no such mode {mode} is supported")
+    t, b, n = GEO.orthonormal_frame(s_world)   # the joint axis is the joint frame's local z axis
+    q_world = GEO.quat_from_matrix(np.column_stack([t, b, n]))
+    k = np.array([0.0, 0.0, 1.0])
+    hinge.parent, hinge.child = parent, child
+    hinge.arm_p = GEO.quat_rotate(GEO.quat_conj(parent.q), o_world - parent.r)
+    hinge.arm_c = GEO.quat_rotate(GEO.quat_conj(child.q), o_world - child.r)
+    hinge.axis_p = GEO.quat_rotate(GEO.quat_prod(GEO.quat_conj(parent.q), q_world), k)
+    hinge.axis_c = GEO.quat_rotate(GEO.quat_prod(GEO.quat_conj(child.q), q_world), k)
 
 
 def create_shape(engine, shape_name, mesh, transform_to_body_frame=True):

@@ -63,6 +63,10 @@ struct Workspace {
     int32_t* sweeps32;   // S   FP32 sweeps done per scene (-1: the scene is solved in FP64 only)
     int32_t* nlev;       // S   levels (or colours) the FP32 phase found for the scene
     double* eterm;       // 2N  kinetic and potential energy of each body (profiled steps)
+    // hinge joints (H of them): J and W J^T blocks (5 rows x 12), b, diag, r, x, sol, body pairs (ascending),
+    // level order and starts per scene, per-body hinge lists, the hinge problem's own accumulators w
+    double *hJ, *hWJT, *hb, *hdiag, *hr, *hx, *hsol, *hw;
+    int32_t *hlohi, *hlev, *hlev_order, *hlev_ptr, *hbody_ptr, *hbody_list, *hlast;
     // scans and counters
     int32_t* scan_tmp;   // kScanBlocks + 1
     int32_t* counters;   // 16
@@ -74,7 +78,7 @@ inline size_t align_up(size_t v) { return (v + 255) & ~size_t(255); }
 
 // Computes (and, when base != nullptr, assigns) every array; returns the total bytes.
 inline size_t layout(Workspace* ws, char* base, int64_t N, int64_t NV, int64_t NT, int64_t NC, int64_t P,
-                     int64_t C, int64_t K, int64_t S) {
+                     int64_t C, int64_t K, int64_t S, int64_t H) {
     size_t off = 0;
     auto take = [&](auto*& ptr, int64_t count) {
         using T = std::remove_reference_t<decltype(*ptr)>;
@@ -99,6 +103,10 @@ inline size_t layout(Workspace* ws, char* base, int64_t N, int64_t NV, int64_t N
     take(w->lev_of, K); take(w->lev_order, K); take(w->lev_ptr, K + S + 1); take(w->lev_cur, K + S + 1);
     take(w->cpred, 2 * K);
     take(w->sweeps32, S); take(w->nlev, S); take(w->eterm, 2 * N);
+    take(w->hJ, 60 * H); take(w->hWJT, 60 * H); take(w->hb, 5 * H); take(w->hdiag, 5 * H); take(w->hr, 5 * H);
+    take(w->hx, 5 * H); take(w->hsol, 5 * H); take(w->hlohi, 2 * H); take(w->hlev_order, H);
+    take(w->hlev_ptr, H + S + 1); take(w->hbody_ptr, N + 1); take(w->hbody_list, 2 * H); take(w->hw, 6 * N);
+    take(w->hlast, N); take(w->hlev, H);
     take(w->scan_tmp, kScanBlocks + 1); take(w->counters, 16);
     return off;
 }

@@ -1125,9 +1125,299 @@ __device__ double scene_residual(const StepArgs& a, const G& g, const SceneRange
     return mres / (mx > 1.0 ? mx : 1.0);
 }
 
+// ---------------------------------------------------------------------------------------------------------
+// hinge joints (constraints/hinges.py): 5 rows per hinge between a parent and a child body
+// ---------------------------------------------------------------------------------------------------------
+// per-body hinge lists of each scene (thread per scene): entries (hinge << 1 | side), hinges ascending; every
+// hinge gives both of its bodies an entry, so scene s's entries fill [2 h0, 2 h1) exactly
+__global__ void k_hinge_lists(const StepArgs a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.bd.n_scenes || a.ws.counters[kAbort]) return;
+    const int b0 = a.bd.scene_start[s], b1 = a.bd.scene_start[s + 1];
+    const int h0 = a.bd.scene_hinge_start[s], h1 = a.bd.scene_hinge_start[s + 1];
+    int32_t* cnt = a.ws.hlast;
+    for (int b = b0; b < b1; ++b) cnt[b] = 0;
+    for (int k = h0; k < h1; ++k) { cnt[a.bd.hinge_bodies[2 * k]]++; cnt[a.bd.hinge_bodies[2 * k + 1]]++; }
+    int pos = 2 * h0;
+    for (int b = b0; b < b1; ++b) { a.ws.hbody_ptr[b] = pos; pos += cnt[b]; cnt[b] = 0; }
+    if (s == a.bd.n_scenes - 1) a.ws.hbody_ptr[a.bd.n_bodies] = pos;
+    for (int k = h0; k < h1; ++k)
+        for (int side = 0; side < 2; ++side) {
+            const int P = a.bd.hinge_bodies[2 * k], C = a.bd.hinge_bodies[2 * k + 1];
+            const int b = side ? max(P, C) : min(P, C);
+            a.ws.hbody_list[a.ws.hbody_ptr[b] + cnt[b]++] = (k << 1) | side;
+        }
+}
+
+// hinges.py:28-50 Hinges.initialize with _compute_jacobian_matrix (:95-180) and _compute_error_vector
+// (:188-218): J, W J^T (bsr_matmat order), b = (J u + J dt du_ext) + g, diag = sum(J .* WJT^T) (zeros -> 1),
+// r = 1/diag, x = sol = 0.  Thread per hinge.
+__global__ void k_hinges(const StepArgs a) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.bd.n_hinges || a.ws.counters[kAbort]) return;
+    const int A = a.bd.hinge_bodies[2 * k], B = a.bd.hinge_bodies[2 * k + 1];
+    const double* f = a.bd.hinge_frames + 12 * (size_t)k;
+    const double* qA = a.bd.x + 7 * A + 3;
+    const double* qB = a.bd.x + 7 * B + 3;
+    const d3 ap = quat_rotate(qA, ld3(f)), ac = quat_rotate(qB, ld3(f + 3)), np_ = quat_rotate(qA, ld3(f + 6));
+    d3 t, bb, nn;
+    make_orthonormal_vectors(np_, t, bb, nn);
+    // JA_v[0:3] = I, JA_w[0:3] = -star(arm_p), JA_w[3] = t, JA_w[4] = b; JB_v[0:3] = -I, JB_w[0:3] = star(arm_c),
+    // JB_w[3] = -t, JB_w[4] = -b; star(v) = [[0, -v2, v1], [v2, 0, -v0], [-v1, v0, 0]]
+    const double sp[3][3] = {{0.0, -ap.z, ap.y}, {ap.z, 0.0, -ap.x}, {-ap.y, ap.x, 0.0}};
+    const double sc[3][3] = {{0.0, -ac.z, ac.y}, {ac.z, 0.0, -ac.x}, {-ac.y, ac.x, 0.0}};
+    double JA[5][6], JB[5][6];
+    for (int i = 0; i < 5; ++i)
+        for (int j = 0; j < 6; ++j) { JA[i][j] = 0.0; JB[i][j] = 0.0; }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            JA[i][j] = i == j ? 1.0 : 0.0;
+            JA[i][3 + j] = -sp[i][j];
+            JB[i][j] = -(i == j ? 1.0 : 0.0);
+            JB[i][3 + j] = sc[i][j];
+        }
+    const double tv[3] = {t.x, t.y, t.z}, bv[3] = {bb.x, bb.y, bb.z};
+    for (int j = 0; j < 3; ++j) {
+        JA[3][3 + j] = tv[j]; JA[4][3 + j] = bv[j];
+        JB[3][3 + j] = -tv[j]; JB[4][3 + j] = -bv[j];
+    }
+    const int lo = min(A, B), hi = max(A, B);
+    a.ws.hlohi[2 * k] = lo;
+    a.ws.hlohi[2 * k + 1] = hi;
+    double* J = a.ws.hJ + 60 * (size_t)k;
+    double* W = a.ws.hWJT + 60 * (size_t)k;
+    for (int row = 0; row < 5; ++row)
+        for (int j = 0; j < 6; ++j) {
+            J[12 * row + (A == lo ? 0 : 6) + j] = JA[row][j];
+            J[12 * row + (B == lo ? 0 : 6) + j] = JB[row][j];
+        }
+    bool hasw[2];
+    for (int side = 0; side < 2; ++side) {
+        const int bd = side ? hi : lo;
+        hasw[side] = !a.bd.fixed[bd];
+        const double m = hasw[side] ? 1.0 / a.bd.mass[bd] : 0.0;
+        const double* Wi = a.ws.Winv + 9 * (size_t)bd;
+        for (int row = 0; row < 5; ++row) {
+            const double* Jr = J + 12 * row + 6 * side;
+            double* Wr = W + 12 * row + 6 * side;
+            for (int i = 0; i < 3; ++i) {
+                double s = 0.0;
+                s += (i == 0 ? m : 0.0) * Jr[0];
+                s += (i == 1 ? m : 0.0) * Jr[1];
+                s += (i == 2 ? m : 0.0) * Jr[2];
+                double u = 0.0;
+                u += Wi[3 * i + 0] * Jr[3];
+                u += Wi[3 * i + 1] * Jr[4];
+                u += Wi[3 * i + 2] * Jr[5];
+                Wr[i] = hasw[side] ? s : 0.0;
+                Wr[3 + i] = hasw[side] ? u : 0.0;
+            }
+        }
+    }
+    double g[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (a.pr.use_pre_stabilization) {
+        const d3 rp = add(ap, ld3(a.bd.x + 7 * A)), rc = add(ac, ld3(a.bd.x + 7 * B));
+        const d3 ncv = quat_rotate(qB, ld3(f + 9));
+        const d3 u = cross_np(nn, ncv);
+        const double rate = a.pr.gap_reduction / a.pr.dt;
+        g[0] = (rc.x - rp.x) * rate;
+        g[1] = (rc.y - rp.y) * rate;
+        g[2] = (rc.z - rp.z) * rate;
+        g[3] = dot3_np(t, u) * rate;
+        g[4] = dot3_np(bb, u) * rate;
+    }
+    const double* ulo = a.bd.u + 6 * lo;
+    const double* uhi = a.bd.u + 6 * hi;
+    const double* dlo = a.ws.du + 6 * lo;
+    const double* dhi = a.ws.du + 6 * hi;
+    for (int row = 0; row < 5; ++row) {
+        const double* Jr = J + 12 * row;
+        const double* Wr = W + 12 * row;
+        a.ws.hb[5 * (size_t)k + row] = (jrow_dot(Jr, ulo, uhi) + jrow_dot(Jr, dlo, dhi)) + g[row];
+        double prods[12];
+        int m = 0;
+        for (int c = 0; c < 12; ++c) {
+            if (!hasw[c / 6]) continue;
+            const double prod = Jr[c] * Wr[c];
+            if (prod != 0.0) prods[m++] = prod;
+        }
+        const double d = np_reduce_sum(prods, m);
+        const double diag = d == 0.0 ? 1.0 : d;
+        a.ws.hdiag[5 * (size_t)k + row] = diag;
+        a.ws.hr[5 * (size_t)k + row] = 1.0 / diag;
+        a.ws.hx[5 * (size_t)k + row] = 0.0;
+        a.ws.hsol[5 * (size_t)k + row] = 0.0;
+    }
+}
+
+// w = W J^T x of the hinge problem for every body of the scene (hinges ascending, 5 rows each)
+template <class G>
+__device__ void hinge_wjt(const StepArgs& a, const G& g, const SceneRange& R) {
+    for (int b = R.b0 + g.rank(); b < R.b1; b += g.size()) {
+        double s6[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (!a.bd.fixed[b])
+            for (int e = a.ws.hbody_ptr[b]; e < a.ws.hbody_ptr[b + 1]; ++e) {
+                const int code = a.ws.hbody_list[e];
+                const int k = code >> 1, side = code & 1;
+                const double* Wk = a.ws.hWJT + 60 * (size_t)k + 6 * side;
+                for (int d = 0; d < 6; ++d) {
+                    double t = s6[d];
+                    for (int row = 0; row < 5; ++row) t += Wk[12 * row + d] * a.ws.hx[5 * (size_t)k + row];
+                    s6[d] = t;
+                }
+            }
+        for (int d = 0; d < 6; ++d) a.ws.hw[6 * (size_t)b + d] = s6[d];
+    }
+    g.sync();
+}
+
+// hinges.py:62-90: x_b -= r_b (J w + b)_b from the w before this hinge, then w += WJT[:, b] dx
+__device__ __forceinline__ void hinge_update(const StepArgs& a, int k) {
+    const int lo = a.ws.hlohi[2 * k], hi = a.ws.hlohi[2 * k + 1];
+    const double* J = a.ws.hJ + 60 * (size_t)k;
+    double* wlo = a.ws.hw + 6 * (size_t)lo;
+    double* whi = a.ws.hw + 6 * (size_t)hi;
+    double jw[5], delta[5];
+    for (int row = 0; row < 5; ++row) jw[row] = jrow_dot(J + 12 * row, wlo, whi);
+    for (int row = 0; row < 5; ++row) {
+        const size_t i = 5 * (size_t)k + row;
+        const double xo = a.ws.hx[i];
+        const double xn = xo - a.ws.hr[i] * (jw[row] + a.ws.hb[i]);
+        a.ws.hx[i] = xn;
+        delta[row] = xn - xo;
+    }
+    for (int side = 0; side < 2; ++side) {
+        const int bd = side ? hi : lo;
+        if (a.bd.fixed[bd]) continue;
+        double* wb = side ? whi : wlo;
+        const double* Ws = a.ws.hWJT + 60 * (size_t)k + 6 * side;
+        for (int d = 0; d < 6; ++d) {
+            double t = 0.0;
+            for (int row = 0; row < 5; ++row) t += Ws[12 * row + d] * delta[row];
+            wb[d] = wb[d] + t;
+        }
+    }
+}
+
+// levels of the scene's hinges in their serial order (a hinge follows the earlier hinges on its non-fixed
+// bodies), by one thread: hlev_order[h0 ..] lists the hinges level by level, ascending inside a level, and
+// hlev_ptr[h0 + s + l - 1] .. hlev_ptr[h0 + s + l] index the hinges of level l.  Returns the number of levels.
+template <class G>
+__device__ int hinge_levels(const StepArgs& a, const G& g, const SceneRange& R, int s, int h0, int h1) {
+    int L = 0;
+    if (g.rank() == 0) {
+        int32_t* last = a.ws.hlast;
+        for (int b = R.b0; b < R.b1; ++b) last[b] = 0;
+        int32_t* lev = a.ws.hlev;
+        for (int k = h0; k < h1; ++k) {
+            const int lo = a.ws.hlohi[2 * k], hi = a.ws.hlohi[2 * k + 1];
+            const int l0 = a.bd.fixed[lo] ? 0 : last[lo], l1 = a.bd.fixed[hi] ? 0 : last[hi];
+            const int l = 1 + max(l0, l1);
+            if (!a.bd.fixed[lo]) last[lo] = l;
+            if (!a.bd.fixed[hi]) last[hi] = l;
+            lev[k] = l;
+            L = max(L, l);
+        }
+        int32_t* ptr = a.ws.hlev_ptr + h0 + s;
+        for (int l = 0; l <= L; ++l) ptr[l] = 0;
+        for (int k = h0; k < h1; ++k) ptr[lev[k]]++;
+        for (int l = 1; l <= L; ++l) ptr[l] += ptr[l - 1];          // ptr[l] = end of level l
+        for (int l = L; l >= 1; --l) ptr[l] = ptr[l - 1];          // ptr[l] = start of level l, used as
+        ptr[0] = 0;                                                  // the level's cursor: after the fill
+        for (int k = h0; k < h1; ++k) a.ws.hlev_order[h0 + ptr[lev[k]]++] = k;   // it is the level's end
+    }
+    g.sync();
+    return g.imax(L);
+}
+
+// The reference stepper's Gauss-Seidel loop over [contacts (when any), hinges] (gauss_seidel_solver.py:14-101):
+// every iteration sweeps each problem in turn (each with its own accumulators w, built from its own x at the
+// start of its sweep), accepts or rolls back its iterate against that problem's own last merit and adapts its
+// r-factors; the convergence tests use the largest merit of the iteration.  FP64, serial order, merit rule.
+template <class G>
+__device__ void solve_scene_hinges(const StepArgs& a, const G& g, int s, double* w_smem, int smem_bodies) {
+    const int max_it = a.pr.max_iterations;
+    double* x = a.ws.x;
+    double* sol = a.out.contact_sol;
+    const double* b = a.ws.b;
+    double* r = a.ws.r;
+    const SceneRange R = scene_range(a, s);
+    const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
+    const int h0 = a.bd.scene_hinge_start[s], h1 = a.bd.scene_hinge_start[s + 1];
+    rb_scene_stats* st = a.out.stats + s;
+    double* hist = (a.out.residuals && a.pr.profiling) ? a.out.residuals + (size_t)s * a.caps.max_iterations : nullptr;
+    if (g.rank() == 0) {
+        st->n_contacts = K; st->contact_start = R.c0; st->iterations = -1; st->exitcode = -1;
+        st->merit = 0.0; st->residual = 0.0; st->post_iterations = -1; st->post_exitcode = -1;
+        st->n_levels = 0; st->fp32_sweeps = 0;
+    }
+    if (hist) for (int i = g.rank(); i < max_it; i += g.size()) hist[i] = INFINITY;
+    const bool on_chip = w_smem != nullptr && nb <= smem_bodies;
+    const WView w = {on_chip ? w_smem : a.ws.w + 6 * R.b0, R.b0};
+    const int L = K > 0 ? scene_levels(a, g, R, s) : 0;
+    const int HL = hinge_levels(a, g, R, s, h0, h1);
+    if (g.rank() == 0) st->n_levels = L;
+    const int* hptr = a.ws.hlev_ptr + h0 + s;
+    double last_c = INFINITY, last_h = INFINITY, global_last = INFINITY, shown = 0.0;
+    int iterations = max_it, exitcode = 0;
+    for (int it = 0; it < max_it; ++it) {
+        double gm = 0.0;
+        if (K > 0) {   // Contacts.sweep, then the accept / roll-back rule
+            scene_wjt(a, g, R, x, w);
+            gs_sweep_levels(a, g, R, s, L, b, r, x, w, false);
+            double m = 0.0;
+            for (int i = 4 * R.c0 + g.rank(); i < 4 * R.c1; i += g.size()) m = nanmax(m, fabs(x[i] - sol[i]));
+            const double merit = g.max(m);
+            const bool reject = merit > last_c;
+            const bool inc = !reject && last_c - merit < a.pr.too_small_merit_change;
+            for (int i = 4 * R.c0 + g.rank(); i < 4 * R.c1; i += g.size()) {
+                if (reject) { r[i] = a.pr.nu_reduce * r[i]; x[i] = sol[i]; }
+                else { sol[i] = x[i]; if (inc) r[i] = a.pr.nu_increase * r[i]; }
+            }
+            if (reject) gm = gm > last_c ? gm : last_c;
+            else { last_c = merit; gm = gm > merit ? gm : merit; }
+            g.sync();
+        }
+        {              // Hinges.sweep, then the same rule with the hinge problem's own merit and r-factors
+            hinge_wjt(a, g, R);
+            for (int l = 1; l <= HL; ++l) {
+                for (int i = hptr[l - 1] + g.rank(); i < hptr[l]; i += g.size()) hinge_update(a, a.ws.hlev_order[h0 + i]);
+                g.sync();
+            }
+            double m = 0.0;
+            for (int i = 5 * h0 + g.rank(); i < 5 * h1; i += g.size()) m = nanmax(m, fabs(a.ws.hx[i] - a.ws.hsol[i]));
+            const double merit = g.max(m);
+            const bool reject = merit > last_h;
+            const bool inc = !reject && last_h - merit < a.pr.too_small_merit_change;
+            for (int i = 5 * h0 + g.rank(); i < 5 * h1; i += g.size()) {
+                if (reject) { a.ws.hr[i] = a.pr.nu_reduce * a.ws.hr[i]; a.ws.hx[i] = a.ws.hsol[i]; }
+                else { a.ws.hsol[i] = a.ws.hx[i]; if (inc) a.ws.hr[i] = a.pr.nu_increase * a.ws.hr[i]; }
+            }
+            if (reject) gm = gm > last_h ? gm : last_h;
+            else { last_h = merit; gm = gm > merit ? gm : merit; }
+            g.sync();
+        }
+        if (hist && g.rank() == 0) hist[it] = gm;
+        shown = gm;
+        bool stop = false;
+        if (gm < a.pr.absolute_tolerance) { stop = true; exitcode = 1; }
+        else if (fabs(gm - global_last) < a.pr.relative_tolerance * global_last) { stop = true; exitcode = 2; }
+        global_last = gm;
+        if (stop) { iterations = it; break; }
+    }
+    if (a.out.hinge_sol)
+        for (int i = 5 * h0 + g.rank(); i < 5 * h1; i += g.size()) a.out.hinge_sol[i] = a.ws.hsol[i];
+    if (g.rank() == 0) { st->iterations = iterations; st->exitcode = exitcode; st->merit = shown; }
+    g.sync();
+}
+
 // The proximal solve of one scene (gauss_seidel_solver.py:14 / solver_interface.py:123).
 template <class G>
 __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, double* w_smem, int smem_bodies) {
+    if (!post && a.bd.n_hinges > 0 && a.bd.scene_hinge_start[s + 1] > a.bd.scene_hinge_start[s]) {
+        solve_scene_hinges(a, g, s, w_smem, smem_bodies);
+        return;
+    }
     const int scheme = post ? RB_SCHEME_RIGID_GS : a.pr.scheme;
     const bool rigid = scheme == RB_SCHEME_RIGID_GS;
     const bool jacobi = scheme == RB_SCHEME_JACOBI || scheme == RB_SCHEME_JACOBI_HYBRID;
@@ -1801,6 +2091,19 @@ __global__ void k_integrate(const StepArgs a) {
         body_wjt_dot(a.ws, b, a.out.contact_sol, dc);
         for (int d = 0; d < 6; ++d) du[d] = du[d] + dc[d];
     }
+    if (a.bd.n_hinges > 0 && !a.bd.fixed[b] && a.ws.hbody_ptr[b + 1] > a.ws.hbody_ptr[b]) {
+        // then the hinge problem's WJT sol (hinges.py:52), hinges ascending, 5 rows each
+        for (int d = 0; d < 6; ++d) {
+            double t = 0.0;
+            for (int e = a.ws.hbody_ptr[b]; e < a.ws.hbody_ptr[b + 1]; ++e) {
+                const int code = a.ws.hbody_list[e];
+                const int k = code >> 1, side = code & 1;
+                const double* Wk = a.ws.hWJT + 60 * (size_t)k + 6 * side;
+                for (int row = 0; row < 5; ++row) t += Wk[12 * row + d] * a.ws.hsol[5 * (size_t)k + row];
+            }
+            du[d] = du[d] + t;
+        }
+    }
     for (int d = 0; d < 6; ++d) ub[d] = ub[d] + du[d];
     if (a.bd.fixed[b]) return;
     position_update(a.bd.x + 7 * b, ub, a.pr.dt);
@@ -1994,8 +2297,10 @@ int rb_workspace_bytes(const rb_bodies* bd, const rb_caps* caps, size_t* bytes) 
     if (bd->n_bodies < 0 || bd->n_body_vertices < 0 || bd->n_body_triangles < 0 || bd->n_clusters < 0 ||
         caps->pair_capacity < 0 || caps->item_capacity < 0 || caps->contact_capacity < 0)
         return fail(RB_ERR_ARG, "rb_workspace_bytes: negative size");
+    if (bd->n_hinges < 0) return fail(RB_ERR_ARG, "rb_workspace_bytes: negative hinge count");
     *bytes = rb::layout(nullptr, nullptr, bd->n_bodies, bd->n_body_vertices, bd->n_body_triangles, bd->n_clusters,
-                        caps->pair_capacity, caps->item_capacity, caps->contact_capacity, bd->n_scenes);
+                        caps->pair_capacity, caps->item_capacity, caps->contact_capacity, bd->n_scenes,
+                        bd->n_hinges);
     return RB_OK;
 }
 
@@ -2065,6 +2370,12 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
         return fail(RB_ERR_UNSUPPORTED, "rb_step: unknown solver scheme");
     if (pr->ordering != RB_ORDER_SERIAL && pr->ordering != RB_ORDER_COLOURED)
         return fail(RB_ERR_ARG, "rb_step: unknown contact ordering");
+    if (bd->n_hinges < 0 || (bd->n_hinges > 0 && (!bd->scene_hinge_start || !bd->hinge_bodies || !bd->hinge_frames)))
+        return fail(RB_ERR_ARG, "rb_step: hinge arrays missing");
+    if (bd->n_hinges > 0 && (pr->scheme != RB_SCHEME_RIGID_GS || pr->termination != RB_TERMINATE_MERIT ||
+                             pr->ordering != RB_ORDER_SERIAL || pr->precision != RB_PRECISION_FP64))
+        return fail(RB_ERR_UNSUPPORTED, "rb_step: hinge joints are solved with the reference stepper's rule only "
+                                        "(rigid Gauss-Seidel, merit termination, serial order, FP64)");
     // launch shapes
     const int small_slab = pr->fp32_small_slab > 0 ? pr->fp32_small_slab : kS32SmallSlab;
     const int mid_slab = pr->fp32_mid_slab > 0 ? pr->fp32_mid_slab : kS32MidSlab;
@@ -2099,7 +2410,7 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     StepArgs a;
     a.sh = *sh; a.bd = *bd; a.caps = *caps; a.pr = *pr; a.out = *out;
     rb::layout(&a.ws, (char*)workspace, bd->n_bodies, n_body_vertices, n_body_triangles, n_clusters,
-               caps->pair_capacity, caps->item_capacity, caps->contact_capacity, bd->n_scenes);
+               caps->pair_capacity, caps->item_capacity, caps->contact_capacity, bd->n_scenes, bd->n_hinges);
     if (n_body_vertices <= 0 || n_body_triangles <= 0 || n_clusters <= 0)
         return fail(RB_ERR_ARG, "rb_step: bodies without geometry");
     const int N = bd->n_bodies;
@@ -2139,6 +2450,10 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     prof_mark(prof, 4, st);
     // contact problem
     k_contacts<<<G, 128, 0, st>>>(a); note_launch();
+    if (bd->n_hinges > 0) {   // the hinge problem of every scene that has hinges
+        k_hinge_lists<<<blocks_for(bd->n_scenes, 64), 64, 0, st>>>(a); note_launch();
+        k_hinges<<<blocks_for(bd->n_hinges, 128), 128, 0, st>>>(a); note_launch();
+    }
     k_body_contacts_count<<<G, 256, 0, st>>>(a); note_launch();
     scan(a.ws.bc_ptr, nullptr, N, a.ws.scan_tmp, nullptr, st);
     k_body_contacts_fill<<<G, 256, 0, st>>>(a); note_launch();

@@ -20,8 +20,6 @@ def _force_kind(force):
 
 def scene_arrays(engine, shape_cache=None):
     """Flat arrays of one scene.  ``shape_cache`` (dict) reuses the packed arrays of unchanged shapes."""
-    if getattr(engine, "hinges", None):
-        raise NotImplementedError("hinge joints (constraints/hinges.py) are not implemented by the GPU stepper")
     out = {}
     shapes = list(engine.shapes.values())
     shape_index = {id(s): i for i, s in enumerate(shapes)}
@@ -98,6 +96,14 @@ def scene_arrays(engine, shape_cache=None):
     out["material_mu"] = mu
     out["material_epsilon"] = eps
     out["params"] = np.array([float(getattr(engine.params, f)) for f in PARAM_FIELDS])
+    # hinge joints (types.py:304), Hinge.idx order: parent/child body indices, body-frame arms and axes
+    hinges = sorted(getattr(engine, "hinges", {}).values(), key=lambda h: h.idx)
+    if [h.idx for h in hinges] != list(range(len(hinges))):
+        raise RuntimeError("hinge indices are not 0 .. n-1")
+    out["hinge_bodies"] = np.array([[h.parent.idx, h.child.idx] for h in hinges], dtype=np.int32).reshape(-1, 2)
+    out["hinge_frames"] = np.array([np.concatenate([np.asarray(h.arm_p, np.float64), np.asarray(h.arm_c, np.float64),
+                                                    np.asarray(h.axis_p, np.float64), np.asarray(h.axis_c, np.float64)])
+                                    for h in hinges], dtype=np.float64).reshape(-1, 12)
     return out
 
 
@@ -110,6 +116,9 @@ def static_signature(engine):
                     b.material, tuple(id(f) for f in b.forces)))
     for s in engine.shapes.values():
         sig.append((id(s), id(s.mesh.V), id(s.mesh.T), id(s.grid), id(s.grid.values)))
+    for h in sorted(getattr(engine, "hinges", {}).values(), key=lambda h: h.idx):
+        sig.append((id(h), h.parent.idx, h.child.idx,
+                    tuple(np.concatenate([np.ravel(h.arm_p), np.ravel(h.arm_c), np.ravel(h.axis_p), np.ravel(h.axis_c)]))))
     for f in engine.forces.values():
         sig.append((id(f), tuple(np.ravel(getattr(f, "up", [0.0]))), float(getattr(f, "g", 0.0)),
                     float(getattr(f, "alpha", 0.0)), float(getattr(f, "beta", 0.0))))
@@ -201,4 +210,13 @@ def engine_from_arrays(arrays, names=None):
     for name, v in zip(PARAM_FIELDS, p):
         cur = getattr(engine.params, name)
         setattr(engine.params, name, type(cur)(v) if not isinstance(cur, bool) else bool(v))
+    bodies = list(engine.bodies.values())
+    hb = np.asarray(a.get("hinge_bodies", np.zeros((0, 2))), np.int64).reshape(-1, 2)
+    hf = np.asarray(a.get("hinge_frames", np.zeros((0, 12))), np.float64).reshape(-1, 12)
+    for k in range(len(hb)):
+        h = TY.Hinge("hinge%d" % k)
+        h.idx = k
+        h.parent, h.child = bodies[int(hb[k, 0])], bodies[int(hb[k, 1])]
+        h.arm_p, h.arm_c, h.axis_p, h.axis_c = hf[k, 0:3].copy(), hf[k, 3:6].copy(), hf[k, 6:9].copy(), hf[k, 9:12].copy()
+        engine.hinges[h.name] = h
     return engine

@@ -57,6 +57,23 @@ def quat_axis_angle(radians, axis):
     return np.array([c, s * n[0], s * n[1], s * n[2]], dtype=np.float64)
 
 
+def orthonormal_frame(n):
+    """(t, b, n) completing the direction n (vector3.py:75 make_orthonormal_vectors): the tangent guess is the
+    coordinate axis along the smallest |n_i| (a later tie wins), b = unit(n x t), t = b x n."""
+    n = np.asarray(n, dtype=np.float64) / np.linalg.norm(n)
+    a = np.fabs(n)
+    t = np.zeros(3)
+    if a[0] <= a[1] and a[0] <= a[2]:
+        t = np.array([1.0, 0.0, 0.0])
+    if a[1] <= a[0] and a[1] <= a[2]:
+        t = np.array([0.0, 1.0, 0.0])
+    if a[2] <= a[0] and a[2] <= a[1]:
+        t = np.array([0.0, 0.0, 1.0])
+    b = np.cross(n, t)
+    b = b / np.linalg.norm(b)
+    return np.cross(b, n), b, n
+
+
 def quat_from_matrix(M):
     """Rotation matrix to quaternion (the trace / largest-diagonal method of quaternion.py:132)."""
     tr = M[0, 0] + M[1, 1] + M[2, 2]

@@ -123,6 +123,8 @@ class SceneBlock:
         self.n_materials = M
         self.material_mu = np.asarray(scene["material_mu"], np.float64).reshape(M * M, 3)
         self.material_eps = np.asarray(scene["material_epsilon"], np.float64).reshape(M * M)
+        self.hinge_bodies = np.asarray(scene.get("hinge_bodies", np.zeros((0, 2))), np.int64).reshape(-1, 2)
+        self.hinge_frames = np.asarray(scene.get("hinge_frames", np.zeros((0, 12))), np.float64).reshape(-1, 12)
         self.x0 = np.concatenate([np.asarray(scene["body_r"]).reshape(nb, 3),
                                   np.asarray(scene["body_q"]).reshape(nb, 4)], axis=1)
         self.u0 = np.concatenate([np.asarray(scene["body_v"]).reshape(nb, 3),
@@ -161,10 +163,12 @@ def pack_blocks(blocks, library):
     if max(P["n_body_vertices"], P["n_body_triangles"], 48 * P["n_clusters"]) >= 2 ** 31:
         raise ValueError("scene batch too large for 32-bit topology indices")
     P["n_bodies"] = int(nb.sum())
+    W.hinge_arrays(P, [b.hinge_bodies for b in blocks], [b.hinge_frames for b in blocks])
     return P
 
 
 _BODY_TENSORS = {
+    "scene_hinge_start": torch.int32, "hinge_bodies": torch.int32, "hinge_frames": torch.float64,
     "scene_start": torch.int32, "body_shape": torch.int32, "body_mass": torch.float64,
     "body_inertia": torch.float64, "body_fixed": torch.uint8, "body_material": torch.int32,
     "force_ptr": torch.int32, "force_list": torch.int32, "scene_force_start": torch.int32,
@@ -216,6 +220,8 @@ class ServingBatch(W.DeviceWorld):
         self.rb_shapes = library.rb_shapes
         bd = N.RbBodies()
         bd.n_bodies, bd.n_scenes, bd.n_forces = nbod, self.n_scenes, self.n_forces
+        self.n_hinges = int(P["n_hinges"])
+        bd.n_hinges = self.n_hinges
         bd.n_body_vertices, bd.n_body_triangles, bd.n_clusters = self.n_body_vertices, self.n_body_triangles, self.n_clusters
         bd.max_scene_bodies = int(np.diff(self.scene_start).max())
         for f, key in W.BODY_FIELDS.items():
@@ -293,6 +299,8 @@ class ServingBatch(W.DeviceWorld):
         out.needed = self.t_status.data_ptr() + 8
         out.cache_key, out.cache_sol = self.t_cache_key.data_ptr(), self.t_cache_sol.data_ptr()
         out.cache_count = self.t_cache_count.data_ptr()
+        self.t_hsol = self._pooled("hsol", max(1, 5 * self.n_hinges), torch.float64)
+        out.hinge_sol = self.t_hsol.data_ptr()
         self.rb_outputs = out
         nbytes = ctypes.c_size_t(0)
         N.check(self.lib.rb_workspace_bytes(ctypes.byref(self.rb_bodies), ctypes.byref(self.caps), ctypes.byref(nbytes)),

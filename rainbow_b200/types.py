@@ -137,6 +137,21 @@ class ContactPoint:
         self.g = gap
 
 
+class Hinge:
+    """types.py:304 Hinge: a revolute joint between a parent and a child body; arm_* and axis_* are the joint
+    origin and axis in each body's own frame (set by api.set_hinge)."""
+
+    def __init__(self, name):
+        self.name = name
+        self.idx = None
+        self.parent = None
+        self.child = None
+        self.arm_p = None
+        self.arm_c = None
+        self.axis_p = None
+        self.axis_c = None
+
+
 class Parameters:
     """types.py:356 Parameters, plus the solver options of the GPU stepper.
 

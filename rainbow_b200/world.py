@@ -82,6 +82,7 @@ PACKED_DTYPES = {
     "scene_material_count": torch.int32, "material_mu": torch.float64, "material_eps": torch.float64,
     "body_v0": torch.int32, "body_t0": torch.int32, "body_c0": torch.int32, "vert_body": torch.int32,
     "tri_body": torch.int32, "clu_body": torch.int32, "x": torch.float64, "u": torch.float64,
+    "scene_hinge_start": torch.int32, "hinge_bodies": torch.int32, "hinge_frames": torch.float64,
 }
 
 # rb_bodies field -> packed array
@@ -92,7 +93,8 @@ BODY_FIELDS = {
     "scene_material_offset": "scene_material_offset", "scene_material_count": "scene_material_count",
     "material_mu": "material_mu", "material_eps": "material_eps", "body_v0": "body_v0", "body_t0": "body_t0",
     "body_c0": "body_c0", "vert_body": "vert_body", "tri_body": "tri_body", "clu_body": "clu_body",
-    "x": "x", "u": "u",
+    "x": "x", "u": "u", "scene_hinge_start": "scene_hinge_start", "hinge_bodies": "hinge_bodies",
+    "hinge_frames": "hinge_frames",
 }
 
 
@@ -207,7 +209,26 @@ def pack_scenes(scenes):
     P["material_mu"] = np.array(mu, np.float64).reshape(-1)
     P["material_eps"] = np.array(eps, np.float64)
     P["n_forces"] = len(fkind)
+    hinge_arrays(P, [np.asarray(s_["hinge_bodies"], np.int64).reshape(-1, 2) if "hinge_bodies" in s_
+                     else np.zeros((0, 2), np.int64) for s_ in scenes],
+                 [np.asarray(s_["hinge_frames"], np.float64).reshape(-1, 12) if "hinge_frames" in s_
+                  else np.zeros((0, 12)) for s_ in scenes])
     return P
+
+
+def hinge_arrays(P, bodies, frames):
+    """Hinges of the packed scenes (per scene: parent/child body indices local to the scene, 12 frame values)
+    into P: scene_hinge_start, hinge_bodies (global body indices), hinge_frames, n_hinges."""
+    start = np.asarray(P["scene_start"], np.int64)
+    counts = np.array([len(hb) for hb in bodies], np.int64)
+    P["n_hinges"] = int(counts.sum())
+    P["scene_hinge_start"] = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+    if P["n_hinges"]:
+        P["hinge_bodies"] = np.concatenate([hb + start[i] for i, hb in enumerate(bodies)]).astype(np.int32).reshape(-1)
+        P["hinge_frames"] = np.concatenate(frames).astype(np.float64).reshape(-1)
+    else:
+        P["hinge_bodies"] = np.zeros(2, np.int32)
+        P["hinge_frames"] = np.zeros(12)
 
 
 class DeviceWorld:
@@ -261,6 +282,8 @@ class DeviceWorld:
         bd = N.RbBodies()
         bd.n_bodies, bd.n_scenes = self.n_bodies, self.n_scenes
         bd.n_forces = self.n_forces
+        self.n_hinges = int(P["n_hinges"])
+        bd.n_hinges = self.n_hinges
         bd.n_body_vertices, bd.n_body_triangles, bd.n_clusters = self.n_body_vertices, self.n_body_triangles, self.n_clusters
         bd.max_scene_bodies = int(np.diff(self.scene_start).max())
         for f, key in BODY_FIELDS.items():
@@ -297,6 +320,8 @@ class DeviceWorld:
             self.t_cache_count = torch.zeros(1, dtype=torch.int32, device=dev)
         out.cache_key, out.cache_sol = self.t_cache_key.data_ptr(), self.t_cache_sol.data_ptr()
         out.cache_count = self.t_cache_count.data_ptr()
+        self.t_hsol = torch.zeros(max(1, 5 * self.n_hinges), dtype=torch.float64, device=dev)
+        out.hinge_sol = self.t_hsol.data_ptr()
         self.rb_outputs = out
         nbytes = ctypes.c_size_t(0)
         N.check(self.lib.rb_workspace_bytes(ctypes.byref(self.rb_bodies), ctypes.byref(self.caps), ctypes.byref(nbytes)),
@@ -358,6 +383,10 @@ class DeviceWorld:
         raw = self.t_stats.cpu().numpy().tobytes()
         size = ctypes.sizeof(N.RbSceneStats)
         return [N.RbSceneStats.from_buffer_copy(raw[i * size:(i + 1) * size]) for i in range(self.n_scenes)]
+
+    def hinge_solution(self):
+        """The hinge problem's solution of the last step (5 values per hinge, Hinge.idx order per scene)."""
+        return self.t_hsol[:5 * self.n_hinges].cpu().numpy()
 
     def n_contacts_total(self):
         return int(self.t_status[1].item())

@@ -8,7 +8,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-FIXTURES = ["boxes8", "tower6", "spheres", "flags", "c1_boxes64"]
+FIXTURES = ["boxes8", "tower6", "spheres", "flags", "c1_boxes64", "hinges", "hinges_stab"]
 
 
 def pytest_configure(config):

@@ -33,6 +33,9 @@ def _assert_step(world, d, s, scene=0):
     assert st.iterations == d["step_iterations"][s]
     assert st.exitcode == d["step_exitcode"][s]
     assert st.post_iterations == d["step_post_iterations"][s]
+    if world.n_hinges and "step_hinge_sol_len" in d:
+        np.testing.assert_array_equal(world.hinge_solution(), step_slice(d, "hinge_sol", s),
+                                      err_msg="step %d hinge sol" % s)
     x, u = world.state()
     b0, b1 = world.scene_start[scene], world.scene_start[scene + 1]
     np.testing.assert_array_equal(x[b0:b1].ravel(), d["step_x"][s], err_msg="step %d x" % s)
@@ -321,3 +324,40 @@ def test_coloured_fp32_refine_meets_the_tolerance():
                             termination="residual_fixed_r", residual_tolerance=1e-6))
     st = w.stats()[0]
     assert st.exitcode == 3 and st.residual <= 1e-6 and st.fp32_sweeps > 0
+
+
+def test_hinge_scenes_batched_with_others_equal_alone():
+    """Hinge chains packed with contact-only scenes: every scene gives the same bits as alone (the hinge
+    problem of one scene never sees another scene's bodies)."""
+    from rainbow_b200 import world as W
+    ds = [load_fixture(n) for n in ("boxes8", "hinges", "tower6", "hinges_stab")]
+    params = W.params_from_vector(ds[1]["params"])
+    cap = int(params["max_iterations"])
+    alone = []
+    for d in ds:
+        w = _world(d, max_iterations=cap)
+        for _ in range(5):
+            w.step(W.make_rb_params(params))
+        alone.append((w.state(), w.hinge_solution() if w.n_hinges else None))
+    batch = W.DeviceWorld(ds, max_iterations=cap)
+    for _ in range(5):
+        batch.step(W.make_rb_params(params))
+    x, u = batch.state()
+    hs = batch.hinge_solution()
+    h = 0
+    for i, ((xa, ua), ha) in enumerate(alone):
+        b0, b1 = batch.scene_start[i], batch.scene_start[i + 1]
+        np.testing.assert_array_equal(x[b0:b1], xa)
+        np.testing.assert_array_equal(u[b0:b1], ua)
+        if ha is not None:
+            np.testing.assert_array_equal(hs[h:h + len(ha)], ha)
+            h += len(ha)
+
+
+def test_hinges_reject_other_solver_settings():
+    from rainbow_b200 import _native as N
+    from rainbow_b200 import world as W
+    d = load_fixture("hinges")
+    w = _world(d)
+    with pytest.raises(N.NativeError, match="hinge"):
+        w.step(W.make_rb_params(W.params_from_vector(d["params"]), termination="residual_fixed_r"))

@@ -53,11 +53,23 @@ def test_pack_two_scenes():
     np.testing.assert_array_equal(P["u"].reshape(-1, 6)[:na, :3], a["body_v"])
 
 
-def test_hinges_are_rejected():
-    engine = engine_io.engine_from_arrays(load_fixture("boxes8"))
-    engine.hinges = {"h": object()}
-    with pytest.raises(NotImplementedError):
-        engine_io.scene_arrays(engine)
+def test_hinges_round_trip_through_engines_and_packing():
+    """Hinge joints (types.py:304) survive engine -> arrays -> engine, and packing rebases their body indices
+    onto each scene's body range."""
+    from rainbow_b200 import world as W
+    d = load_fixture("hinges")
+    back = engine_io.scene_arrays(engine_io.engine_from_arrays(d))
+    np.testing.assert_array_equal(back["hinge_bodies"], d["hinge_bodies"])
+    np.testing.assert_array_equal(back["hinge_frames"], d["hinge_frames"])
+    e = load_fixture("hinges_stab")
+    P = W.pack_scenes([load_fixture("boxes8"), d, e])
+    nb0 = len(load_fixture("boxes8")["body_mass"])
+    nb1 = len(d["body_mass"])
+    H1, H2 = len(d["hinge_bodies"]), len(e["hinge_bodies"])
+    np.testing.assert_array_equal(P["scene_hinge_start"], [0, 0, H1, H1 + H2])
+    hb = P["hinge_bodies"].reshape(-1, 2)
+    np.testing.assert_array_equal(hb[:H1], d["hinge_bodies"] + nb0)
+    np.testing.assert_array_equal(hb[H1:], e["hinge_bodies"] + nb0 + nb1)
 
 
 def test_massless_body_is_rejected():
@@ -80,3 +92,25 @@ def test_reads_reference_engine_objects():
     d = load_fixture("boxes8")
     for k in SCENE_KEYS:
         np.testing.assert_array_equal(np.asarray(a[k]), np.asarray(d[k]).reshape(np.asarray(a[k]).shape), err_msg=k)
+
+
+def test_api_set_hinge_matches_the_reference_frames():
+    """api.create_hinge / set_hinge (api.py:71-156) give the arms and axes the reference stored for the
+    golden hinge chain (world-mode origin and axis, sockets in both bodies' frames)."""
+    from rainbow_b200 import api as A
+    d = load_fixture("hinges")
+    engine = engine_io.engine_from_arrays(d)
+    names = list(engine.bodies)
+    engine.hinges = {}
+    for k in range(len(d["hinge_bodies"])):
+        p, c = names[d["hinge_bodies"][k][0]], names[d["hinge_bodies"][k][1]]
+        A.create_hinge(engine, "h%d" % k)
+        origin = (engine.bodies[p].r + engine.bodies[c].r) / 2.0
+        A.set_hinge(engine, "h%d" % k, p, c, origin, np.array([0.0, 0.0, 1.0]), mode="world")
+    back = engine_io.scene_arrays(engine)
+    np.testing.assert_array_equal(back["hinge_bodies"], d["hinge_bodies"])
+    np.testing.assert_allclose(back["hinge_frames"], d["hinge_frames"], rtol=0, atol=1e-15)
+    with pytest.raises(RuntimeError):
+        A.create_hinge(engine, "h0")
+    with pytest.raises(ValueError):
+        A.set_hinge(engine, "h0", names[0], names[1], np.zeros(3), np.array([0.0, 0.0, 1.0]), mode="nope")
