@@ -48,6 +48,7 @@ struct Workspace {
     float* c32;          // 48K   compact FP32 contacts of the scenes whose copy does not fit in shared memory
     uint32_t* blist32;   // 2K    ... their per-body contact lists
     uint16_t* pos32;     // K     ... and level-order positions
+    float* body32;       // 16N   ... and, for scenes with too many bodies for the slab, their body records
     double* b;           // 4K
     double* diag;        // 4K
     double* r;           // 4K
@@ -96,7 +97,7 @@ inline size_t layout(Workspace* ws, char* base, int64_t N, int64_t NV, int64_t N
     take(w->item_pair, C); take(w->item_tri, C); take(w->item_flag, C);
     take(w->item_p, 3 * C); take(w->item_n, 3 * C); take(w->item_g, C);
     take(w->lohi, 2 * K); take(w->c_scene, K); take(w->bc_list, 2 * K);
-    take(w->J, 48 * K); take(w->WJT, 48 * K); take(w->c32, 48 * K); take(w->blist32, 2 * K); take(w->pos32, K);
+    take(w->J, 48 * K); take(w->WJT, 48 * K); take(w->c32, 48 * K); take(w->blist32, 2 * K); take(w->pos32, K); take(w->body32, 16 * N);
     take(w->b, 4 * K); take(w->diag, 4 * K); take(w->r, 4 * K); take(w->x, 4 * K); take(w->xold, 4 * K);
     take(w->mu, K);
     take(w->ckey, 2 * K);

@@ -1628,18 +1628,23 @@ __host__ __device__ inline size_t s32_align(size_t v) { return (v + 15) & ~size_
 // shared memory of a scene's FP32 copy; with in_l2 the contact rows, the level-order positions and the
 // per-body contact lists live in global memory (L2) and only the bodies, body indices and level and list
 // starts stay on chip
-__host__ __device__ inline size_t s32_bytes(int K, int nb, bool in_l2 = false) {
+__host__ __device__ inline size_t s32_bytes(int K, int nb, bool in_l2 = false, bool bodies_global = false) {
     return (in_l2 ? 0 : s32_align(sizeof(float) * (size_t)K * kS32Floats) + s32_align(sizeof(uint16_t) * (size_t)K) +
                         s32_align(sizeof(uint32_t) * 2 * (size_t)K)) +
-           s32_align(sizeof(float) * (size_t)nb * kS32BodyFloats) + s32_align(sizeof(uint32_t) * (size_t)K) +
+           (bodies_global ? 0 : s32_align(sizeof(float) * (size_t)nb * kS32BodyFloats)) +
+           s32_align(sizeof(uint32_t) * (size_t)K) +
            s32_align(sizeof(uint16_t) * (size_t)(K + 1)) + s32_align(sizeof(uint16_t) * (size_t)(nb + 1));
 }
-__device__ __forceinline__ S32Scene s32_carve(char* base, int K, int nb, const StepArgs* l2 = nullptr, int c0 = 0) {
+// with l2, the contact rows, positions and body lists go to the workspace; with bodies_global the body
+// records too (the scene's team is the only reader and writer, so block barriers keep them consistent)
+__device__ __forceinline__ S32Scene s32_carve(char* base, int K, int nb, const StepArgs* l2 = nullptr, int c0 = 0,
+                                              bool bodies_global = false, int b0 = 0) {
     S32Scene f;
     size_t o = 0;
     auto take = [&](size_t bytes) { char* p = base + o; o += s32_align(bytes); return p; };
     f.c = l2 ? l2->ws.c32 + kS32Floats * (size_t)c0 : (float*)take(sizeof(float) * (size_t)K * kS32Floats);
-    f.body = (float*)take(sizeof(float) * (size_t)nb * kS32BodyFloats);
+    f.body = (l2 && bodies_global) ? l2->ws.body32 + kS32BodyFloats * (size_t)b0
+                                   : (float*)take(sizeof(float) * (size_t)nb * kS32BodyFloats);
     f.lohi = (uint32_t*)take(sizeof(uint32_t) * (size_t)K);
     f.pos = l2 ? l2->ws.pos32 + c0 : (uint16_t*)take(sizeof(uint16_t) * (size_t)K);
     f.lptr = (uint16_t*)take(sizeof(uint16_t) * (size_t)(K + 1));
@@ -1790,7 +1795,7 @@ __device__ __forceinline__ float s32_residual(const StepArgs& a, const G& g, con
 // +m^-1, -m^-1, I_lo^-1 or I_hi^-1 to it.  Every lane runs the same instructions (lane-dependent offsets);
 // all shared-memory reads are float4 / float2.
 template <class G, bool kL2>
-__device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, float rscale) {
+__device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, float rscale, bool bodies_global) {
     const int q = g.rank() & 3, slot = g.rank() >> 2, nslot = g.size() >> 2;
     const int base = (threadIdx.x & 31) & ~3;
     const unsigned qm = 0xfu << base;
@@ -1805,6 +1810,12 @@ __device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, 
             const int lines = (int)(((size_t)(next_end - end) * kS32Floats * sizeof(float) + 127) / 128);
             for (int t = g.rank(); t < lines; t += g.size())
                 asm volatile("prefetch.global.L1 [%0];" ::"l"(p0 + 128 * (size_t)t));
+            if (bodies_global)   // and the body records those rows touch
+                for (int i = end + g.rank(); i < next_end; i += g.size()) {
+                    const uint32_t lh = f.lohi[i];
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(f.body + kS32BodyFloats * (size_t)(lh & 0xffffu)));
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(f.body + kS32BodyFloats * (size_t)(lh >> 16)));
+                }
         }
         // every lane of a quad runs the same trip count, so the quad's shuffles see all four lanes
         for (int i0 = start; i0 < end; i0 += nslot) {
@@ -1981,13 +1992,16 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
         const SceneRange R = scene_range(a, s);
         const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
         if (K == 0 || K > 32767 || nb > 32767) continue;   // 16-bit positions and list offsets
-        if (kL2) {   // the scenes no slab holds whole, and whose bodies and level order fit one
-            if (s32_bytes(K, nb) <= lo_bytes || s32_bytes(K, nb, true) > slab) continue;
+        bool bodies_global = false;
+        if (kL2) {   // the scenes no slab holds whole: contact rows in L2, and the bodies too if they do not fit
+            if (s32_bytes(K, nb) <= lo_bytes) continue;
+            bodies_global = s32_bytes(K, nb, true) > slab;
+            if (s32_bytes(K, nb, true, bodies_global) > slab) continue;
         } else {
             const size_t bytes = s32_bytes(K, nb);
             if (bytes <= lo_bytes || bytes > slab) continue;
         }
-        const S32Scene f = s32_carve(my_slab, K, nb, kL2 ? &a : nullptr, R.c0);
+        const S32Scene f = s32_carve(my_slab, K, nb, kL2 ? &a : nullptr, R.c0, bodies_global, R.b0);
         const int L = s32_load(a, g, R, s, f, coloured);
         if (g.rank() == 0) a.ws.nlev[s] = L;
         float res = s32_residual(a, g, R, f);   // the warm-started iterate may already be good enough
@@ -1995,7 +2009,7 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
         int sweeps = 0, stalls = 0, corrections = 0;
         for (;;) {
             while (res > tol && sweeps < budget) {
-                s32_sweep<G, kL2>(g, f, L, rscale);
+                s32_sweep<G, kL2>(g, f, L, rscale, bodies_global);
                 ++sweeps;
                 if (sweeps % interval == 0 || sweeps == budget) {
                     res = s32_residual(a, g, R, f);
@@ -2139,34 +2153,37 @@ __global__ void k_post_apply(const StepArgs a) {
 }
 
 // energies and largest penetration (state_storage.py:188, contacts.py:222): thread per scene, body order
+// one warp per scene: the deepest gap and the pair / candidate counts by warp reductions (order-free), the
+// energy sums by lane 0 in body order (their rounding follows state_storage.py:188-237)
 __global__ void k_scene_summary(const StepArgs a) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (s >= a.bd.n_scenes || a.ws.counters[kAbort]) return;
     rb_scene_stats* st = a.out.stats + s;
     const SceneRange R = scene_range(a, s);
     double gap = 0.0;
-    for (int k = R.c0; k < R.c1; ++k) gap = fmin(gap, a.out.contact_g[k]);
-    st->max_penetration = -gap;
-    {
-        const int p0 = a.ws.pair_cnt[R.b0], p1 = a.ws.pair_cnt[R.b1];
-        st->n_pairs = p1 - p0;
-        int ovl = 0, cand = 0;
-        if (a.pr.profiling)
-            for (int p = p0; p < p1; ++p) { ovl += a.ws.pair_ovl[p]; cand += a.ws.pair_itemsA[p]; }
-        st->n_candidates = cand;
-        st->n_leaf_overlaps = ovl;
+    for (int k = R.c0 + lane; k < R.c1; k += 32) gap = fmin(gap, a.out.contact_g[k]);
+    for (int o = 16; o > 0; o >>= 1) gap = fmin(gap, __shfl_xor_sync(0xffffffffu, gap, o));
+    const int p0 = a.ws.pair_cnt[R.b0], p1 = a.ws.pair_cnt[R.b1];
+    int ovl = 0, cand = 0;
+    if (a.pr.profiling)
+        for (int p = p0 + lane; p < p1; p += 32) { ovl += a.ws.pair_ovl[p]; cand += a.ws.pair_itemsA[p]; }
+    for (int o = 16; o > 0; o >>= 1) {
+        ovl += __shfl_xor_sync(0xffffffffu, ovl, o);
+        cand += __shfl_xor_sync(0xffffffffu, cand, o);
     }
+    if (lane != 0) return;
+    st->max_penetration = -gap;
+    st->n_pairs = p1 - p0;
+    st->n_candidates = cand;
+    st->n_leaf_overlaps = ovl;
     if (!a.pr.profiling) return;
-    double G[3] = {0.0, 0.0, 0.0};
     int has_gravity = 0;
     for (int f = a.bd.scene_force_start[s]; f < a.bd.scene_force_start[s + 1]; ++f)
-        if (a.bd.force_kind[f] == 0) {
-            const double* fp = a.bd.force_params + 4 * f;
-            for (int i = 0; i < 3; ++i) G[i] = G[i] + fp[1 + i] * fp[0];
-            has_gravity = 1;
-        }
-    // the per-body terms come from k_body_energy; summed here in body order (state_storage.py:188-237)
+        if (a.bd.force_kind[f] == 0) has_gravity = 1;
+    // the per-body terms come from k_body_energy
     double kinetic = 0.0, potential = 0.0;
+#pragma unroll 8
     for (int b = R.b0; b < R.b1; ++b) {
         if (a.bd.fixed[b]) continue;
         if (has_gravity) potential += a.ws.eterm[2 * (size_t)b + 1];
@@ -2506,7 +2523,7 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
         k_post_apply<<<blocks_for(N, 128), 128, 0, st>>>(a); note_launch();
     }
     if (prof) { k_body_energy<<<blocks_for(N, 128), 128, 0, st>>>(a); note_launch(); }
-    k_scene_summary<<<blocks_for(bd->n_scenes, 64), 64, 0, st>>>(a); note_launch();
+    k_scene_summary<<<blocks_for(32 * (int64_t)bd->n_scenes, 128), 128, 0, st>>>(a); note_launch();
     k_cache_store<<<G, 256, 0, st>>>(a); note_launch();
     k_finish<<<1, 1, 0, st>>>(a); note_launch();
     prof_mark(prof, 6, st);

@@ -37,3 +37,28 @@ def test_fp32_modes_track_fp64_on_the_mass_ratio_tower():
         # converged steps: the same share meets the 1e-6 tolerance; the rest: residuals of the FP64 size
         assert np.mean(rm <= 1e-6) >= np.mean(r64 <= 1e-6) - 0.05, (mode, np.mean(rm <= 1e-6), np.mean(r64 <= 1e-6))
         assert np.median(rm) <= max(1e-6, 2.0 * np.median(r64)), (mode, np.median(rm), np.median(r64))
+
+
+def test_fp32_solve_of_a_scene_with_more_bodies_than_a_slab_holds():
+    """4097 bodies (the 16^3 box/sphere lattice on a ground): too many for one SM's shared memory, so the FP32
+    phase keeps contact rows and body records in global memory.  It must run (FP32 sweeps > 0) and agree with
+    the FP64 solve of the same step to a small fraction of the velocity scale, at a residual of the same
+    size."""
+    from rainbow_b200 import engine_io, scenes
+    from rainbow_b200 import world as W
+    arrays = engine_io.scene_arrays(scenes.mixed_lattice(n=16, resolution=16))
+    params = W.params_from_vector(arrays["params"])
+    kw = dict(termination="residual_fixed_r", residual_tolerance=1e-6, residual_interval=4)
+    w = W.DeviceWorld(arrays, max_iterations=100)
+    for _ in range(30):
+        w.step(W.make_rb_params(params, **kw))
+    x0, u0 = w.state()
+    out = {}
+    for mode in ("fp64", "fp32_refine"):
+        w.set_state(x0, u0)
+        w.step(W.make_rb_params(params, precision=mode, **kw))
+        out[mode] = (w.state()[1], w.stats()[0])
+    (u64, s64), (u32, s32) = out["fp64"], out["fp32_refine"]
+    assert s64.n_contacts > 0 and s32.fp32_sweeps > 0
+    assert np.abs(u32 - u64).max() <= 1e-3 * np.abs(u64).max()
+    assert s32.residual <= 2.0 * s64.residual + 1e-6
