@@ -35,7 +35,7 @@ sys.path.insert(0, ROOT)
 
 
 
-PROFILED_SOLVE_DRAM_BYTES = 44_989_440   # FP32 solve kernels of one batch1024 step (ncu, cold caches)
+PROFILED_SOLVE_DRAM_BYTES = 46_865_664   # FP32 solve kernels of one batch1024 step (ncu, cold caches)
 LONG_SWEEPS = 4000   # iteration cap of the converged reference solve the error figures are measured against
 
 
