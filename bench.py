@@ -333,7 +333,7 @@ def run_ours(args):
     if not args.no_autotune and args.workload == "batch1024":
         from rainbow_b200 import autotune
         t0 = time.perf_counter()
-        best, info = autotune.tune(world, rp, steps=3)
+        best, info = autotune.tune(world, rp)
         autotune.apply(rp, best)
         autotune.apply(rp_prof, best)
         tuning = dict(best, seconds=time.perf_counter() - t0, **info)

@@ -71,9 +71,10 @@ def signature(world):
     return (world.n_scenes, int(round(np.log(max(world.n_bodies, 1)) * 100)), int(nb.max()))
 
 
-def tune(world, rb_params, steps=3, rounds=2, memo=True):
-    """Fastest launch shapes for `world` stepped with `rb_params` (device time of `steps` steps per trial,
-    each trial from the same saved state, warm-start cache included).  The world is left in its saved state."""
+def tune(world, rb_params, steps=4, rounds=2, memo=True, repeats=3):
+    """Fastest launch shapes for `world` stepped with `rb_params`: a trial times `steps` steps from the same
+    saved state (warm-start cache included) `repeats` times and keeps the median.  The world is left in its
+    saved state."""
     import torch
     key = signature(world) if memo else None
     if key is not None and key in _memo:
@@ -97,15 +98,18 @@ def tune(world, rb_params, steps=3, rounds=2, memo=True):
         rp = apply(type(rb_params).from_buffer_copy(rb_params), setting)
         restore()
         world.launch(rp)                      # warm
-        restore()
-        torch.cuda.synchronize(world.device)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(steps):
-            world.launch(rp)
-        e1.record(stream)
-        torch.cuda.synchronize(world.device)
-        return e0.elapsed_time(e1) / steps
+        times = []
+        for _ in range(repeats):
+            restore()
+            torch.cuda.synchronize(world.device)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                world.launch(rp)
+            e1.record(stream)
+            torch.cuda.synchronize(world.device)
+            times.append(e0.elapsed_time(e1) / steps)
+        return float(np.median(times))
 
     best, best_ms, n = coordinate_descent(cost, rounds=rounds)
     restore()

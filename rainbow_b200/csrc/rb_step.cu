@@ -1414,6 +1414,7 @@ __device__ void solve_scene_hinges(const StepArgs& a, const G& g, int s, double*
 // The proximal solve of one scene (gauss_seidel_solver.py:14 / solver_interface.py:123).
 template <class G>
 __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, double* w_smem, int smem_bodies) {
+    if (!post && a.ws.fin32[s]) return;   // finished by the FP32 phase
     if (!post && a.bd.n_hinges > 0 && a.bd.scene_hinge_start[s + 1] > a.bd.scene_hinge_start[s]) {
         solve_scene_hinges(a, g, s, w_smem, smem_bodies);
         return;
@@ -1891,7 +1892,8 @@ __device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, 
 // FP64 problem's solution: at the current x the corrected FP32 problem has the FP64 problem's residual.  The
 // FP32 w must hold W J^T x for this x (the residual test just before rebuilt it).
 template <class G>
-__device__ __forceinline__ double s32_correct(const StepArgs& a, const G& g, const SceneRange& R, const S32Scene& f) {
+__device__ __forceinline__ double s32_correct(const StepArgs& a, const G& g, const SceneRange& R, const S32Scene& f,
+                                              bool correct = true) {
     const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
     const int* order = a.ws.lev_order + R.c0;
     double* w64 = a.ws.w + 6 * (size_t)R.b0;   // the scene's FP64 accumulators, unused until the FP64 solve
@@ -1927,8 +1929,10 @@ __device__ __forceinline__ double s32_correct(const StepArgs& a, const G& g, con
             for (int c = 0; c < 6; ++c) v64 = fma(J[c], wl[c], v64);
             for (int c = 0; c < 6; ++c) v64 = fma(J[6 + c], wh[c], v64);
             float* row = f.c + kS32Floats * i + 12 * q;
-            const float v32 = s32_jw(row, q, wl32, wh32) + row[3];
-            row[3] += (float)(v64 - (double)v32);
+            if (correct) {
+                const float v32 = s32_jw(row, q, wl32, wh32) + row[3];
+                row[3] += (float)(v64 - (double)v32);
+            }
             x[q] = (double)row[11];
             z[q] = x[q] - v64 / a.ws.diag[4 * k + q];
         }
@@ -2007,6 +2011,7 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
         float res = s32_residual(a, g, R, f);   // the warm-started iterate may already be good enough
         float best = res;
         int sweeps = 0, stalls = 0, corrections = 0;
+        double r64 = -1.0;   // FP64 residual of the current iterate, once evaluated
         for (;;) {
             while (res > tol && sweeps < budget) {
                 s32_sweep<G, kL2>(g, f, L, rscale, bodies_global);
@@ -2023,25 +2028,51 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
             // problem's b by the FP64 defect and sweep on in FP32 (a few times at most)
             if (a.pr.precision != RB_PRECISION_FP32_REFINE || sweeps >= budget || corrections >= kS32Corrections)
                 break;
-            const double r64 = s32_correct(a, g, R, f);
+            r64 = s32_correct(a, g, R, f);
             ++corrections;
             if (r64 <= a.pr.residual_tolerance) break;
+            r64 = -1.0;   // the sweeps that follow change the iterate
             res = s32_residual(a, g, R, f);
             best = res;
             stalls = 0;
         }
+        // the FP64 residual of the iterate decides whether FP64 sweeps follow; when none do, this kernel
+        // finishes the scene (solution, statistics) and the FP64 solver skips it
+        if (r64 < 0.0) r64 = s32_correct(a, g, R, f, false);
+        const bool finished = r64 <= a.pr.residual_tolerance || sweeps >= max_it ||
+                              a.pr.precision == RB_PRECISION_FP32;
         for (int t = g.rank(); t < 4 * K; t += g.size()) {   // back to contact order
             const int i = t >> 2, q = t & 3;
-            a.ws.x[4 * (size_t)a.ws.lev_order[R.c0 + i] + q] = (double)f.c[kS32Floats * i + 12 * q + 11];
+            const size_t k4 = 4 * (size_t)a.ws.lev_order[R.c0 + i] + q;
+            const double xv = (double)f.c[kS32Floats * i + 12 * q + 11];
+            a.ws.x[k4] = xv;
+            if (finished) a.out.contact_sol[k4] = xv;
         }
-        if (g.rank() == 0) a.ws.sweeps32[s] = sweeps;
+        if (finished && a.out.residuals && a.pr.profiling)
+            for (int i = g.rank(); i < max_it; i += g.size()) a.out.residuals[(size_t)s * a.caps.max_iterations + i] = INFINITY;
+        if (g.rank() == 0) {
+            a.ws.sweeps32[s] = sweeps;
+            a.ws.fin32[s] = finished ? 1 : 0;
+            if (finished) {
+                const bool ok = r64 <= a.pr.residual_tolerance;
+                rb_scene_stats* st = a.out.stats + s;
+                st->n_contacts = K; st->contact_start = R.c0;
+                st->iterations = ok ? max(sweeps - 1, 0) : max_it;
+                st->exitcode = ok ? 3 : 0;
+                st->merit = r64; st->residual = r64;
+                st->post_iterations = -1; st->post_exitcode = -1;
+                st->n_levels = L; st->fp32_sweeps = sweeps;
+            }
+        }
         g.sync();
     }
 }
 
 __global__ void k_sweeps32_init(const StepArgs a) {
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.bd.n_scenes; s += gridDim.x * blockDim.x)
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.bd.n_scenes; s += gridDim.x * blockDim.x) {
         a.ws.sweeps32[s] = -1;
+        a.ws.fin32[s] = 0;
+    }
 }
 
 constexpr int kSolveBlock = 128;   // threads per scene in the block solver (levels rarely hold more contacts)
