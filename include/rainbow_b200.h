@@ -204,6 +204,8 @@ typedef struct rb_scene_stats {
     double kinetic_energy;        /* state_storage.py:188 (profiling only) */
     double potential_energy;
     double max_penetration;       /* contacts.py:222 */
+    double solve_start_us;        /* device clock (%globaltimer, microseconds) when the scene's solve started (profiling only) */
+    double solve_us;              /* device time of the scene's contact solve, FP32 and FP64 phases (profiling only) */
 } rb_scene_stats;
 
 /* Outputs: device buffers sized by rb_caps.contact_capacity / n_scenes / max_iterations. */

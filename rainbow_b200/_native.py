@@ -77,6 +77,7 @@ class RbSceneStats(ctypes.Structure):
         ("n_leaf_overlaps", _i32), ("n_grid_lookups", _i32),
         ("n_levels", _i32), ("fp32_sweeps", _i32), ("merit", ctypes.c_double), ("residual", ctypes.c_double), ("kinetic_energy", ctypes.c_double),
         ("potential_energy", ctypes.c_double), ("max_penetration", ctypes.c_double),
+        ("solve_start_us", ctypes.c_double), ("solve_us", ctypes.c_double),
     ]
 
 

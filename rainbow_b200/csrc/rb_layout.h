@@ -64,6 +64,7 @@ struct Workspace {
     int32_t* sweeps32;   // S   FP32 sweeps done per scene (-1: the scene is solved in FP64 only)
     int32_t* nlev;       // S   levels (or colours) the FP32 phase found for the scene
     int32_t* fin32;      // S   1 when the FP32 phase finished the scene (no FP64 sweeps needed)
+    int32_t* list32;     // S   the FP32 phase's scenes by size class, larger contact counts first
     double* eterm;       // 2N  kinetic and potential energy of each body (profiled steps)
     // hinge joints (H of them): J and W J^T blocks (5 rows x 12), b, diag, r, x, sol, body pairs (ascending),
     // level order and starts per scene, per-body hinge lists, the hinge problem's own accumulators w
@@ -104,7 +105,7 @@ inline size_t layout(Workspace* ws, char* base, int64_t N, int64_t NV, int64_t N
     take(w->ckey, 2 * K);
     take(w->lev_of, K); take(w->lev_order, K); take(w->lev_ptr, K + S + 1); take(w->lev_cur, K + S + 1);
     take(w->cpred, 2 * K);
-    take(w->sweeps32, S); take(w->nlev, S); take(w->fin32, S); take(w->eterm, 2 * N);
+    take(w->sweeps32, S); take(w->nlev, S); take(w->fin32, S); take(w->list32, S); take(w->eterm, 2 * N);
     take(w->hJ, 60 * H); take(w->hWJT, 60 * H); take(w->hb, 5 * H); take(w->hdiag, 5 * H); take(w->hr, 5 * H);
     take(w->hx, 5 * H); take(w->hsol, 5 * H); take(w->hlohi, 2 * H); take(w->hlev_order, H);
     take(w->hlev_ptr, H + S + 1); take(w->hbody_ptr, N + 1); take(w->hbody_list, 2 * H); take(w->hw, 6 * N);

@@ -1411,10 +1411,35 @@ __device__ void solve_scene_hinges(const StepArgs& a, const G& g, int s, double*
     g.sync();
 }
 
-// The proximal solve of one scene (gauss_seidel_solver.py:14 / solver_interface.py:123).
+// device clock in microseconds (the global nanosecond timer)
+__device__ __forceinline__ double device_us() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return 1e-3 * (double)t;
+}
+
+template <class G>
+__device__ void solve_scene_body(const StepArgs& a, const G& g, int s, int post, double* w_smem, int smem_bodies);
+
+// The proximal solve of one scene (gauss_seidel_solver.py:14 / solver_interface.py:123); with profiling on,
+// its device time goes to the scene's statistics (added to the FP32 phase's time when one ran).
 template <class G>
 __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, double* w_smem, int smem_bodies) {
     if (!post && a.ws.fin32[s]) return;   // finished by the FP32 phase
+    const bool timed = !post && a.pr.profiling;
+    const double t0 = timed ? device_us() : 0.0;
+    solve_scene_body(a, g, s, post, w_smem, smem_bodies);
+    if (!post && g.rank() == 0) {
+        rb_scene_stats* st = a.out.stats + s;
+        const bool fp32_phase = a.pr.precision != RB_PRECISION_FP64 && a.ws.sweeps32[s] >= 0;
+        if (!timed) { st->solve_start_us = 0.0; st->solve_us = 0.0; }
+        else if (fp32_phase) st->solve_us += device_us() - t0;
+        else { st->solve_start_us = t0; st->solve_us = device_us() - t0; }
+    }
+}
+
+template <class G>
+__device__ void solve_scene_body(const StepArgs& a, const G& g, int s, int post, double* w_smem, int smem_bodies) {
     if (!post && a.bd.n_hinges > 0 && a.bd.scene_hinge_start[s + 1] > a.bd.scene_hinge_start[s]) {
         solve_scene_hinges(a, g, s, w_smem, smem_bodies);
         return;
@@ -1587,8 +1612,9 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
 // ---------------------------------------------------------------------------------------------------------
 // FP32 phase of the FP32 precision modes.  A scene's whole contact problem is copied into shared memory as
 // FP32 in a compact form and swept there, level by level (or colour by colour), with the fixed-r rule until
-// the FP32 residual meets the tolerance, stalls near FP32 rounding, or the sweep budget is spent; the FP64
-// solver then tests the iterate in FP64 and refines it with the sweeps left.
+// the FP32 residual meets the tolerance, stalls near FP32 rounding, or the sweep budget is spent; the iterate
+// is then tested in FP64 and, if it misses the tolerance, refined by the same team with FP64 sweeps (the
+// budget left).
 //
 // Compact form.  A contact's Jacobian rows are [lin_lo | ang_lo | lin_hi | ang_hi] with lin_hi = -lin_lo
 // (the frame direction, zero on the torsion row) and W J^T = (m^-1 lin, I_w^-1 ang) per body, so a contact
@@ -1605,6 +1631,7 @@ __device__ void solve_scene(const StepArgs& a, const G& g, int s, int post, doub
 // ---------------------------------------------------------------------------------------------------------
 constexpr int kS32Floats = 48;                       // floats per contact
 constexpr int kQueueFp32 = 5;                        // counters[5..8]: scene queues of the four size classes
+constexpr int kClassEnd32 = 9;                       // counters[9..12]: end of each class's range in list32
 constexpr int kS32BodyFloats = 16;                   // floats per body
 constexpr int kFp32Block = 128;                      // threads per block of the FP32 launches
 constexpr int kFp32BlockMax = 256;                   // ... and of the launch for scenes beyond any slab
@@ -1870,12 +1897,11 @@ __device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, 
                 const float dw0 = fmaf(i0, S0, fmaf(i1, S1, i2 * S2));
                 const float dw1 = fmaf(i1, S0, fmaf(i3, S1, i4 * S2));
                 const float dw2 = fmaf(i2, S0, fmaf(i4, S1, i5 * S2));
+                // the lane's three components of w: linear (0-2) or angular (3-5), without a branch
+                const int off = linear ? 0 : 3;
+                const float o0 = linear ? w0.x : w0.w, o1 = linear ? w0.y : w1.x, o2 = linear ? w0.z : w1.y;
                 if (w1.w == 0.0f) {   // not a fixed body
-                    if (linear) {
-                        B[0] = w0.x + dw0; B[1] = w0.y + dw1; B[2] = w0.z + dw2;
-                    } else {
-                        B[3] = w0.w + dw0; B[4] = w1.x + dw1; B[5] = w1.y + dw2;
-                    }
+                    B[off] = o0 + dw0; B[off + 1] = o1 + dw1; B[off + 2] = o2 + dw2;
                 }
             }
         }
@@ -1952,6 +1978,62 @@ __device__ __forceinline__ double s32_correct(const StepArgs& a, const G& g, con
     return mres / (mx > 1.0 ? mx : 1.0);
 }
 
+// size class of a scene's FP32 copy: 0 and 1 warp teams with small and mid slabs, 2 block teams with the
+// large slab, 3 block teams with the contact rows in L2; -1 for a scene the FP32 phase leaves to FP64
+__host__ __device__ inline int s32_class(int K, int nb, size_t small_slab, size_t mid_slab) {
+    if (K == 0 || K > 32767 || nb > 32767) return -1;   // 16-bit positions and list offsets
+    const size_t bytes = s32_bytes(K, nb);
+    if (bytes <= small_slab) return 0;
+    if (bytes <= mid_slab) return 1;
+    if (bytes <= (size_t)kFp32LargeSmem) return 2;
+    const bool bodies_global = s32_bytes(K, nb, true) > (size_t)kFp32LargeSmem;
+    return s32_bytes(K, nb, true, bodies_global) <= (size_t)kFp32LargeSmem ? 3 : -1;
+}
+
+// Per-scene FP32 bookkeeping of the step, and the scene list of each size class with the larger contact
+// counts first, so that every team's next scene is one of its class and the longest chains start first.
+// One block.
+__global__ void __launch_bounds__(1024) k_fp32_classes(const StepArgs a, size_t small_slab, size_t mid_slab) {
+    __shared__ int cnt[4 * 32];
+    const int S = a.bd.n_scenes;
+    // no lists after an overflow: the contact ranges are not valid then, and the solvers do not run
+    const bool fp32 = a.pr.precision != RB_PRECISION_FP64 && !a.ws.counters[kAbort];
+    for (int t = threadIdx.x; t < 4 * 32; t += blockDim.x) cnt[t] = 0;
+    __syncthreads();
+    auto slot = [&](int s) -> int {   // class x 32 + contact-count bucket (descending), or -1
+        const SceneRange R = scene_range(a, s);
+        const int K = R.c1 - R.c0;
+        const int c = s32_class(K, R.b1 - R.b0, small_slab, mid_slab);
+        if (c < 0) return -1;
+        const int lg = (int)(3.0f * log2f((float)K + 1.0f));   // buckets of a factor 2^(1/3)
+        return 32 * c + 31 - min(lg, 31);
+    };
+    for (int s = threadIdx.x; s < S; s += blockDim.x) {
+        a.ws.sweeps32[s] = -1;
+        a.ws.fin32[s] = 0;
+        if (fp32) {
+            const int t = slot(s);
+            if (t >= 0) atomicAdd(&cnt[t], 1);
+        }
+    }
+    __syncthreads();
+    if (!fp32) return;
+    if (threadIdx.x == 0) {   // counts -> starts; class ends to the counters
+        int run = 0;
+        for (int t = 0; t < 4 * 32; ++t) {
+            const int n = cnt[t];
+            cnt[t] = run;
+            run += n;
+            if ((t & 31) == 31) a.ws.counters[kClassEnd32 + (t >> 5)] = run;
+        }
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < S; s += blockDim.x) {
+        const int t = slot(s);
+        if (t >= 0) a.ws.list32[atomicAdd(&cnt[t], 1)] = s;
+    }
+}
+
 template <class G>
 __device__ __forceinline__ int team_next(const G& g, int* counter, int* slot) {
     int s = 0;
@@ -1962,6 +2044,12 @@ __device__ __forceinline__ int team_next(const G& g, int* counter, int* slot) {
     s = *slot;
     __syncthreads();
     return s;
+}
+
+// the FP64 solve of a scene as a call of its own, so that it does not raise the FP32 kernel's registers
+template <class G>
+__device__ __noinline__ void solve_scene_call(const StepArgs& a, const G& g, int s) {
+    solve_scene(a, g, s, 0, nullptr, 0);
 }
 
 // FP32 phase for the scenes whose compact copy takes lo_bytes < bytes <= slab bytes; G = WarpGroup gives
@@ -1990,9 +2078,13 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
     if (a.pr.relaxation > 0.0) rs *= a.pr.relaxation;
     const float rscale = (float)rs;
     const bool coloured = a.pr.scheme == RB_SCHEME_COLOURED_GS || a.pr.ordering == RB_ORDER_COLOURED;
+    const int cls = queue - kQueueFp32;
+    const int list0 = cls == 0 ? 0 : a.ws.counters[kClassEnd32 + cls - 1];
+    const int list1 = a.ws.counters[kClassEnd32 + cls];
     for (;;) {
-        const int s = team_next(g, a.ws.counters + queue, &next_slot);
-        if (s >= a.bd.n_scenes) break;
+        const int idx = list0 + team_next(g, a.ws.counters + queue, &next_slot);
+        if (idx >= list1) break;
+        const int s = a.ws.list32[idx];
         const SceneRange R = scene_range(a, s);
         const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
         if (K == 0 || K > 32767 || nb > 32767) continue;   // 16-bit positions and list offsets
@@ -2005,6 +2097,7 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
             const size_t bytes = s32_bytes(K, nb);
             if (bytes <= lo_bytes || bytes > slab) continue;
         }
+        const double t0 = a.pr.profiling ? device_us() : 0.0;
         const S32Scene f = s32_carve(my_slab, K, nb, kL2 ? &a : nullptr, R.c0, bodies_global, R.b0);
         const int L = s32_load(a, g, R, s, f, coloured);
         if (g.rank() == 0) a.ws.nlev[s] = L;
@@ -2037,7 +2130,8 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
             stalls = 0;
         }
         // the FP64 residual of the iterate decides whether FP64 sweeps follow; when none do, this kernel
-        // finishes the scene (solution, statistics) and the FP64 solver skips it
+        // finishes the scene (solution, statistics), and when some do, this team runs them right away, so
+        // the FP64 solver launched after the FP32 phase skips the scene either way
         if (r64 < 0.0) r64 = s32_correct(a, g, R, f, false);
         const bool finished = r64 <= a.pr.residual_tolerance || sweeps >= max_it ||
                               a.pr.precision == RB_PRECISION_FP32;
@@ -2053,9 +2147,11 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
         if (g.rank() == 0) {
             a.ws.sweeps32[s] = sweeps;
             a.ws.fin32[s] = finished ? 1 : 0;
+            rb_scene_stats* st = a.out.stats + s;
+            st->solve_start_us = t0;
+            st->solve_us = a.pr.profiling ? device_us() - t0 : 0.0;
             if (finished) {
                 const bool ok = r64 <= a.pr.residual_tolerance;
-                rb_scene_stats* st = a.out.stats + s;
                 st->n_contacts = K; st->contact_start = R.c0;
                 st->iterations = ok ? max(sweeps - 1, 0) : max_it;
                 st->exitcode = ok ? 3 : 0;
@@ -2065,13 +2161,11 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
             }
         }
         g.sync();
-    }
-}
-
-__global__ void k_sweeps32_init(const StepArgs a) {
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.bd.n_scenes; s += gridDim.x * blockDim.x) {
-        a.ws.sweeps32[s] = -1;
-        a.ws.fin32[s] = 0;
+        if (!finished) {   // FP64 sweeps with the budget left, by this team at once (w in global memory)
+            solve_scene_call(a, g, s);
+            if (g.rank() == 0) a.ws.fin32[s] = 1;
+            g.sync();
+        }
     }
 }
 
@@ -2380,28 +2474,48 @@ int ensure_kernel_attributes() {
     return RB_OK;
 }
 
-// Side streams of the FP32 size classes, per host thread and device, made on the thread's first step on
-// the device (an uncaptured call).  Each step forks them from its stream with an event and joins them back,
-// which a stream capture records as parallel branches.
+// Side streams of the FP32 size classes, per host thread and device: kSideSets sets, all made on the thread's
+// first step on the device (an uncaptured call).  Each caller stream gets a set of its own (round robin over
+// the sets, so steps on different streams run their solves concurrently); a step forks its set from its
+// stream with an event and joins it back, which a stream capture records as parallel branches.
 constexpr int kSideStreams = 4;
+constexpr int kSideSets = 4;
 struct SideStreams {
     cudaStream_t s[kSideStreams] = {};
     cudaEvent_t fork = nullptr, join[kSideStreams] = {};
 };
-thread_local SideStreams g_side[64];
-int side_streams(SideStreams** out) {
+struct SideSets {
+    SideStreams set[kSideSets];
+    const void* key[kSideSets] = {};
+    int next = 0;
+    bool made = false;
+};
+thread_local SideSets g_side[64];
+int side_streams(cudaStream_t caller, SideStreams** out) {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return fail(RB_ERR_CUDA, "rb_step: no current device");
-    SideStreams& ss = g_side[dev];
-    if (!ss.fork) {
-        cudaError_t e = cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming);
-        for (int c = 0; c < kSideStreams && e == cudaSuccess; ++c) {
-            e = cudaStreamCreateWithFlags(&ss.s[c], cudaStreamNonBlocking);
-            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ss.join[c], cudaEventDisableTiming);
+    SideSets& ss = g_side[dev];
+    if (!ss.made) {
+        cudaError_t e = cudaSuccess;
+        for (int k = 0; k < kSideSets && e == cudaSuccess; ++k) {
+            SideStreams& t = ss.set[k];
+            e = cudaEventCreateWithFlags(&t.fork, cudaEventDisableTiming);
+            for (int c = 0; c < kSideStreams && e == cudaSuccess; ++c) {
+                e = cudaStreamCreateWithFlags(&t.s[c], cudaStreamNonBlocking);
+                if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t.join[c], cudaEventDisableTiming);
+            }
         }
         if (e != cudaSuccess) return fail(RB_ERR_CUDA, std::string("rb_step: side streams: ") + cudaGetErrorString(e));
+        ss.made = true;
     }
-    *out = &ss;
+    int k = 0;
+    while (k < kSideSets && ss.key[k] != (const void*)caller) ++k;
+    if (k == kSideSets) {   // a caller stream not seen before takes the next set
+        k = ss.next;
+        ss.next = (ss.next + 1) % kSideSets;
+        ss.key[k] = (const void*)caller;
+    }
+    *out = &ss.set[k];
     return RB_OK;
 }
 }  // namespace
@@ -2517,13 +2631,13 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     const int smem_bodies = bd->max_scene_bodies <= kSolveSmemBodies ? bd->max_scene_bodies : 0;
     const size_t block_smem = (size_t)6 * sizeof(double) * (smem_bodies > 0 ? smem_bodies : 1);
     const int bg = bd->n_scenes < 148 * 16 ? bd->n_scenes : 148 * 16;
-    k_sweeps32_init<<<blocks_for(bd->n_scenes, 256), 256, 0, st>>>(a); note_launch();
+    k_fp32_classes<<<1, 1024, 0, st>>>(a, small_slab, mid_slab); note_launch();
     if (pr->precision != RB_PRECISION_FP64) {
         // FP32 phase, four size classes side by side: warp teams with 28 KB slabs (8 scenes per SM), warp
         // teams with 56 KB slabs (4 per SM), block teams with 224 KB (1 per SM), and 256-thread block teams
         // for the scenes beyond that, whose contact rows stay in L2
         SideStreams* ss = nullptr;
-        rc = side_streams(&ss);
+        rc = side_streams(st, &ss);
         if (rc != RB_OK) return rc;
         cudaEventRecord(ss->fork, st);
         for (int c = 0; c < kSideStreams; ++c) cudaStreamWaitEvent(ss->s[c], ss->fork, 0);
