@@ -24,7 +24,6 @@ struct Workspace {
     int32_t* bc_fill;    // N
     // per body-vertex / triangle / cluster
     double* Vw;          // 3 NV world vertices
-    double* leaf;        // 6 NT leaf boxes
     double* clu;         // 6 NC cluster boxes
     // pairs
     int32_t* pairs;      // 2P
@@ -94,7 +93,7 @@ inline size_t layout(Workspace* ws, char* base, int64_t N, int64_t NV, int64_t N
     take(w->Winv, 9 * N); take(w->dux, 6 * N); take(w->du, 6 * N); take(w->root, 6 * N);
     take(w->w, 6 * N); take(w->w2, 6 * N);
     take(w->pair_cnt, N + 1); take(w->bc_ptr, N + 1); take(w->bc_fill, N);
-    take(w->Vw, 3 * NV); take(w->leaf, 6 * NT); take(w->clu, 6 * NC);
+    take(w->Vw, 3 * NV); take(w->clu, 6 * NC);
     take(w->pairs, 2 * P); take(w->pair_items, P + 1); take(w->pair_itemsA, P); take(w->pair_cont, P + 1); take(w->pair_ovl, P);
     take(w->item_pair, C); take(w->item_tri, C); take(w->item_flag, C);
     take(w->item_p, 3 * C); take(w->item_n, 3 * C); take(w->item_g, C);

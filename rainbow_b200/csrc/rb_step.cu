@@ -6,7 +6,7 @@
 //
 //   k_bodies          forces, gyroscopic torque, world inverse inertia, W f_ext      state_storage.py:43-185
 //   k_world_vertices  rotate_array(q, V) + r for every body vertex                   collision_detection.py:32
-//   k_clusters        leaf boxes (k-DOP K=3 + envelope), 32-leaf cluster boxes        kdop_bvh.py:52, kdop.py:53
+//   k_clusters        32-leaf cluster boxes (unions of k-DOP K=3 leaf boxes + envelope) kdop_bvh.py:52, kdop.py:53
 //   k_roots           body boxes (the BVH root)                                         kdop_bvh.py:215
 //   k_pairs           body pairs in combinations() order whose roots overlap           collision_detection.py:70
 //   k_mid             per pair, the triangles of each side whose leaf overlaps a leaf   kdop_bvh.py:127, :234
@@ -244,8 +244,25 @@ __global__ void k_world_vertices(const StepArgs a, int n_verts) {
     st3(a.ws.Vw + 3 * (size_t)g, d3{p.x + xb[0], p.y + xb[1], p.z + xb[2]});
 }
 
-// leaf boxes (kdop.py:53 make with K=3: min/max of the triangle's coordinates -/+ envelope) and the box of
-// every run of 32 consecutive triangles of a body; one warp per cluster
+// leaf box of triangle t of a body (kdop.py:53 make with K=3: min/max of the triangle's world coordinates
+// -/+ envelope), from the body's world vertices Vw and its shape's triangles T; L = (lo[3], hi[3])
+__device__ __forceinline__ void leaf_box(const int32_t* T, const double* Vw, int t, double env, double* L) {
+    const int32_t* tri = T + 3 * (size_t)t;
+    const int v[3] = {tri[0], tri[1], tri[2]};
+    for (int axis = 0; axis < 3; ++axis) {
+        double l = INFINITY, h = -INFINITY;
+        for (int k = 0; k < 3; ++k) {
+            const double pr = Vw[3 * v[k] + axis];
+            if (pr < l) l = pr;
+            if (pr > h) h = pr;
+        }
+        L[axis] = l - env;
+        L[3 + axis] = h + env;
+    }
+}
+
+// the box of every run of 32 consecutive triangles of a body (the union of their leaf boxes); one warp per
+// cluster.  Leaf boxes are not stored: the mid phase recomputes the few it tests from the world vertices.
 __global__ void k_clusters(const StepArgs a, int n_clusters) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= n_clusters) return;
@@ -254,23 +271,11 @@ __global__ void k_clusters(const StepArgs a, int n_clusters) {
     const int s = a.bd.shape[b];
     const int nt = a.sh.t_off[s + 1] - a.sh.t_off[s];
     const int t = 32 * c + lane;
-    const double env = a.pr.envelope;
     double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     if (t < nt) {
-        const int32_t* tri = a.sh.T + 3 * (size_t)(a.sh.t_off[s] + t);
-        const double* Vw = a.ws.Vw + 3 * (size_t)a.bd.body_v0[b];
-        for (int axis = 0; axis < 3; ++axis) {
-            double l = INFINITY, h = -INFINITY;
-            for (int k = 0; k < 3; ++k) {
-                const double pr = Vw[3 * tri[k] + axis];
-                if (pr < l) l = pr;
-                if (pr > h) h = pr;
-            }
-            lo[axis] = l - env;
-            hi[axis] = h + env;
-        }
-        double* L = a.ws.leaf + 6 * (size_t)(a.bd.body_t0[b] + t);
-        L[0] = lo[0]; L[1] = lo[1]; L[2] = lo[2]; L[3] = hi[0]; L[4] = hi[1]; L[5] = hi[2];
+        double L[6];
+        leaf_box(a.sh.T + 3 * (size_t)a.sh.t_off[s], a.ws.Vw + 3 * (size_t)a.bd.body_v0[b], t, a.pr.envelope, L);
+        for (int axis = 0; axis < 3; ++axis) { lo[axis] = L[axis]; hi[axis] = L[3 + axis]; }
     }
     for (int axis = 0; axis < 3; ++axis) {
         for (int o = 16; o > 0; o >>= 1) {
@@ -369,8 +374,13 @@ __global__ void __launch_bounds__(kBlock) k_mid(const StepArgs a, int max_cluste
         const int A = a.ws.pairs[2 * p], B = a.ws.pairs[2 * p + 1];
         const int cA0 = a.bd.body_c0[A], ncA = a.bd.body_c0[A + 1] - cA0;
         const int cB0 = a.bd.body_c0[B], ncB = a.bd.body_c0[B + 1] - cB0;
-        const int tA0 = a.bd.body_t0[A], ntA = a.bd.body_t0[A + 1] - tA0;
-        const int tB0 = a.bd.body_t0[B], ntB = a.bd.body_t0[B + 1] - tB0;
+        const int ntA = a.bd.body_t0[A + 1] - a.bd.body_t0[A];
+        const int ntB = a.bd.body_t0[B + 1] - a.bd.body_t0[B];
+        const int32_t* TA = a.sh.T + 3 * (size_t)a.sh.t_off[a.bd.shape[A]];
+        const int32_t* TB = a.sh.T + 3 * (size_t)a.sh.t_off[a.bd.shape[B]];
+        const double* VwA = a.ws.Vw + 3 * (size_t)a.bd.body_v0[A];
+        const double* VwB = a.ws.Vw + 3 * (size_t)a.bd.body_v0[B];
+        const double env = a.pr.envelope;
         const double* rootA = a.ws.root + 6 * A;
         const double* rootB = a.ws.root + 6 * B;
         if (ncA > max_clusters || ncB > max_clusters) {
@@ -406,8 +416,8 @@ __global__ void __launch_bounds__(kBlock) k_mid(const StepArgs a, int max_cluste
             for (int k = 0; k < 6; ++k) CA[k] = a.ws.clu[6 * (size_t)(cA0 + ca) + k];
             const int ta = 32 * ca + lane;
             const bool validA = ta < ntA;
-            double LA[6];
-            for (int k = 0; k < 6; ++k) LA[k] = validA ? a.ws.leaf[6 * (size_t)(tA0 + ta) + k] : 0.0;
+            double LA[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            if (validA) leaf_box(TA, VwA, ta, env, LA);
             bool hitA = false;
             for (int ib = 0; ib < nB; ++ib) {
                 const int cb = listB[ib];
@@ -418,8 +428,8 @@ __global__ void __launch_bounds__(kBlock) k_mid(const StepArgs a, int max_cluste
                 if (!amask) continue;
                 const int tb = 32 * cb + lane;
                 const bool validB = tb < ntB;
-                double LB[6];
-                for (int k = 0; k < 6; ++k) LB[k] = validB ? a.ws.leaf[6 * (size_t)(tB0 + tb) + k] : 0.0;
+                double LB[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                if (validB) leaf_box(TB, VwB, tb, env, LB);
                 unsigned bmask = __ballot_sync(0xffffffffu, validB && overlap(LB, CA));
                 unsigned hitB = 0u;
                 const bool mine = (amask >> lane) & 1u;
@@ -471,7 +481,7 @@ __global__ void __launch_bounds__(kBlock) k_mid(const StepArgs a, int max_cluste
 // ---------------------------------------------------------------------------------------------------------
 // narrow phase (collision_detection.py:87 _compute_contacts): one thread per candidate triangle
 // ---------------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_narrow(const StepArgs a) {
+__global__ void __launch_bounds__(256, 2) k_narrow(const StepArgs a) {
     if (a.ws.counters[kAbort]) return;
     const int n_items = a.ws.counters[kNItems];
     const int max_it = a.pr.contact_optimization_max_iterations;
@@ -505,7 +515,7 @@ __global__ void __launch_bounds__(256) k_narrow(const StepArgs a) {
         int best = 0;
         if (gn[1] < gn[best]) best = 1;
         if (gn[2] < gn[best]) best = 2;
-        d3 x = ps[best];
+        d3 x = best == 0 ? ps[0] : (best == 1 ? ps[1] : ps[2]);   // selects keep ps in registers
         int n_fw = 0;
         for (int i = 0; i < max_it; ++i) {   // Frank-Wolfe (:144-165)
             ++n_fw;
@@ -517,7 +527,7 @@ __global__ void __launch_bounds__(256) k_narrow(const StepArgs a) {
             if (o1 < ov) { v = 1; ov = o1; }
             if (o2 < ov) { v = 2; ov = o2; }
             const double alpha = 2.0 / (double)(i + 2);
-            const d3 s = ps[v];
+            const d3 s = v == 0 ? ps[0] : (v == 1 ? ps[1] : ps[2]);
             x = d3{x.x + alpha * (s.x - x.x), x.y + alpha * (s.y - x.y), x.z + alpha * (s.z - x.z)};
             if (ov > tol) break;
         }
