@@ -1855,10 +1855,8 @@ __device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, 
                     asm volatile("prefetch.global.L1 [%0];" ::"l"(f.body + kS32BodyFloats * (size_t)(lh >> 16)));
                 }
         }
-        // every lane of a quad runs the same trip count, so the quad's shuffles see all four lanes
-        for (int i0 = start; i0 < end; i0 += nslot) {
-            const int i = i0 + slot;
-            if (i < end) {
+        // one contact update; every lane of a quad takes the same contacts, so its shuffles see all four lanes
+        auto update = [&](int i) {
                 const float4* C4 = reinterpret_cast<const float4*>(f.c + kS32Floats * i);
                 const uint32_t lh = f.lohi[i];
                 float* Bl = f.body + kS32BodyFloats * (int)(lh & 0xffffu);
@@ -1913,7 +1911,12 @@ __device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, 
                 if (w1.w == 0.0f) {   // not a fixed body
                     B[off] = o0 + dw0; B[off + 1] = o1 + dw1; B[off + 2] = o2 + dw2;
                 }
-            }
+        };
+        // the first pass outside the loop: most levels hold no more contacts than a team has quads
+        int i = start + slot;
+        if (i < end) {
+            update(i);
+            for (i += nslot; i < end; i += nslot) update(i);
         }
         g.sync();
         start = end;
