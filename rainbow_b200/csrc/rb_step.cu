@@ -1777,20 +1777,20 @@ __device__ __forceinline__ float s32_residual(const StepArgs& a, const G& g, con
     for (int bl = g.rank(); bl < nb; bl += g.size()) {
         float* B = f.body + kS32BodyFloats * bl;
         float P[3] = {0.f, 0.f, 0.f}, T[3] = {0.f, 0.f, 0.f};
-        if (B[7] == 0.0f) {
+        if (B[7] == 0.0f) {   // rows read as float4 groups (lin, b | ang_lo, 1/diag | ang_hi, x)
             for (int e = f.bptr[bl]; e < f.bptr[bl + 1]; ++e) {
                 const uint32_t code = f.blist[e];
                 const int side = code & 1;
-                const float* c = f.c + kS32Floats * (code >> 1);
+                const float4* C4 = reinterpret_cast<const float4*>(f.c + kS32Floats * (code >> 1));
                 for (int q = 0; q < 4; ++q) {
-                    const float* row = c + 12 * q;
-                    const float xq = row[11];
+                    const float4 lin = C4[3 * q], alo = C4[3 * q + 1], ahi = C4[3 * q + 2];
+                    const float xq = ahi.w;
                     if (q < 3) {
                         const float sx = side ? -xq : xq;
-                        P[0] = fmaf(row[0], sx, P[0]); P[1] = fmaf(row[1], sx, P[1]); P[2] = fmaf(row[2], sx, P[2]);
+                        P[0] = fmaf(lin.x, sx, P[0]); P[1] = fmaf(lin.y, sx, P[1]); P[2] = fmaf(lin.z, sx, P[2]);
                     }
-                    const float* ang = row + (side ? 8 : 4);
-                    T[0] = fmaf(ang[0], xq, T[0]); T[1] = fmaf(ang[1], xq, T[1]); T[2] = fmaf(ang[2], xq, T[2]);
+                    const float4 ang = side ? ahi : alo;
+                    T[0] = fmaf(ang.x, xq, T[0]); T[1] = fmaf(ang.y, xq, T[1]); T[2] = fmaf(ang.z, xq, T[2]);
                 }
             }
         }
@@ -1802,19 +1802,27 @@ __device__ __forceinline__ float s32_residual(const StepArgs& a, const G& g, con
     g.sync();
     float m = 0.0f, xm = 0.0f;
     for (int i = g.rank(); i < K; i += g.size()) {
-        const float* c = f.c + kS32Floats * i;
+        const float4* C4 = reinterpret_cast<const float4*>(f.c + kS32Floats * i);
         const uint32_t lh = f.lohi[i];
-        const float* wl = f.body + kS32BodyFloats * (int)(lh & 0xffffu);
-        const float* wh = f.body + kS32BodyFloats * (int)(lh >> 16);
+        const float* Bl = f.body + kS32BodyFloats * (int)(lh & 0xffffu);
+        const float* Bh = f.body + kS32BodyFloats * (int)(lh >> 16);
+        const float4 l0 = *reinterpret_cast<const float4*>(Bl), l1 = *reinterpret_cast<const float4*>(Bl + 4);
+        const float4 h0 = *reinterpret_cast<const float4*>(Bh), h1 = *reinterpret_cast<const float4*>(Bh + 4);
         float z[4], x[4];
-        for (int q = 0; q < 4; ++q) {
-            const float* row = c + 12 * q;
-            x[q] = row[11];
-            z[q] = x[q] - row[7] * (s32_jw(row, q, wl, wh) + row[3]);
+        float mu = 0.0f;
+        for (int q = 0; q < 4; ++q) {   // the expressions of s32_jw, on float4 loads
+            const float4 r0 = C4[3 * q], r1 = C4[3 * q + 1], r2 = C4[3 * q + 2];
+            float lin = 0.0f;
+            if (q < 3) lin = fmaf(r0.x, l0.x - h0.x, fmaf(r0.y, l0.y - h0.y, r0.z * (l0.z - h0.z)));
+            else mu = r0.x;
+            const float alo = fmaf(r1.x, l0.w, fmaf(r1.y, l1.x, r1.z * l1.y));
+            const float ahi = fmaf(r2.x, h0.w, fmaf(r2.y, h1.x, r2.z * h1.y));
+            x[q] = r2.w;
+            z[q] = x[q] - r1.w * (((lin + alo) + ahi) + r0.w);
         }
         const float pn = fmaxf(z[0], 0.0f);
         float fr[3];
-        f32_prox(z[1], z[2], z[3], c[36], pn, fr);
+        f32_prox(z[1], z[2], z[3], mu, pn, fr);
         const float d[4] = {x[0] - pn, x[1] - fr[0], x[2] - fr[1], x[3] - fr[2]};
         for (int t = 0; t < 4; ++t) {
             m = fmaxf(m, fabsf(d[t]));
