@@ -578,21 +578,31 @@ __global__ void k_dedup(const StepArgs a) {
         for (int c0 = i0; c0 < i1; c0 += 32) {
             const int i = c0 + lane;
             bool keep = false;
-            if (i < i1) {
-                if (!WRITE) {
-                    if (a.ws.item_flag[i]) {
-                        const double* pi = a.ws.item_p + 3 * (size_t)i;
-                        const double px = pi[0], py = pi[1], pz = pi[2];
-                        keep = true;
-                        for (int j = i0; j < i; ++j) {
-                            if (!a.ws.item_flag[j]) continue;
-                            const double* pj = a.ws.item_p + 3 * (size_t)j;
-                            if (px == pj[0] && py == pj[1] && pz == pj[2]) { keep = false; break; }
-                        }
+            if (!WRITE) {
+                // candidate i is kept if no earlier accepted candidate of the pair has its position: the
+                // earlier accepted ones, 32 at a time, are found by ballot and their positions broadcast
+                const bool mine = i < i1 && a.ws.item_flag[i] != 0;
+                double px = 0.0, py = 0.0, pz = 0.0;
+                if (mine) { const double* pi = a.ws.item_p + 3 * (size_t)i; px = pi[0]; py = pi[1]; pz = pi[2]; }
+                keep = mine;
+                for (int e0 = i0; e0 <= c0; e0 += 32) {
+                    const int j = e0 + lane;
+                    const bool fj = j < i1 && (e0 == c0 ? mine : a.ws.item_flag[j] != 0);
+                    double qx = 0.0, qy = 0.0, qz = 0.0;
+                    if (fj) { const double* pj = a.ws.item_p + 3 * (size_t)j; qx = pj[0]; qy = pj[1]; qz = pj[2]; }
+                    unsigned m = __ballot_sync(0xffffffffu, fj);
+                    while (m) {   // in the own chunk only lanes below this one count as earlier
+                        const int b = __ffs(m) - 1;
+                        m &= m - 1;
+                        const double bx = __shfl_sync(0xffffffffu, qx, b);
+                        const double by = __shfl_sync(0xffffffffu, qy, b);
+                        const double bz = __shfl_sync(0xffffffffu, qz, b);
+                        const bool earlier = e0 < c0 || b < lane;
+                        if (keep && earlier && px == bx && py == by && pz == bz) keep = false;
                     }
-                } else {
-                    keep = a.ws.item_flag[i] == 2;
                 }
+            } else {
+                keep = i < i1 && a.ws.item_flag[i] == 2;
             }
             const unsigned bal = __ballot_sync(0xffffffffu, keep);
             if (!WRITE && i < i1 && keep) a.ws.item_flag[i] = 2;   // the write pass reads flag 2 = kept
