@@ -432,16 +432,33 @@ __global__ void __launch_bounds__(kBlock) k_mid(const StepArgs a, int max_cluste
                 if (validB) leaf_box(TB, VwB, tb, env, LB);
                 unsigned bmask = __ballot_sync(0xffffffffu, validB && overlap(LB, CA));
                 unsigned hitB = 0u;
-                const bool mine = (amask >> lane) & 1u;
-                while (bmask) {
-                    const int jb = __ffs(bmask) - 1;
-                    bmask &= bmask - 1;
-                    double Lj[6];
-                    for (int k = 0; k < 6; ++k) Lj[k] = __shfl_sync(0xffffffffu, LB[k], jb);
-                    if (mine && overlap(LA, Lj)) { hitA = true; hitB |= 1u << jb; }
+                // every candidate leaf pair is tested once, broadcasting the leaves of the side with fewer
+                if (__popc(bmask) <= __popc(amask)) {   // B leaves to the A lanes
+                    const bool mine = (amask >> lane) & 1u;
+                    while (bmask) {
+                        const int jb = __ffs(bmask) - 1;
+                        bmask &= bmask - 1;
+                        double Lj[6];
+                        for (int k = 0; k < 6; ++k) Lj[k] = __shfl_sync(0xffffffffu, LB[k], jb);
+                        if (mine && overlap(LA, Lj)) { hitA = true; hitB |= 1u << jb; }
+                    }
+                    n_ovl += __popc(hitB);
+                    hitB = __reduce_or_sync(0xffffffffu, hitB);
+                } else {                                 // A leaves to the B lanes
+                    const bool mineB = (bmask >> lane) & 1u;
+                    unsigned am = amask, hitAbits = 0u;
+                    bool bhit = false;
+                    while (am) {
+                        const int ja = __ffs(am) - 1;
+                        am &= am - 1;
+                        double Li[6];
+                        for (int k = 0; k < 6; ++k) Li[k] = __shfl_sync(0xffffffffu, LA[k], ja);
+                        if (mineB && overlap(Li, LB)) { bhit = true; hitAbits |= 1u << ja; ++n_ovl; }
+                    }
+                    hitB = __ballot_sync(0xffffffffu, bhit);
+                    hitAbits = __reduce_or_sync(0xffffffffu, hitAbits);
+                    if ((hitAbits >> lane) & 1u) hitA = true;
                 }
-                n_ovl += __popc(hitB);
-                hitB = __reduce_or_sync(0xffffffffu, hitB);
                 if (lane == 0) maskB[ib] |= hitB;
             }
             const unsigned bal = __ballot_sync(0xffffffffu, hitA);
