@@ -1012,6 +1012,36 @@ __device__ int scene_levels(const StepArgs& a, const G& g, const SceneRange& R, 
     return bucket_classes(a, g, R, s);
 }
 
+// The same levels with the relaxation in shared memory: scratch holds 3 K int16 (the two predecessors of each
+// contact, scene-local, and its level); the levels then go to lev_of.  Same fixed point, so the same levels.
+template <class G>
+__device__ int scene_levels_smem(const StepArgs& a, const G& g, const SceneRange& R, int s, int16_t* scratch) {
+    const int K = R.c1 - R.c0;
+    int16_t* pred = scratch;
+    volatile int16_t* lev = scratch + 2 * K;
+    for (int k = g.rank(); k < K; k += g.size()) {
+        const int p0 = a.ws.cpred[2 * (R.c0 + k)], p1 = a.ws.cpred[2 * (R.c0 + k) + 1];
+        pred[2 * k] = (int16_t)(p0 >= 0 ? p0 - R.c0 : -1);
+        pred[2 * k + 1] = (int16_t)(p1 >= 0 ? p1 - R.c0 : -1);
+        lev[k] = 1;
+    }
+    g.sync();
+    for (;;) {
+        bool changed = false;
+        for (int k = g.rank(); k < K; k += g.size()) {
+            const int p0 = pred[2 * k], p1 = pred[2 * k + 1];
+            const int l0 = p0 >= 0 ? lev[p0] : 0;
+            const int l1 = p1 >= 0 ? lev[p1] : 0;
+            const int l = 1 + max(l0, l1);
+            if (l != lev[k]) { lev[k] = (int16_t)l; changed = true; }
+        }
+        if (!g.any(changed)) break;
+    }
+    for (int k = g.rank(); k < K; k += g.size()) a.ws.lev_of[R.c0 + k] = lev[k];
+    g.sync();
+    return bucket_classes(a, g, R, s);
+}
+
 // Groups the scene's contacts by their class lev_of[k] (1-based level or colour): lev_ptr[c-1] .. lev_ptr[c]
 // index lev_order, which lists the contacts of class c.  Returns the number of classes.
 template <class G>
@@ -1746,9 +1776,11 @@ __device__ __forceinline__ float s32_jw(const float* row, int q, const float* wl
 // copy scene R into the team's slab as FP32, contacts in level order; returns the number of levels
 template <class G>
 __device__ __forceinline__ int s32_load(const StepArgs& a, const G& g, const SceneRange& R, int s, const S32Scene& f,
-                                        bool coloured) {
+                                        bool coloured, int16_t* scratch) {
     const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
-    const int L = coloured ? scene_colours(a, g, R, s) : scene_levels(a, g, R, s);
+    // levels by relaxation in shared memory when a scratch of 3 K int16 is given (the rows' room, not yet filled)
+    const int L = coloured ? scene_colours(a, g, R, s)
+                : scratch ? scene_levels_smem(a, g, R, s, scratch) : scene_levels(a, g, R, s);
     const int* order = a.ws.lev_order + R.c0;
     for (int t = g.rank(); t < 16 * K; t += g.size()) {   // (position, row, float4 group; part 3 idle)
         const int i = t >> 4, q = (t >> 2) & 3, part = t & 3;
@@ -2147,7 +2179,15 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
         }
         const double t0 = a.pr.profiling ? device_us() : 0.0;
         const S32Scene f = s32_carve(my_slab, K, nb, kL2 ? &a : nullptr, R.c0, bodies_global, R.b0);
-        const int L = s32_load(a, g, R, s, f, coloured);
+        // scratch for the level relaxation: the rows' room of the slab, or with rows in L2 what the slab has left
+        int16_t* scratch = nullptr;
+        if (!kL2) {
+            scratch = reinterpret_cast<int16_t*>(f.c);
+        } else {
+            const size_t off = (s32_bytes(K, nb, true, bodies_global) + 15) & ~size_t(15);
+            if (off + 6 * (size_t)K <= slab) scratch = reinterpret_cast<int16_t*>(my_slab + off);
+        }
+        const int L = s32_load(a, g, R, s, f, coloured, scratch);
         if (g.rank() == 0) a.ws.nlev[s] = L;
         float res = s32_residual(a, g, R, f);   // the warm-started iterate may already be good enough
         float best = res;
