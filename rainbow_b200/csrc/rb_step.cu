@@ -1012,13 +1012,17 @@ __device__ int scene_levels(const StepArgs& a, const G& g, const SceneRange& R, 
     return bucket_classes(a, g, R, s);
 }
 
-// The same levels with the relaxation in shared memory: scratch holds 3 K int16 (the two predecessors of each
-// contact, scene-local, and its level); the levels then go to lev_of.  Same fixed point, so the same levels.
+// The same levels with the relaxation and the bucketing in shared memory: scratch (s32_level_scratch bytes)
+// holds the two predecessors of each contact (scene-local int16), its level (int16) and one counter per level;
+// the levels then go to lev_of and the buckets to lev_ptr / lev_order.  Same fixed point, same order within a
+// level up to the order of atomics, which no result depends on.
+__host__ __device__ inline size_t s32_level_scratch(int K) { return 6 * (size_t)K + 4 * (size_t)(K + 2) + 16; }
 template <class G>
 __device__ int scene_levels_smem(const StepArgs& a, const G& g, const SceneRange& R, int s, int16_t* scratch) {
     const int K = R.c1 - R.c0;
     int16_t* pred = scratch;
     volatile int16_t* lev = scratch + 2 * K;
+    int* cnt = reinterpret_cast<int*>(reinterpret_cast<char*>(scratch) + ((6 * (size_t)K + 15) & ~size_t(15)));
     for (int k = g.rank(); k < K; k += g.size()) {
         const int p0 = a.ws.cpred[2 * (R.c0 + k)], p1 = a.ws.cpred[2 * (R.c0 + k) + 1];
         pred[2 * k] = (int16_t)(p0 >= 0 ? p0 - R.c0 : -1);
@@ -1037,9 +1041,28 @@ __device__ int scene_levels_smem(const StepArgs& a, const G& g, const SceneRange
         }
         if (!g.any(changed)) break;
     }
-    for (int k = g.rank(); k < K; k += g.size()) a.ws.lev_of[R.c0 + k] = lev[k];
+    int L = 0;
+    for (int k = g.rank(); k < K; k += g.size()) {
+        const int l = lev[k];
+        a.ws.lev_of[R.c0 + k] = l;
+        L = max(L, l);
+    }
+    L = g.imax(L);
+    for (int l = g.rank(); l <= L; l += g.size()) cnt[l] = 0;
     g.sync();
-    return bucket_classes(a, g, R, s);
+    for (int k = g.rank(); k < K; k += g.size()) atomicAdd(cnt + lev[k] - 1, 1);
+    g.sync();
+    int* ptr = a.ws.lev_ptr + R.c0 + s;   // ptr[l-1] .. ptr[l]: contacts of level l (1-based), ptr[L] = K
+    if (g.rank() == 0) {
+        int acc = 0;
+        for (int l = 0; l < L; ++l) { const int c = cnt[l]; ptr[l] = acc; cnt[l] = acc; acc += c; }
+        ptr[L] = acc;
+    }
+    g.sync();
+    // the order within a level does not change any result (its contacts share no body that is written)
+    for (int k = g.rank(); k < K; k += g.size()) a.ws.lev_order[R.c0 + atomicAdd(cnt + lev[k] - 1, 1)] = R.c0 + k;
+    g.sync();
+    return L;
 }
 
 // Groups the scene's contacts by their class lev_of[k] (1-based level or colour): lev_ptr[c-1] .. lev_ptr[c]
@@ -1778,7 +1801,7 @@ template <class G>
 __device__ __forceinline__ int s32_load(const StepArgs& a, const G& g, const SceneRange& R, int s, const S32Scene& f,
                                         bool coloured, int16_t* scratch) {
     const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
-    // levels by relaxation in shared memory when a scratch of 3 K int16 is given (the rows' room, not yet filled)
+    // levels by relaxation in shared memory when a scratch is given (the rows' room, not yet filled)
     const int L = coloured ? scene_colours(a, g, R, s)
                 : scratch ? scene_levels_smem(a, g, R, s, scratch) : scene_levels(a, g, R, s);
     const int* order = a.ws.lev_order + R.c0;
@@ -2181,11 +2204,11 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
         const S32Scene f = s32_carve(my_slab, K, nb, kL2 ? &a : nullptr, R.c0, bodies_global, R.b0);
         // scratch for the level relaxation: the rows' room of the slab, or with rows in L2 what the slab has left
         int16_t* scratch = nullptr;
-        if (!kL2) {
+        if (!kL2) {   // 192 bytes per contact there, more than s32_level_scratch needs
             scratch = reinterpret_cast<int16_t*>(f.c);
         } else {
             const size_t off = (s32_bytes(K, nb, true, bodies_global) + 15) & ~size_t(15);
-            if (off + 6 * (size_t)K <= slab) scratch = reinterpret_cast<int16_t*>(my_slab + off);
+            if (off + s32_level_scratch(K) <= slab) scratch = reinterpret_cast<int16_t*>(my_slab + off);
         }
         const int L = s32_load(a, g, R, s, f, coloured, scratch);
         if (g.rank() == 0) a.ws.nlev[s] = L;
