@@ -404,13 +404,18 @@ class DeviceWorld:
             self.h_u = torch.empty(6 * self.n_bodies, dtype=torch.float64, pin_memory=True)
         return self.h_x, self.h_u
 
-    def state(self):
-        """Host copies of (x, u) through pinned staging buffers: (N, 7) and (N, 6) arrays."""
+    def state(self, copy=True):
+        """(x, u) read back through pinned staging buffers: (N, 7) and (N, 6) arrays.
+
+        With ``copy=False`` the arrays are views of the pinned buffers themselves (no host copy): they hold this
+        state until the next ``state`` or ``set_state`` call, and passing them back to ``set_state`` uploads
+        them without a host copy either."""
         hx, hu = self._pinned()
         hx.copy_(self.t_x, non_blocking=True)
         hu.copy_(self.t_u, non_blocking=True)
         torch.cuda.current_stream(self.device).synchronize()
-        return hx.numpy().reshape(-1, 7).copy(), hu.numpy().reshape(-1, 6).copy()
+        x, u = hx.numpy().reshape(-1, 7), hu.numpy().reshape(-1, 6)
+        return (x.copy(), u.copy()) if copy else (x, u)
 
 
     def reset_warm_start(self):
@@ -418,11 +423,15 @@ class DeviceWorld:
         self.t_cache_count.zero_()
 
     def set_state(self, x, u):
-        """Upload (x, u) through pinned staging buffers (asynchronous on the current stream)."""
+        """Upload (x, u) through pinned staging buffers (asynchronous on the current stream).  Arrays that are
+        the staging buffers themselves (``state(copy=False)``) are uploaded without a host copy."""
         hx, hu = self._pinned()
         torch.cuda.current_stream(self.device).synchronize()   # staging buffers may still feed a copy
-        hx.numpy()[:] = np.asarray(x, np.float64).reshape(-1)
-        hu.numpy()[:] = np.asarray(u, np.float64).reshape(-1)
+        for src, dst in ((x, hx), (u, hu)):
+            d = dst.numpy()
+            if not (isinstance(src, np.ndarray) and src.dtype == np.float64 and src.size == d.size
+                    and src.__array_interface__["data"][0] == d.__array_interface__["data"][0]):
+                d[:] = np.asarray(src, np.float64).reshape(-1)
         self.t_x.copy_(hx, non_blocking=True)
         self.t_u.copy_(hu, non_blocking=True)
 

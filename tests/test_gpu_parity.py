@@ -269,6 +269,30 @@ def test_graph_replay_equals_direct_steps():
         np.testing.assert_array_equal(cb[key], ca[key], err_msg=key)
 
 
+def test_pinned_state_views_round_trip():
+    """state(copy=False) hands out the pinned staging buffers; passing them back to set_state uploads them
+    without a host copy, and the steps that follow are the same bits as with copied arrays."""
+    from rainbow_b200 import world as W
+    ds = [load_fixture(n) for n in ("boxes8", "spheres")]
+    p = W.params_from_vector(ds[0]["params"])
+    p["max_iterations"] = 100
+    rp = W.make_rb_params(p)
+    copied = W.DeviceWorld(ds, max_iterations=100)
+    viewed = W.DeviceWorld(ds, max_iterations=100)
+    x, u = copied.state()
+    hx, hu = viewed.state(copy=False)
+    np.testing.assert_array_equal(hx, x)
+    for _ in range(3):
+        copied.set_state(x, u)
+        copied.step(rp)
+        x, u = copied.state()
+        viewed.set_state(hx, hu)
+        viewed.step(rp)
+        hx, hu = viewed.state(copy=False)
+        np.testing.assert_array_equal(hx, x)
+        np.testing.assert_array_equal(hu, u)
+
+
 def test_fp32_refine_spends_the_same_sweep_budget():
     """Unconverged FP32+FP64 solves use exactly max_iterations sweeps, like the FP64 solve they stand in for,
     with the reserved FP64 sweeps at the end."""
