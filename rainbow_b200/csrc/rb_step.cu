@@ -1724,7 +1724,8 @@ constexpr int kQueueFp32 = 5;                        // counters[5..8]: scene qu
 constexpr int kClassEnd32 = 9;                       // counters[9..12]: end of each class's range in list32
 constexpr int kS32BodyFloats = 16;                   // floats per body
 constexpr int kFp32Block = 128;                      // threads per block of the FP32 launches
-constexpr int kFp32BlockMax = 256;                   // ... and of the launch for scenes beyond any slab
+constexpr int kFp32BlockMax = 256;                   // ... at most, in the launches for slab scenes
+constexpr int kFp32L2Block = 512;                    // threads of the launch for the scenes beyond any slab
 constexpr int kFp32LargeSmem = 224 * 1024;           // slab of a block team (one scene per SM)
 constexpr int kS32SmallSlab = 28 * 1024;             // slab of a warp team, small class (8 scenes per SM)
 constexpr int kS32MidSlab = 56 * 1024;               // slab of a warp team, mid class (4 scenes per SM)
@@ -2160,7 +2161,7 @@ __device__ __noinline__ void solve_scene_call(const StepArgs& a, const G& g, int
 // scenes too large for any slab, with their contact rows in global memory (L2-resident) and the rest of
 // the copy in the slab.
 template <class G, bool kL2>
-__global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs a, int queue, size_t lo_bytes, size_t slab) {
+__global__ void __launch_bounds__(kL2 ? kFp32L2Block : kFp32BlockMax, 1) k_solve_fp32(const StepArgs a, int queue, size_t lo_bytes, size_t slab) {
     extern __shared__ __align__(16) char f32_smem[];
     __shared__ double red[33];
     __shared__ int ired[33];
@@ -2272,7 +2273,7 @@ __global__ void __launch_bounds__(kFp32BlockMax, 1) k_solve_fp32(const StepArgs 
             }
         }
         g.sync();
-        if (!finished) {   // FP64 sweeps with the budget left, by this team at once (w in global memory)
+        if (!kL2 && !finished) {   // FP64 sweeps with the budget left, by this team at once (w in global memory)
             solve_scene_call(a, g, s);
             if (g.rank() == 0) a.ws.fin32[s] = 1;
             g.sync();
@@ -2745,14 +2746,14 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     k_fp32_classes<<<1, 1024, 0, st>>>(a, small_slab, mid_slab); note_launch();
     if (pr->precision != RB_PRECISION_FP64) {
         // FP32 phase, four size classes side by side: warp teams with 28 KB slabs (8 scenes per SM), warp
-        // teams with 56 KB slabs (4 per SM), block teams with 224 KB (1 per SM), and 256-thread block teams
+        // teams with 56 KB slabs (4 per SM), block teams with 224 KB (1 per SM), and 512-thread block teams
         // for the scenes beyond that, whose contact rows stay in L2
         SideStreams* ss = nullptr;
         rc = side_streams(st, &ss);
         if (rc != RB_OK) return rc;
         cudaEventRecord(ss->fork, st);
         for (int c = 0; c < kSideStreams; ++c) cudaStreamWaitEvent(ss->s[c], ss->fork, 0);
-        k_solve_fp32<BlockGroup, true><<<148, kFp32BlockMax, (size_t)kFp32LargeSmem, ss->s[3]>>>(
+        k_solve_fp32<BlockGroup, true><<<148, kFp32L2Block, (size_t)kFp32LargeSmem, ss->s[3]>>>(
             a, kQueueFp32 + 3, kFp32LargeSmem, kFp32LargeSmem); note_launch();
         k_solve_fp32<BlockGroup, false><<<148, kFp32Block, (size_t)kFp32LargeSmem, ss->s[2]>>>(
             a, kQueueFp32 + 2, mid_slab, kFp32LargeSmem); note_launch();
