@@ -97,7 +97,9 @@ def build_workload(name, device, n_scenes=1024):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed region: NVML read every 10 ms (one
+    sample at the start and one at the end, so short regions still get several), nvidia-smi if NVML is
+    unavailable.  Reads only; no setting of the GPU is touched."""
     FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
              "clocks_event_reasons.sw_power_cap"
@@ -107,25 +109,56 @@ class ClockSampler:
         self.samples = []
         self._stop = threading.Event()
         self._t = threading.Thread(target=self._run, daemon=True)
+        self._nvml = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(gpu_index).uuid)
+            h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            self._nvml = (pynvml, h)
+        except Exception:
+            self._nvml = None
+
+    def _sample(self):
+        if self._nvml is not None:
+            n, h = self._nvml
+            try:
+                sm = n.nvmlDeviceGetClockInfo(h, n.NVML_CLOCK_SM)
+                mx = n.nvmlDeviceGetMaxClockInfo(h, n.NVML_CLOCK_SM)
+                pw = n.nvmlDeviceGetPowerUsage(h) / 1000.0
+                r = n.nvmlDeviceGetCurrentClocksEventReasons(h)
+                act = lambda bit: "Active" if r & bit else "Not Active"  # noqa: E731
+                self.samples.append([str(self.gpu), str(sm), str(mx), "%.1f" % pw, hex(r),
+                                     act(n.nvmlClocksEventReasonHwSlowdown),
+                                     act(n.nvmlClocksEventReasonHwThermalSlowdown),
+                                     act(n.nvmlClocksEventReasonSwThermalSlowdown),
+                                     act(n.nvmlClocksEventReasonSwPowerCap)])
+                return
+            except Exception:
+                self._nvml = None
+        try:
+            out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                  "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+            for line in out.stdout.strip().splitlines():
+                self.samples.append([v.strip() for v in line.split(",")])
+        except Exception:
+            pass
 
     def _run(self):
         while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                for line in out.stdout.strip().splitlines():
-                    self.samples.append([v.strip() for v in line.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+            self._sample()
+            self._stop.wait(0.01 if self._nvml is not None else 0.2)
 
     def __enter__(self):
+        self._sample()
         self._t.start()
         return self
 
     def __exit__(self, *a):
         self._stop.set()
         self._t.join(timeout=10)
+        self._sample()
 
     def summary(self):
         if not self.samples:
