@@ -659,106 +659,94 @@ __device__ __forceinline__ double jrow_dot(const double* Jr, const double* wlo, 
 }
 
 __global__ void k_contacts(const StepArgs a) {
+    // one thread per (contact, row): row q's J and W J^T blocks, b, Delassus diagonal, r and start impulse;
+    // the row-0 thread also writes the contact's body pair and mu
     if (a.ws.counters[kAbort]) return;
     const int K = a.ws.counters[kNContacts];
     const double dt = a.pr.dt;
     double r_scale = a.pr.scheme == RB_SCHEME_RIGID_GS ? 1.0 : 0.1;   // solver_interface.py:48
     if (a.pr.termination == RB_TERMINATE_RESIDUAL_FIXED_R && a.pr.relaxation > 0.0) r_scale *= a.pr.relaxation;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 4 * K; t += gridDim.x * blockDim.x) {
+        const int k = t >> 2, row = t & 3;
         const int A = a.out.contact_ids[2 * k], B = a.out.contact_ids[2 * k + 1];
         const d3 p = ld3(a.out.contact_p + 3 * k);
         const d3 rA = sub(p, ld3(a.bd.x + 7 * A)), rB = sub(p, ld3(a.bd.x + 7 * B));
         d3 vs, vt, vn;
         make_orthonormal_vectors(ld3(a.out.contact_n + 3 * k), vs, vt, vn);   // (t, b, n)
-        const d3 dirs[3] = {vn, vs, vt};
         const int lo = min(A, B), hi = max(A, B);
         const int offA = (A == lo) ? 0 : 6, offB = (B == lo) ? 0 : 6;
-        double* J = a.ws.J + 48 * (size_t)k;
-        double* W = a.ws.WJT + 48 * (size_t)k;
-        for (int row = 0; row < 3; ++row) {   // contacts.py:140-147
-            const d3 d = dirs[row];
+        double* J = a.ws.J + 48 * (size_t)k + 12 * row;
+        double* W = a.ws.WJT + 48 * (size_t)k + 12 * row;
+        double* JA = J + offA;
+        double* JB = J + offB;
+        if (row < 3) {   // contacts.py:140-147
+            const d3 d = row == 0 ? vn : (row == 1 ? vs : vt);
             const d3 ca = cross_np(rA, d), cb = cross_np(rB, d);
-            double* JA = J + 12 * row + offA;
-            double* JB = J + 12 * row + offB;
             JA[0] = -d.x; JA[1] = -d.y; JA[2] = -d.z; JA[3] = -ca.x; JA[4] = -ca.y; JA[5] = -ca.z;
             JB[0] = d.x; JB[1] = d.y; JB[2] = d.z; JB[3] = cb.x; JB[4] = cb.y; JB[5] = cb.z;
-        }
-        {
-            double* JA = J + 36 + offA;
-            double* JB = J + 36 + offB;
+        } else {
             JA[0] = -0.0; JA[1] = -0.0; JA[2] = -0.0; JA[3] = -vn.x; JA[4] = -vn.y; JA[5] = -vn.z;
             JB[0] = 0.0; JB[1] = 0.0; JB[2] = 0.0; JB[3] = vn.x; JB[4] = vn.y; JB[5] = vn.z;
         }
-        a.ws.lohi[2 * k] = lo;
-        a.ws.lohi[2 * k + 1] = hi;
         bool hasw[2];
         for (int side = 0; side < 2; ++side) {   // WJT = W J^T (bsr_matmat order)
             const int bb = side ? hi : lo;
             hasw[side] = !a.bd.fixed[bb];
             const double m = hasw[side] ? 1.0 / a.bd.mass[bb] : 0.0;
             const double* Wi = a.ws.Winv + 9 * bb;
-            for (int row = 0; row < 4; ++row) {
-                const double* Jr = J + 12 * row + 6 * side;
-                double* Wr = W + 12 * row + 6 * side;
-                for (int i = 0; i < 3; ++i) {
-                    double s = 0.0;
-                    s += (i == 0 ? m : 0.0) * Jr[0];
-                    s += (i == 1 ? m : 0.0) * Jr[1];
-                    s += (i == 2 ? m : 0.0) * Jr[2];
-                    double t = 0.0;
-                    t += Wi[3 * i + 0] * Jr[3];
-                    t += Wi[3 * i + 1] * Jr[4];
-                    t += Wi[3 * i + 2] * Jr[5];
-                    Wr[i] = hasw[side] ? s : 0.0;
-                    Wr[3 + i] = hasw[side] ? t : 0.0;
-                }
+            const double* Jr = J + 6 * side;
+            double* Wr = W + 6 * side;
+            for (int i = 0; i < 3; ++i) {
+                double s = 0.0;
+                s += (i == 0 ? m : 0.0) * Jr[0];
+                s += (i == 1 ? m : 0.0) * Jr[1];
+                s += (i == 2 ? m : 0.0) * Jr[2];
+                double tt = 0.0;
+                tt += Wi[3 * i + 0] * Jr[3];
+                tt += Wi[3 * i + 1] * Jr[4];
+                tt += Wi[3 * i + 2] * Jr[5];
+                Wr[i] = hasw[side] ? s : 0.0;
+                Wr[3 + i] = hasw[side] ? tt : 0.0;
             }
         }
         // b = (1 + e) v + J (dt W f_ext) + g   (contacts.py:46)
         const int sc = scene_of(a.bd.scene_start, a.bd.n_scenes, A);
         const int M = a.bd.scene_material_count[sc];
         const int entry = a.bd.scene_material_offset[sc] + a.bd.material[A] * M + a.bd.material[B];
-        const double mu = a.bd.material_mu[3 * entry];
         const double eps = a.pr.use_bounce ? a.bd.material_eps[entry] : 0.0;
         const double* ulo = a.bd.u + 6 * lo;
         const double* uhi = a.bd.u + 6 * hi;
         const double* dlo = a.ws.du + 6 * lo;
         const double* dhi = a.ws.du + 6 * hi;
-        const double gap = a.out.contact_g[k];
-        double vrow[4];
-        for (int row = 0; row < 4; ++row) vrow[row] = jrow_dot(J + 12 * row, ulo, uhi);
+        const double vrow = jrow_dot(J, ulo, uhi);
         double gk0 = 0.0;
-        if (a.pr.use_pre_stabilization) {   // contacts.py:188 _compute_error_vector
+        if (row == 0 && a.pr.use_pre_stabilization) {   // contacts.py:188 _compute_error_vector
+            const double gap = a.out.contact_g[k];
             const double rate = a.pr.gap_reduction / dt;
             const double upper = -a.pr.max_gap_value / dt;
             const double lower = -a.pr.min_gap_value;
-            if (gap < lower && vrow[0] <= 0.0) {
-                const double t = rate * gap;
-                gk0 = upper > t ? upper : t;
+            if (gap < lower && vrow <= 0.0) {
+                const double tg = rate * gap;
+                gk0 = upper > tg ? upper : tg;
             }
         }
-        for (int row = 0; row < 4; ++row) {
-            const double jd = jrow_dot(J + 12 * row, dlo, dhi);
-            const double e = row == 0 ? eps : 0.0;
-            const double g = row == 0 ? gk0 : 0.0;
-            a.ws.b[4 * k + row] = ((1.0 + e) * vrow[row] + jd) + g;
-            // Delassus diagonal: reduceat over the nonzero products J .* WJT^T in column order (contacts.py:49)
-            double prods[12];
-            int m = 0;
-            for (int c = 0; c < 12; ++c) {
-                if (!hasw[c / 6]) continue;
-                const double pr = J[12 * row + c] * W[12 * row + c];
-                if (pr != 0.0) prods[m++] = pr;
-            }
-            double dg = np_reduce_sum(prods, m);
-            if (dg == 0.0) dg = 1.0;
-            a.ws.diag[4 * k + row] = dg;
-            a.ws.r[4 * k + row] = r_scale / dg;
-            a.ws.x[4 * k + row] = 0.0;
-            a.out.contact_sol[4 * k + row] = 0.0;
+        const double jd = jrow_dot(J, dlo, dhi);
+        const double e = row == 0 ? eps : 0.0;
+        a.ws.b[4 * k + row] = ((1.0 + e) * vrow + jd) + gk0;
+        // Delassus diagonal: reduceat over the nonzero products J .* WJT^T in column order (contacts.py:49)
+        double prods[12];
+        int m = 0;
+        for (int c = 0; c < 12; ++c) {
+            if (!hasw[c / 6]) continue;
+            const double pr = J[c] * W[c];
+            if (pr != 0.0) prods[m++] = pr;
         }
-        a.ws.mu[k] = mu;
-        if (a.pr.warm_start && a.out.cache_count) {   // previous impulses of the same contact (binary search)
+        double dg = np_reduce_sum(prods, m);
+        if (dg == 0.0) dg = 1.0;
+        a.ws.diag[4 * k + row] = dg;
+        a.ws.r[4 * k + row] = r_scale / dg;
+        double x0 = 0.0;
+        if (a.pr.warm_start && a.out.cache_count) {   // previous impulse of the same contact (binary search)
             const int64_t k1 = a.ws.ckey[2 * k], k2 = a.ws.ckey[2 * k + 1];
             int lo_i = 0, hi_i = min(*a.out.cache_count, a.caps.contact_capacity);
             while (lo_i < hi_i) {
@@ -767,11 +755,14 @@ __global__ void k_contacts(const StepArgs a) {
                 if (m1 < k1 || (m1 == k1 && m2 < k2)) lo_i = mid + 1; else hi_i = mid;
             }
             if (lo_i < *a.out.cache_count && a.out.cache_key[2 * lo_i] == k1 && a.out.cache_key[2 * lo_i + 1] == k2)
-                for (int row = 0; row < 4; ++row) {
-                    const double v = a.out.cache_sol[4 * lo_i + row];
-                    a.ws.x[4 * k + row] = v;
-                    a.out.contact_sol[4 * k + row] = v;
-                }
+                x0 = a.out.cache_sol[4 * lo_i + row];
+        }
+        a.ws.x[4 * k + row] = x0;
+        a.out.contact_sol[4 * k + row] = x0;
+        if (row == 0) {
+            a.ws.lohi[2 * k] = lo;
+            a.ws.lohi[2 * k + 1] = hi;
+            a.ws.mu[k] = a.bd.material_mu[3 * entry];
         }
     }
 }
@@ -2723,7 +2714,7 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     k_dedup<true><<<G, kBlock, 0, st>>>(a); note_launch();
     prof_mark(prof, 4, st);
     // contact problem
-    k_contacts<<<G, 128, 0, st>>>(a); note_launch();
+    k_contacts<<<2 * G, 128, 0, st>>>(a); note_launch();   // a thread per contact row
     if (bd->n_hinges > 0) {   // the hinge problem of every scene that has hinges
         k_hinge_lists<<<blocks_for(bd->n_scenes, 64), 64, 0, st>>>(a); note_launch();
         k_hinges<<<blocks_for(bd->n_hinges, 128), 128, 0, st>>>(a); note_launch();
