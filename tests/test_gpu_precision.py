@@ -62,3 +62,41 @@ def test_fp32_solve_of_a_scene_with_more_bodies_than_a_slab_holds():
     assert s64.n_contacts > 0 and s32.fp32_sweeps > 0
     assert np.abs(u32 - u64).max() <= 1e-3 * np.abs(u64).max()
     assert s32.residual <= 2.0 * s64.residual + 1e-6
+
+
+def _s32_bytes(K, nb):
+    """Shared memory of a scene's whole FP32 copy (the solver's size classes): 48 floats per contact, its
+    level-order position (2 B), body list entries (8 B) and body index pair (4 B), 16 floats per body, level
+    and list starts; each piece rounded up to 16 bytes."""
+    a = lambda v: (v + 15) // 16 * 16  # noqa: E731
+    return a(192 * K) + a(2 * K) + a(8 * K) + a(64 * nb) + a(4 * K) + a(2 * (K + 1)) + a(2 * (nb + 1))
+
+
+def test_fp32_solve_of_scenes_whose_rows_live_in_l2():
+    """Piles of 1500-2048 bodies: their contact rows no longer fit one SM's shared memory (more than 224 KB),
+    so the FP32 phase keeps the rows in global memory and the body records on chip, in 512-thread teams.  The
+    step must agree with the FP64 solve of the same step to a small fraction of the velocity scale, at a
+    residual of the same size."""
+    from rainbow_b200 import scenes
+    from rainbow_b200 import world as W
+    arrays, params = scenes.batch_arrays(n_scenes=2, seed=1, pool=8, body_range=(1500, 2048), resolution=16,
+                                         device="cuda:0", ground=40.0)
+    kw = dict(termination="residual_fixed_r", residual_tolerance=1e-6, residual_interval=4)
+    w = W.DeviceWorld(arrays, max_iterations=100)
+    for _ in range(100):
+        w.step(W.make_rb_params(params, precision="fp32_refine", **kw))
+    x0, u0 = w.state()
+    out = {}
+    for mode in ("fp64", "fp32_refine"):
+        w.set_state(x0, u0)
+        w.step(W.make_rb_params(params, precision=mode, **kw))
+        out[mode] = (w.state()[1], w.stats())
+    (u64, s64), (u32, s32) = out["fp64"], out["fp32_refine"]
+    nb = [len(a["body_mass"]) for a in arrays]
+    in_l2 = [i for i, s in enumerate(s32) if _s32_bytes(s.n_contacts, nb[i]) > 224 * 1024 and 64 * nb[i] < 150 * 1024]
+    assert in_l2, [(s.n_contacts, n) for s, n in zip(s32, nb)]
+    for i in in_l2:
+        b0, b1 = w.scene_start[i], w.scene_start[i + 1]
+        assert s32[i].fp32_sweeps > 0
+        assert np.abs(u32[b0:b1] - u64[b0:b1]).max() <= 1e-3 * np.abs(u64[b0:b1]).max()
+        assert s32[i].residual <= 2.0 * s64[i].residual + 1e-6
