@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--ordering", default="serial", choices=["serial", "coloured"],
                     help="contact order of the Gauss-Seidel sweeps (both arms use the same)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
-    ap.add_argument("--cpu-scenes", type=int, default=16, help="scenes in the CPU baseline sample")
+    ap.add_argument("--cpu-scenes", type=int, default=64, help="scenes in the CPU baseline sample (stratified)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the built-in launch shapes")
     ap.add_argument("--serve-seconds", type=float, default=20.0,
@@ -175,47 +175,82 @@ class ClockSampler:
 # --------------------------------------------------------------------------------------------------------------
 # CPU baseline: the oracle (C restatement of the reference step), bounded sample
 # --------------------------------------------------------------------------------------------------------------
-def _cpu_worker(job):
+def _cpu_task(job):
+    """One scene of the CPU baseline sample on one host core: bring it to the timed state (the GPU's state
+    after its pre-roll when given, else the oracle's own pre-roll), one untimed step (fills the warm-start
+    cache), then timed steps until `seconds` have passed (at least one).  Returns (steps, elapsed, bodies)."""
     sys.path.insert(0, ROOT)
     from oracle import oracle as O
-    scenes, scheme, tol_mode, tol, pre_roll, seconds, kw = job
-    objs = [O.OracleScene(a) for a in scenes]
-    for sc in objs:
+    scene, state, pre_roll, pre_cap, max_it, seconds, kw = job
+    sc = O.OracleScene(scene)
+    if state is not None:
+        sc.set_state(*state)
+    else:
+        sc.set_param("max_iterations", pre_cap)
         for _ in range(pre_roll):
-            sc.step(scheme=scheme, tol_mode=tol_mode, tol=tol, **kw)
+            sc.step(**kw)
+    sc.set_param("max_iterations", max_it)
+    sc.step(**kw)
     steps, t0 = 0, time.perf_counter()
     while True:
-        for sc in objs:
-            sc.step(scheme=scheme, tol_mode=tol_mode, tol=tol, **kw)
-            steps += 1
+        sc.step(**kw)
+        steps += 1
         el = time.perf_counter() - t0
-        if el >= seconds or steps >= 400:
-            break
-    return steps, el
+        if el >= seconds:
+            return steps, el, sc.n_bodies
 
 
-def cpu_baseline(arrays, args, workers):
-    """scene-steps/s of the oracle on the host: `workers` processes, each stepping its share of the sample."""
+def stratified_sample(body_counts, n):
+    """Indices of n scenes spread evenly over the scenes sorted by body count (every size stratum sampled)."""
+    order = np.argsort(np.asarray(body_counts), kind="stable")
+    n = max(1, min(n, len(order)))
+    return [int(order[int((k + 0.5) * len(order) / n)]) for k in range(n)]
+
+
+def cpu_baseline(arrays, args, workers, states=None, pre_cap=100):
+    """scene-steps/s of the oracle on the host cores for the workload's scene mix.
+
+    A stratified sample of the scenes (--cpu-scenes, by body count) goes through a shared task queue, largest
+    scenes first, so no core idles while another still has work; each task times one scene's steps on one
+    core while the others are busy too.  With t_i the measured time per step of sample scene i, the host
+    steps the whole mix (every scene once per step) at cores x n / sum(t_i) scene-steps/s -- the rate of a
+    perfectly load-balanced host -- and cores x sum(bodies_i) / sum(t_i) body-steps/s.  `states` gives each
+    scene's (x, u) at the start of the timed region (from the GPU run); without it each task pre-rolls its
+    scene on the oracle first."""
     import multiprocessing as mp
     from oracle import oracle as O
     O.build()
     tol_mode = {"merit": 0, "residual": 1, "residual_fixed_r": 2}[args.termination]
-    sample = arrays[:max(1, min(len(arrays), args.cpu_scenes))]
-    workers = max(1, min(workers, len(sample)))
-    kw = {"ordering": args.ordering,
-          "residual_interval": args.residual_interval if args.termination == "residual_fixed_r" else 1}
-    jobs = [(sample[w::workers], args.scheme, tol_mode, args.tolerance, args.pre_roll, args.cpu_seconds, kw)
-            for w in range(workers)]
+    idx = stratified_sample([len(a["body_mass"]) for a in arrays], args.cpu_scenes)
+    idx.sort(key=lambda i: -len(arrays[i]["body_mass"]))
+    kw = {"scheme": args.scheme, "tol_mode": tol_mode, "tol": args.tolerance, "ordering": args.ordering,
+          "residual_interval": args.residual_interval if args.termination == "residual_fixed_r" else 1,
+          "warm_start": not args.no_warm_start}
+    max_it = args.max_iterations or int(arrays[0]["params"][1])
+    per_task = max(0.05, args.cpu_seconds * workers / len(idx))
+    jobs = [(arrays[i], None if states is None else states[i], args.pre_roll, pre_cap, max_it, per_task, kw)
+            for i in idx]
+    workers = max(1, min(workers, len(jobs)))
+    t0 = time.perf_counter()
     if workers == 1:
-        res = [_cpu_worker(jobs[0])]
+        res = [_cpu_task(j) for j in jobs]
     else:
         with mp.get_context("spawn").Pool(workers) as pool:
-            res = pool.map(_cpu_worker, jobs)
-    steps = sum(r[0] for r in res)
-    el = max(r[1] for r in res)
-    return steps / el, {"cores": workers, "kind": "port",
-                        "sample": "%d scene(s) of the workload after a %d-step pre-roll, %d scene-steps in %.1f s on "
-                                  "%d process(es)" % (len(sample), args.pre_roll, steps, el, workers)}
+            res = list(pool.imap_unordered(_cpu_task, jobs))
+    wall = time.perf_counter() - t0
+    t = np.array([el / st for st, el, _ in res])          # seconds per step of each sample scene
+    bodies = np.array([nb for _, _, nb in res])
+    steps = int(sum(r[0] for r in res))
+    rate = workers * len(res) / t.sum()
+    return rate, {"cores": workers, "kind": "port", "body_steps_per_s": float(workers * bodies.sum() / t.sum()),
+                  "sample": "%d of %d scenes stratified by body count (%d..%d bodies), %s; %d timed scene-steps "
+                            "(%.2f s per scene on one core of %d busy ones, shared queue, %.1f s wall); rate = "
+                            "cores x scenes / sum of per-scene step times"
+                            % (len(res), len(arrays), int(bodies.min()), int(bodies.max()),
+                               "from the GPU's state after its pre-roll" if states is not None
+                               else "after a %d-step oracle pre-roll" % args.pre_roll,
+                               steps, per_task, workers, wall),
+                  "seconds_per_step_p50_max": [float(np.median(t)), float(t.max())]}
 
 
 def run_reference(args):

@@ -64,6 +64,7 @@ class OStepOut(ctypes.Structure):
         ("residuals", _d), ("delta_u_ext", _d),
         ("kinetic", ctypes.c_double), ("potential", ctypes.c_double), ("max_penetration", ctypes.c_double),
         ("hinge_b", _d), ("hinge_diag", _d), ("hinge_sol", _d),
+        ("warm_count", ctypes.c_int32), ("warm_key", _i64), ("warm_sol", _d), ("keys", _i64),
     ]
 
 
@@ -253,16 +254,31 @@ class OracleScene:
         self.q = np.ascontiguousarray(a["body_q"], dtype=np.float64).copy()
         self.v = np.ascontiguousarray(a["body_v"], dtype=np.float64).copy()
         self.w = np.ascontiguousarray(a["body_w"], dtype=np.float64).copy()
+        # warm-start cache of the last step: contact keys (2 int64 each, ascending) and impulses (4 each)
+        self.cache_key = np.zeros((0, 2), np.int64)
+        self.cache_sol = np.zeros((0, 4), np.float64)
+
+    def set_state(self, x, u):
+        """Body state from (N, 7) x = (r, q) and (N, 6) u = (v, w) arrays."""
+        x, u = np.asarray(x, np.float64).reshape(-1, 7), np.asarray(u, np.float64).reshape(-1, 6)
+        self.r[:] = x[:, :3]; self.q[:] = x[:, 3:]
+        self.v[:] = u[:, :3]; self.w[:] = u[:, 3:]
+
+    def reset_warm_start(self):
+        self.cache_key = np.zeros((0, 2), np.int64)
+        self.cache_sol = np.zeros((0, 4), np.float64)
 
     def set_param(self, name, value):
         self.params[PARAM_FIELDS.index(name)] = float(value)
 
     def step(self, dt=None, scheme="rigid_gauss_seidel", capacity=None, tol_mode=0, tol=0.0, residual_interval=1,
-             relaxation=1.0, ordering="serial"):
+             relaxation=1.0, ordering="serial", warm_start=False):
         """Advance one step; returns a dict with the contact set, solver result and statistics.
 
         ordering="coloured" makes the Gauss-Seidel schemes visit contacts colour by colour (the colouring of
-        rbo_colour_contacts); scheme "parallel_gauss_seidel" always does."""
+        rbo_colour_contacts); scheme "parallel_gauss_seidel" always does.  warm_start=True starts each contact
+        from the impulses the previous step found for the same key (body pair, side, triangle), as the GPU
+        step's cache does; the cache is always refreshed."""
         dt = float(self.params[0] if dt is None else dt)
         cap = int(capacity or max(1024, 64 * self.n_bodies))
         max_it = int(self.params[PARAM_FIELDS.index("max_iterations")])
@@ -276,6 +292,14 @@ class OracleScene:
         bufs.update(hinge_b=np.zeros(5 * H), hinge_diag=np.zeros(5 * H), hinge_sol=np.zeros(5 * H))
         for k in ("hinge_b", "hinge_diag", "hinge_sol"):
             setattr(out, k, _ptr(bufs[k], _d))
+        keys = np.zeros((cap, 2), np.int64)
+        out.keys = _ptr(keys, _i64)
+        wk = np.ascontiguousarray(self.cache_key, np.int64)
+        ws = np.ascontiguousarray(self.cache_sol, np.float64)
+        out.warm_count = len(wk) if warm_start else 0
+        out.warm_key = _ptr(wk if len(wk) else np.zeros((1, 2), np.int64), _i64)
+        out.warm_sol = _ptr(ws if len(ws) else np.zeros((1, 4)), _d)
+        self._warm_keep = (wk, ws)
         out.ids = _ptr(bufs["ids"], _i32)
         for k in ("p", "n", "g", "b", "diag", "sol", "residuals", "delta_u_ext"):
             setattr(out, k, _ptr(bufs[k], _d))
@@ -294,7 +318,9 @@ class OracleScene:
             raise NotImplementedError("hinge joints are solved with the reference stepper's rule only "
                                       "(rigid Gauss-Seidel, merit termination, serial order)")
         K = out.n_contacts
-        return dict(
+        self.cache_key = keys[:K].copy()
+        self.cache_sol = bufs["sol"][:4 * K].reshape(-1, 4).copy()
+        return dict(keys=self.cache_key.copy(),
             n_contacts=K, ids=bufs["ids"][:K].copy(), p=bufs["p"][:K].copy(), n=bufs["n"][:K].copy(),
             g=bufs["g"][:K].copy(), b=bufs["b"][:4 * K].copy(), diag=bufs["diag"][:4 * K].copy(),
             sol=bufs["sol"][:4 * K].copy(), iterations=out.iterations, exitcode=out.exitcode,

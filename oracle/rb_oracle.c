@@ -282,6 +282,14 @@ typedef struct {
     double* delta_u_ext;         /* 6 per body */
     double kinetic, potential, max_penetration;
     double* hinge_b; double* hinge_diag; double* hinge_sol;   /* 5 per hinge (NULL: not recorded) */
+    /* warm start (an option of the GPU step, not of the reference, which starts from zero, contacts.py:53):
+       contact k starts from the impulses of the cache entry with its key, when there is one.  Key of a
+       contact = (lower body << 31 | higher body, side << 30 | triangle), side 1 when the mesh owner is the
+       higher body; the contacts of a step come out in ascending key order. */
+    int32_t warm_count;          /* entries of warm_key / warm_sol (0: every contact starts from zero) */
+    const int64_t* warm_key;     /* 2 per entry, ascending */
+    const double* warm_sol;      /* 4 per entry */
+    int64_t* keys;               /* out: 2 per contact (NULL: not recorded) */
 } OStepOut;
 
 typedef struct { double lo[3], hi[3]; } AABB;
@@ -306,21 +314,27 @@ typedef struct {
     int n;
     int cap;
     int32_t* ids; double* p; double* n_; double* g;
+    int64_t* key;   /* 2 per contact: warm-start key (see OStepOut.warm_key) */
 } ContactList;
 
-static void contacts_push(ContactList* cl, int a, int b, const double* p, const double* n, double g) {
+static void contacts_push(ContactList* cl, int a, int b, const double* p, const double* n, double g, int tri) {
     if (cl->n == cl->cap) {
         cl->cap = cl->cap ? 2 * cl->cap : 64;
         cl->ids = (int32_t*)realloc(cl->ids, sizeof(int32_t) * 2 * cl->cap);
         cl->p = (double*)realloc(cl->p, sizeof(double) * 3 * cl->cap);
         cl->n_ = (double*)realloc(cl->n_, sizeof(double) * 3 * cl->cap);
         cl->g = (double*)realloc(cl->g, sizeof(double) * cl->cap);
+        cl->key = (int64_t*)realloc(cl->key, sizeof(int64_t) * 2 * cl->cap);
     }
     int k = cl->n++;
     cl->ids[2 * k] = a; cl->ids[2 * k + 1] = b;
     memcpy(cl->p + 3 * k, p, 3 * sizeof(double));
     memcpy(cl->n_ + 3 * k, n, 3 * sizeof(double));
     cl->g[k] = g;
+    /* a = SDF owner, b = mesh owner */
+    const int lo = a < b ? a : b, hi = a < b ? b : a;
+    cl->key[2 * k] = ((int64_t)lo << 31) | (int64_t)hi;
+    cl->key[2 * k + 1] = ((int64_t)(b == hi) << 30) | (int64_t)tri;
 }
 
 /* collision_detection.py:87 _compute_contacts: triangles of body A (mesh) against the SDF of body B */
@@ -388,7 +402,7 @@ static void compute_contacts(const OScene* sc, const double* params, const doubl
                     quat_rotate(qB, x, xr);
                     pw[0] = xr[0] + rB[0]; pw[1] = xr[1] + rB[1]; pw[2] = xr[2] + rB[2];
                     double un[3] = {nw[0] / ln, nw[1] / ln, nw[2] / ln};
-                    contacts_push(out, B, A, pw, un, phi);
+                    contacts_push(out, B, A, pw, un, phi, tris[ti]);
                 }
             }
         }
@@ -500,6 +514,7 @@ static void run_collision_detection(const OScene* sc, const double* params, cons
         if (unique) {
             if (kept != k) {
                 cl->ids[2 * kept] = a; cl->ids[2 * kept + 1] = b;
+                cl->key[2 * kept] = cl->key[2 * k]; cl->key[2 * kept + 1] = cl->key[2 * k + 1];
                 memmove(cl->p + 3 * kept, pk, 3 * sizeof(double));
                 memmove(cl->n_ + 3 * kept, cl->n_ + 3 * k, 3 * sizeof(double));
                 cl->g[kept] = cl->g[k];
@@ -1281,12 +1296,16 @@ int rbo_step(const OScene* sc, const double* params, double dt, double* r, doubl
         free(dux); free(Winv); free(u); free(du);
         return 4;
     }
-    ContactList cl = {0, 0, NULL, NULL, NULL, NULL};
+    ContactList cl = {0, 0, NULL, NULL, NULL, NULL, NULL};
     run_collision_detection(sc, params, r, q, &cl, out);
     const int K = cl.n;
     for (int k = 0; k < K; ++k) {
         double ln = norm3_np(cl.n_ + 3 * k);
-        if (fabs(1.0 - ln) > 0.1) { free(dux); free(Winv); free(u); free(du); return 3; }
+        if (fabs(1.0 - ln) > 0.1) {
+            free(cl.ids); free(cl.p); free(cl.n_); free(cl.g); free(cl.key);
+            free(dux); free(Winv); free(u); free(du);
+            return 3;
+        }
     }
     Problem P;
     memset(&P, 0, sizeof(P));
@@ -1335,6 +1354,20 @@ int rbo_step(const OScene* sc, const double* params, double dt, double* r, doubl
         x = (double*)calloc((size_t)4 * K, sizeof(double));
         sol = (double*)calloc((size_t)4 * K, sizeof(double));
         mu = (double*)malloc(sizeof(double) * K);
+        if (out->warm_count > 0 && out->warm_key && out->warm_sol) {
+            /* warm start: x = sol = the cached impulses of the contact with the same key (binary search) */
+            for (int k = 0; k < K; ++k) {
+                const int64_t k1 = cl.key[2 * k], k2 = cl.key[2 * k + 1];
+                int lo_i = 0, hi_i = out->warm_count;
+                while (lo_i < hi_i) {
+                    const int mid = (lo_i + hi_i) >> 1;
+                    const int64_t m1 = out->warm_key[2 * mid], m2 = out->warm_key[2 * mid + 1];
+                    if (m1 < k1 || (m1 == k1 && m2 < k2)) lo_i = mid + 1; else hi_i = mid;
+                }
+                if (lo_i < out->warm_count && out->warm_key[2 * lo_i] == k1 && out->warm_key[2 * lo_i + 1] == k2)
+                    for (int i = 0; i < 4; ++i) x[4 * k + i] = sol[4 * k + i] = out->warm_sol[4 * lo_i + i];
+            }
+        }
         double* vv = (double*)malloc(sizeof(double) * 4 * K);
         double* jd = (double*)malloc(sizeof(double) * 4 * K);
         double* dtd = (double*)malloc(sizeof(double) * 6 * N);
@@ -1456,6 +1489,7 @@ int rbo_step(const OScene* sc, const double* params, double dt, double* r, doubl
         if (out->b) memcpy(out->b, b, sizeof(double) * 4 * Kc);
         if (out->diag) memcpy(out->diag, diag, sizeof(double) * 4 * Kc);
         if (out->sol) memcpy(out->sol, sol, sizeof(double) * 4 * Kc);
+        if (out->keys) memcpy(out->keys, cl.key, sizeof(int64_t) * 2 * Kc);
     }
     double gap = 0.0;
     for (int k = 0; k < K; ++k) if (cl.g[k] < gap) gap = cl.g[k];
@@ -1463,7 +1497,7 @@ int rbo_step(const OScene* sc, const double* params, double dt, double* r, doubl
     energies(sc, r, q, v, w, &out->kinetic, &out->potential);
     if (K > 0) problem_free(&P);
     free(b); free(diag); free(rr); free(x); free(sol); free(mu);
-    free(cl.ids); free(cl.p); free(cl.n_); free(cl.g);
+    free(cl.ids); free(cl.p); free(cl.n_); free(cl.g); free(cl.key);
     free(dux); free(Winv); free(u); free(du);
     return out->overflow ? 1 : 0;
 }

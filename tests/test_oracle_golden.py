@@ -76,3 +76,31 @@ def test_oracle_hinges_match_reference_step_by_step(oracle_lib, name):
         assert (o["iterations"], o["exitcode"]) == (d["step_iterations"][s], d["step_exitcode"][s]), s
         np.testing.assert_array_equal(o["x"], d["step_x"][s], err_msg="step %d x" % s)
         np.testing.assert_array_equal(o["u"], d["step_u"][s], err_msg="step %d u" % s)
+
+
+def test_oracle_warm_start_cache():
+    """Warm start in the oracle: contact keys come out ascending, a step with an empty cache equals a cold
+    step, and warm-started solves meet the residual tolerance in fewer sweeps over a trajectory."""
+    from oracle import oracle as O
+    d = load_fixture("c1_boxes64")
+    cold, warm = O.OracleScene(d), O.OracleScene(d)
+    for sc in (cold, warm):
+        sc.set_param("max_iterations", 2000)
+    kw = dict(tol_mode=2, tol=1e-6, residual_interval=1)
+    a, b = cold.step(**kw), warm.step(warm_start=True, **kw)
+    np.testing.assert_array_equal(a["sol"], b["sol"])
+    np.testing.assert_array_equal(a["x"], b["x"])
+    sweeps = {False: a["iterations"], True: b["iterations"]}
+    for _ in range(6):
+        a, b = cold.step(**kw), warm.step(warm_start=True, **kw)
+        assert a["exitcode"] == 3 and b["exitcode"] == 3
+        sweeps[False] += a["iterations"]
+        sweeps[True] += b["iterations"]
+        k = b["keys"]
+        assert len(k) == b["n_contacts"]
+        assert all(tuple(k[i]) < tuple(k[i + 1]) for i in range(len(k) - 1))
+        lo = np.minimum(b["ids"][:, 0], b["ids"][:, 1]).astype(np.int64)
+        hi = np.maximum(b["ids"][:, 0], b["ids"][:, 1]).astype(np.int64)
+        np.testing.assert_array_equal(k[:, 0], (lo << 31) | hi)
+        np.testing.assert_array_equal(k[:, 1] >> 30, (b["ids"][:, 1] == hi).astype(np.int64))
+    assert sweeps[True] < sweeps[False]
