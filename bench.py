@@ -2,23 +2,33 @@
 """Benchmark of the prox_rigid_bodies time step on B200: one JSON line on stdout (rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+                    [--max-iterations M]
 
 Workloads (synthetic, seeded; the shapes go through the reference-compatible set-up chain):
   batch1024  1024 independent scenes, 8..256 bodies each (log-uniform), random boxes (side U(0.5, 2)) and spheres
-             (radius U(0.25, 1), 16 x 16 sweep) drawn from a 64 + 64 size pool, random orientations, density 1000,
-             mu U(0.2, 0.8) per scene, on a fixed ground box; SDF resolution 32; dt 0.01 (default)
+             (radius U(0.25, 1), 16 x 16 sweep) with random orientations, density 1000, mu U(0.2, 0.8) per scene,
+             on a fixed ground box; SDF resolution 32; dt 0.01 (default).  --shapes pool draws the sizes from a
+             pool of 64 boxes + 64 spheres shared by all scenes; --shapes per-body gives every body a shape and
+             signed distance grid of its own (the configuration as stated)
   mixed4096  one scene of 4096 bodies (16^3 lattice, spacing 1.2): alternating unit boxes and r = 0.5 spheres,
              random orientations, density 1000, on a fixed ground box; SDF resolution 64
   boxes64    one scene of 64 unit boxes (4^3 lattice, spacing 1.05, jitter +-0.02) on a 20 x 1 x 20 ground
+  tower32    the precision stress alone: 32-box tower, masses 1 / 1000, FP64 vs FP32 + FP64 refinement vs FP32
 A step advances every scene of the workload by one semi-implicit time step.  Bodies start in the air; a
-pre-roll of --pre-roll untimed steps lets them land before warm-up and timing.  Every solve runs to the same
-complementarity residual (--tolerance, FP64) unless --termination merit selects the reference's merit test.
-The metric is scene-steps/s with the p50/p99 step latency.  Scenes do not exchange data: with --gpus N every
-rank steps its own copy of the workload (weak scaling, no collective on the data path) and the value is the
-total over the max-over-ranks time.
+pre-roll of --pre-roll untimed steps (at the configuration's own 100-iteration limit) lets them land.
 
---impl reference times the CPU restatement of the reference step (oracle/rb_oracle.c) on a bounded sample of
-the same workload on the host cores (one process per core for multi-scene workloads).
+Equal residual.  Every solve of every arm (batched, plain one-scene-per-launch FP64, served, CPU) stops at the
+same complementarity residual (--tolerance 1e-6, evaluated in FP64) or at --max-iterations sweeps, whichever
+comes first, with the same solver; the line reports how many scenes met the tolerance in each arm and the
+residuals of those that did not.  The same measurement at the configuration's own 100-sweep limit is
+reported as a second, labelled block (at_100_sweeps).
+
+The metric is scene-steps/s with the p50/p99 step latency, batched and served, against the plain FP64 step.
+Scenes do not exchange data: with --gpus N every rank steps its own share (weak scaling, no collective on the
+data path) and the value is the total over the max-over-ranks time.
+
+--impl reference times the CPU restatement of the reference step (oracle/rb_oracle.c) on a bounded,
+stratified sample of the same workload on all host cores.
 """
 import argparse
 import json
@@ -33,10 +43,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-
-
-PROFILED_SOLVE_DRAM_BYTES = 87_492_096   # FP32 solve kernels of one batch1024 step (ncu, cold caches)
-LONG_SWEEPS = 4000   # iteration cap of the converged reference solve the error figures are measured against
+# DRAM bytes per launch of the dominant kernels, from ncu captures of this build (see the profile summaries):
+# kernel -> (bytes, workload the capture ran on)
+PROFILED_DRAM_BYTES = {}
+EQUAL_RESIDUAL_SWEEPS = 4000   # default sweep cap of the equal-residual measurement
 
 
 def parse():
@@ -45,14 +55,19 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batch1024", choices=["batch1024", "mixed4096", "boxes64", "tower32"],
-                    help="tower32: the precision stress comparison (FP64 / FP32 + FP64 refinement / FP32)")
+    ap.add_argument("--workload", default="batch1024", choices=["batch1024", "mixed4096", "boxes64", "tower32"])
+    ap.add_argument("--shapes", default="pool", choices=["pool", "per-body"],
+                    help="batch1024: sizes from a shared pool of 64 + 64 shapes, or a shape and SDF per body")
     ap.add_argument("--scheme", default="rigid_gauss_seidel")
     ap.add_argument("--termination", default="residual_fixed_r", choices=["residual_fixed_r", "residual", "merit"])
     ap.add_argument("--scenes", type=int, default=1024, help="scenes of the batch1024 workload")
     ap.add_argument("--tolerance", type=float, default=1e-6)
+    ap.add_argument("--max-iterations", type=int, default=EQUAL_RESIDUAL_SWEEPS,
+                    help="sweep cap of every solve of every arm (the equal-residual measurement)")
     ap.add_argument("--pre-roll", type=int, default=60)
-    ap.add_argument("--plain-scenes", type=int, default=32, help="scenes of the one-scene-per-launch baseline")
+    ap.add_argument("--plain-scenes", type=int, default=16,
+                    help="scenes (stratified by body count) of the one-scene-per-launch baseline")
+    ap.add_argument("--plain-steps", type=int, default=3, help="timed steps per plain scene")
     ap.add_argument("--no-warm-start", action="store_true", help="start every solve from zero impulses")
     ap.add_argument("--precision", default="fp32_refine", choices=["fp64", "fp32_refine", "fp32"],
                     help="precision of the batched solve (the plain baseline is always FP64)")
@@ -63,27 +78,32 @@ def parse():
     ap.add_argument("--cpu-scenes", type=int, default=64, help="scenes in the CPU baseline sample (stratified)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the built-in launch shapes")
+    ap.add_argument("--no-100", action="store_true", help="skip the 100-sweep block")
+    ap.add_argument("--no-configs", action="store_true", help="skip the C1 / C2 / C4 sub-results")
     ap.add_argument("--serve-seconds", type=float, default=20.0,
                     help="wall time of the serving run (Poisson arrivals, continuous batching); 0 skips it")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="request arrival rate (requests/s)")
     ap.add_argument("--serve-max-bodies", type=int, default=131072,
                     help="resident-body cap of the server (its step-latency target)")
     ap.add_argument("--serve-templates", type=int, default=192, help="distinct scenes the requests draw from")
+    ap.add_argument("--serve-plain-scenes", type=int, default=8)
     return ap.parse_args()
 
 
 # --------------------------------------------------------------------------------------------------------------
 # workloads
 # --------------------------------------------------------------------------------------------------------------
-def build_workload(name, device, n_scenes=1024):
+def build_workload(name, device, n_scenes=1024, shapes="pool"):
     from rainbow_b200 import engine_io, scenes
     if name == "batch1024":
-        arrays, params = scenes.batch_arrays(n_scenes=n_scenes, seed=0, pool=64, resolution=32, device=device)
+        pool = 64 if shapes == "pool" else None
+        arrays, params = scenes.batch_arrays(n_scenes=n_scenes, seed=0, pool=pool, resolution=32, device=device)
         bodies = sum(len(a["body_mass"]) for a in arrays)
         cfg = {"workload": "batch_%d_scenes" % n_scenes, "scenes": n_scenes, "bodies": int(bodies),
                "bodies_per_scene": "8..256",
-               "shapes": "boxes side U(0.5,2), spheres r U(0.25,1) 16x16, pool 64+64", "sdf_resolution": 32,
-               "dt": 0.01}
+               "shapes": ("boxes side U(0.5,2), spheres r U(0.25,1) 16x16, "
+                          + ("sizes from a pool of 64+64 shapes" if pool else "a shape and SDF per body")),
+               "sdf_resolution": 32, "dt": 0.01}
         return arrays, params, cfg, None
     if name == "mixed4096":
         engine = scenes.mixed_lattice(n=16, spacing=1.2, resolution=64, seed=0, device=device)
@@ -227,10 +247,12 @@ def cpu_baseline(arrays, args, workers, states=None, pre_cap=100):
           "residual_interval": args.residual_interval if args.termination == "residual_fixed_r" else 1,
           "warm_start": not args.no_warm_start}
     max_it = args.max_iterations or int(arrays[0]["params"][1])
-    per_task = max(0.05, args.cpu_seconds * workers / len(idx))
-    jobs = [(arrays[i], None if states is None else states[i], args.pre_roll, pre_cap, max_it, per_task, kw)
+    workers = max(1, min(workers, len(idx)))
+    per_task = max(0.05, args.cpu_seconds * workers / len(idx))   # about cpu_seconds of wall time in all
+    def host(a):   # grids built on the device (per-body shapes) travel to the workers as host arrays
+        return {k: (v.cpu().numpy() if hasattr(v, "cpu") else v) for k, v in a.items()}
+    jobs = [(host(arrays[i]), None if states is None else states[i], args.pre_roll, pre_cap, max_it, per_task, kw)
             for i in idx]
-    workers = max(1, min(workers, len(jobs)))
     t0 = time.perf_counter()
     if workers == 1:
         res = [_cpu_task(j) for j in jobs]
@@ -260,10 +282,15 @@ def run_reference(args):
     workers = os.cpu_count() or 1
     import torch
     dev = "cuda:0" if torch.cuda.is_available() else "cpu"
-    arrays, params, cfg, _ = build_workload(args.workload, dev, args.scenes)
+    if args.workload == "tower32":
+        from rainbow_b200 import engine_io, scenes
+        arrays = [engine_io.scene_arrays(scenes.box_tower(32, device=dev))]
+        cfg = {"workload": "box_tower_32_mass_ratio_1e3", "bodies": 33, "dt": 0.005}
+    else:
+        arrays, _, cfg, _ = build_workload(args.workload, dev, args.scenes, args.shapes)
     value, info = cpu_baseline(arrays, args, workers if len(arrays) > 1 else 1)
     cfg.update({"scheme": args.scheme, "ordering": args.ordering, "termination": args.termination,
-                "tolerance": args.tolerance})
+                "tolerance": args.tolerance, "max_iterations": args.max_iterations})
     line = {
         "impl": "reference", "metric": "scene-steps/s", "value": value, "unit": "scene-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
@@ -276,17 +303,150 @@ def run_reference(args):
 
 
 # --------------------------------------------------------------------------------------------------------------
+# helpers of the GPU arms
+# --------------------------------------------------------------------------------------------------------------
+def scene_cache(key, sol, count, b0, b1):
+    """Warm-start cache entries of the scene owning global bodies b0..b1-1 (device tensors of a batch: keys
+    (lower << 31 | higher, side << 30 | triangle) ascending, 4 impulses each), re-keyed to the scene's own
+    body indices.  Returns host arrays (n, 2) int64 and (n, 4) float64."""
+    n = int(count.reshape(-1)[0].item())
+    k = key[:2 * n].view(n, 2).cpu().numpy().copy()
+    s = sol[:4 * n].view(n, 4).cpu().numpy()
+    lo = k[:, 0] >> 31
+    m = (lo >= b0) & (lo < b1)
+    k = k[m]
+    k[:, 0] -= (np.int64(b0) << 31) + np.int64(b0)
+    return k, s[m].copy()
+
+
+def install_cache(world, keys, sols):
+    """Warm-start cache of a one-scene DeviceWorld (grown first when it cannot hold the entries)."""
+    import torch
+    n = len(keys)
+    if 2 * n > world.t_cache_key.numel():
+        world.caps.contact_capacity = max(n, 2 * world.caps.contact_capacity)
+        world._alloc()
+    world.t_cache_key[:2 * n].copy_(torch.from_numpy(keys.reshape(-1)))
+    world.t_cache_sol[:4 * n].copy_(torch.from_numpy(sols.reshape(-1)))
+    world.t_cache_count.fill_(n)
+
+
+def timed_steps(step_fn, steps, stream, flush):
+    """Device time (ms) of each of `steps` calls of step_fn, which enqueues one step on `stream`."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        flush.zero_()                      # evict L2 (126 MB) between timed steps
+        ev[k][0].record(stream)
+        step_fn()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    return np.array([a.elapsed_time(b) for a, b in ev])   # ms
+
+
+def solve_summary(stats, cap):
+    """Convergence of one step's solves: how many met the tolerance, sweeps, residuals of the others."""
+    act = [s for s in stats if s.n_contacts > 0]
+    if not act:
+        return None
+    conv = [s for s in act if s.exitcode == 3]
+    unc = np.array([s.residual for s in act if s.exitcode != 3])
+    sw = np.array([s.iterations + 1 if s.exitcode == 3 else cap for s in act])
+    return {"scenes_with_contacts": len(act), "met_tolerance": len(conv), "unconverged": len(act) - len(conv),
+            "unconverged_residual_p50_p99_max": [float(np.percentile(unc, 50)), float(np.percentile(unc, 99)),
+                                                 float(unc.max())] if len(unc) else None,
+            "sweeps_p50_p90_max": [float(np.percentile(sw, 50)), float(np.percentile(sw, 90)), int(sw.max())],
+            "residual_median": float(np.median([s.residual for s in act]))}
+
+
+def batched_arm(world, rp, steps, warmup, restore, flush, gpu, dist=None):
+    """Timed graph replays of the whole batch from the saved state: a sizing pass over the timed horizon (so
+    no timed step can overflow a work list), warm-up steps, one CUDA graph of the step, then `steps` replays
+    with the L2 flushed between them.  Returns times (ms), kernel launches, clocks, status and the last
+    step's statistics."""
+    import torch
+    from rainbow_b200 import _native
+    stream = torch.cuda.current_stream()
+    restore()
+    for _ in range(steps):
+        world.step(rp)
+    restore()
+    for _ in range(max(3, warmup)):
+        world.step(rp)
+    lib = _native.load()
+    launches0 = lib.rb_launch_count()
+    graph = world.capture(rp)
+    per_replay = lib.rb_launch_count() - launches0
+    restore()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    world.t_status.zero_()
+    with ClockSampler(gpu) as clocks:
+        times = timed_steps(graph.replay, steps, stream, flush)
+    del graph
+    if dist is not None:
+        dist.barrier()
+    return times, per_replay * steps, clocks.summary(), int(world.t_status[0].item()), world.stats()
+
+
+def plain_arm(world, arrays, idx, x0, u0, cache, rp, steps, flush, max_it):
+    """The plain baseline: each sampled scene alone, one rb_step launch sequence per scene-step, FP64, from the
+    batch's saved state and warm-start cache; timed with direct launches and with graph replays.  FP64
+    results are bit-identical alone and batched, so these are the batched FP64 scene's own steps."""
+    import torch
+    from rainbow_b200 import world as W
+    stream = torch.cuda.current_stream()
+    x0r, u0r = x0.reshape(-1, 7), u0.reshape(-1, 6)
+    pts, gts, last = [], [], []
+    for s in idx:
+        b0, b1 = int(world.scene_start[s]), int(world.scene_start[s + 1])
+        keys, sols = scene_cache(*cache, b0, b1)
+        w1 = W.DeviceWorld(arrays[s], device=world.device, max_iterations=max_it)
+
+        def start():
+            w1.set_state(x0r[b0:b1], u0r[b0:b1])
+            install_cache(w1, keys, sols)
+        start()
+        for _ in range(steps):
+            w1.step(rp)                  # sizes its work lists over the horizon
+        start()
+        torch.cuda.synchronize()
+        pts.append(timed_steps(lambda: w1.launch(rp), steps, stream, flush))
+        last.append(w1.stats()[0])
+        g1 = w1.capture(rp)
+        start()
+        torch.cuda.synchronize()
+        gts.append(timed_steps(g1.replay, steps, stream, flush))
+        del g1, w1
+    pt, gt = np.concatenate(pts), np.concatenate(gts)
+    return {"value": len(pt) / (pt.sum() / 1000.0), "unit": "scene-steps/s", "scenes_sampled": len(idx),
+            "steps_per_scene": steps,
+            "bodies_sampled": [int(world.scene_start[s + 1] - world.scene_start[s]) for s in idx],
+            "p50_ms": float(np.percentile(pt, 50)), "p99_ms": float(np.percentile(pt, 99)),
+            "graph_value": len(gt) / (gt.sum() / 1000.0),
+            "graph_p50_ms": float(np.percentile(gt, 50)), "graph_p99_ms": float(np.percentile(gt, 99)),
+            "solve_last_step": solve_summary(last, max_it),
+            "method": "scenes stratified by body count, each alone: one rb_step launch sequence per scene-step, "
+                      "FP64, same solver settings, from the batch's state and warm-start cache (bit-identical to "
+                      "the batch's FP64 step); graph_* = the same steps replayed from a CUDA graph per scene"}
+
+
+# --------------------------------------------------------------------------------------------------------------
 # serving: Poisson stream of scene simulations through the continuous-batching server
 # --------------------------------------------------------------------------------------------------------------
-def run_serving(args, dev, rp_kw, max_it):
+def run_serving(args, dev, rp_kw, max_it, flush, tuning=None):
     """Requests arrive as a Poisson stream (rate --serve-rate) of scenes with 16..2048 bodies (log-uniform) and
     horizons U[50, 500] steps; the server admits them by its memory budget (80 % of the device) and body cap.
-    Returns throughput and latency of the run and of the same scenes stepped alone, one per launch."""
+    Returns throughput and latency of the run and of resident scenes stepped alone, one per launch, FP64."""
     import torch
-    from rainbow_b200 import scenes, serving, world as W
+    from rainbow_b200 import autotune, scenes, serving, world as W
     templates, params = scenes.batch_arrays(n_scenes=args.serve_templates, seed=1, pool=64,
                                             body_range=(16, 2048), resolution=32, device=dev, ground=40.0)
     rp = W.make_rb_params(params, **rp_kw)
+    rp.max_iterations = max_it
+    if tuning:
+        autotune.apply(rp, {k: v for k, v in tuning.items() if k in autotune.DEFAULTS})
     rng = np.random.default_rng(7)
     srv = serving.Server(rp, device=dev, max_iterations=max_it, hbm_fraction=0.8,
                          max_active_bodies=args.serve_max_bodies)
@@ -303,108 +463,245 @@ def run_serving(args, dev, rp_kw, max_it):
             next_arrival += rng.exponential(1.0 / args.serve_rate)
         srv.tick()
     rep = srv.report()
+    last = srv.batch.stats() if srv.batch is not None else []
     rep.update({"seconds": args.serve_seconds, "arrival_rate": args.serve_rate, "submitted": submitted,
                 "queued_at_end": len(srv.queue), "resident_body_cap": args.serve_max_bodies,
-                "memory_budget_gb": srv.budget / 1e9,
+                "memory_budget_gb": srv.budget / 1e9, "solve_last_tick": solve_summary(last, max_it),
                 "workload": "Poisson requests, scenes of 16..2048 bodies (log-uniform; %d distinct), horizons "
                             "U[50,500], boxes/spheres as the batch workload on a 40 x 1 x 40 ground"
                             % len(templates)})
-    # plain: scenes resident at the end of the run, each stepped alone from its current state, one rb_step per
-    # scene-step (FP64, same solver settings)
+    # plain: scenes resident at the end of the run (seeded pick), each stepped alone from its current state and
+    # warm-start cache, one rb_step per scene-step, FP64, same solver settings
     rp64 = W.make_rb_params(params, **dict(rp_kw, precision="fp64"))
+    rp64.max_iterations = max_it
     stream = torch.cuda.current_stream()
-    times = []
-    resident = [r for r in srv.active if r.done < r.horizon]
-    pick = rng.choice(len(resident), size=min(16, len(resident)), replace=False) if resident else []
-    for i in pick:
-        r = resident[int(i)]
-        x, u = srv.batch.scene_state(r.slot)
+    b = srv.batch
+    resident = sorted([r for r in srv.active if r.done < r.horizon], key=lambda r: r.uid)
+    pick = np.random.default_rng(11).choice(len(resident), size=min(args.serve_plain_scenes, len(resident)),
+                                            replace=False) if resident else []
+    times, last = [], []
+    for i in sorted(int(v) for v in pick):
+        r = resident[i]
+        b0, b1 = int(b.scene_start[r.slot]), int(b.scene_start[r.slot + 1])
+        x, u = b.scene_state(r.slot)
+        keys, sols = scene_cache(b.t_cache_key, b.t_cache_sol, b.t_cache_count, b0, b1)
         w1 = W.DeviceWorld(r.scene, device=dev, max_iterations=max_it)
-        w1.set_state(x, u)
-        w1.step(rp64)                      # sizes its work lists
-        w1.set_state(x, u)
+
+        def start():
+            w1.set_state(x, u)
+            install_cache(w1, keys, sols)
+        start()
+        for _ in range(args.plain_steps):
+            w1.step(rp64)                  # sizes its work lists
+        start()
         torch.cuda.synchronize()
-        for _ in range(5):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            w1.launch(rp64)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            times.append(e0.elapsed_time(e1))
-    times = np.array(times)
-    rep["plain"] = {"value": len(times) / (times.sum() / 1000.0), "unit": "scene-steps/s",
-                    "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
-                    "sample": "%d scenes resident at the end of the run, 5 steps each from their current state, one "
-                              "rb_step per scene-step, FP64" % len(pick)}
-    rep["served_vs_plain"] = rep["scene_steps_per_s"] / rep["plain"]["value"] if rep.get("scene_steps_per_s") else None
+        times.append(timed_steps(lambda: w1.launch(rp64), args.plain_steps, stream, flush))
+        last.append(w1.stats()[0])
+        del w1
+    times = np.concatenate(times) if times else np.zeros(0)
+    if len(times):
+        rep["plain"] = {"value": len(times) / (times.sum() / 1000.0), "unit": "scene-steps/s",
+                        "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
+                        "solve_last_step": solve_summary(last, max_it),
+                        "sample": "%d scenes resident at the end of the run (seeded pick), %d steps each from their "
+                                  "state and warm-start cache, one rb_step per scene-step, FP64"
+                                  % (len(pick), args.plain_steps)}
+        rep["served_vs_plain"] = rep["scene_steps_per_s"] / rep["plain"]["value"] if rep.get("scene_steps_per_s") else None
     return rep
 
 
 # --------------------------------------------------------------------------------------------------------------
-# GPU
+# the configurations beside the headline: C1 (64 boxes, coloured GS, through API.simulate), C2 (4097-body
+# lattice, Gauss-Seidel and Jacobi, FP64 vs FP32 + refinement), C4 (the mass-ratio tower, 500 steps)
 # --------------------------------------------------------------------------------------------------------------
-def timed_steps(step_fn, steps, stream, flush):
-    """Device time (ms) of each of `steps` calls of step_fn, which enqueues one step on `stream`."""
+def config_c1(dev, cpu=True):
+    """64 unit boxes on a ground, coloured proximal Gauss-Seidel, FP64, the reference's merit rule (100
+    iterations, relative tolerance 1e-6), 100 steps through the drop-in GpuStepper and api.simulate, with the
+    engine's bodies read and written every step (host state in and out)."""
     import torch
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-    for k in range(steps):
-        flush.zero_()                      # evict L2 (126 MB) between timed steps
-        ev[k][0].record(stream)
-        step_fn()
-        ev[k][1].record(stream)
+    from rainbow_b200 import api as API, engine_io, scenes
+    engine = scenes.box_lattice(n=4, spacing=1.05, jitter=0.02, resolution=32, seed=0, device=dev)
+    engine.params.proximal_solver = "parallel_gauss_seidel"
+    arrays0 = engine_io.scene_arrays(engine)
+    dt = engine.params.time_step
+    API.simulate(engine, dt)                      # first step: uploads the scene, sizes the work lists
+    walls = []
+    for _ in range(99):
+        t0 = time.perf_counter()
+        API.simulate(engine, dt)
+        walls.append(time.perf_counter() - t0)
     torch.cuda.synchronize()
-    return np.array([a.elapsed_time(b) for a, b in ev])   # ms
+    walls = np.array(walls)
+    out = {"workload": "box_lattice_64 (4^3, spacing 1.05, jitter 0.02), SDF 32, dt 0.01, mu 0.5",
+           "solver": "parallel_gauss_seidel (coloured), FP64, merit rule, max 100 iterations",
+           "api": "rainbow_b200.api.simulate -> GpuStepper.step (engine state in and out every step)",
+           "steps": 100, "steps_per_s": float(len(walls) / walls.sum()),
+           "step_wall_ms_p50_p99": [float(np.percentile(walls, 50) * 1e3), float(np.percentile(walls, 99) * 1e3)],
+           "contacts_last_step": len(engine.contact_points)}
+    if cpu:   # the oracle on one host core, same 100 steps
+        from oracle import oracle as O
+        O.build()
+        sc = O.OracleScene(arrays0)
+        t0 = time.perf_counter()
+        for _ in range(100):
+            sc.step(scheme="parallel_gauss_seidel")
+        el = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 100.0 / el, "unit": "steps/s", "cores": 1, "kind": "port",
+                               "sample": "the same 100 steps on the oracle"}
+    return out
 
 
+def config_c2(dev, args, flush):
+    """4097-body box/sphere lattice (SDF resolution 64), after a 30-step pre-roll: Gauss-Seidel FP64,
+    Gauss-Seidel FP32 + FP64 refinement and proximal Jacobi FP64, each for a few steps from the same state at
+    the equal-residual settings; error of each against Gauss-Seidel FP64 after the first step."""
+    import torch
+    from rainbow_b200 import engine_io, scenes, world as W
+    arrays = engine_io.scene_arrays(scenes.mixed_lattice(n=16, spacing=1.2, resolution=64, seed=0, device=dev))
+    params = W.params_from_vector(arrays["params"])
+    cap = args.max_iterations
+    world = W.DeviceWorld(arrays, device=dev, max_iterations=max(cap, 100))
+    kw = dict(termination="residual_fixed_r", residual_tolerance=args.tolerance,
+              residual_interval=args.residual_interval, warm_start=True)
+    pre = W.make_rb_params(params, precision="fp32_refine", **kw)
+    for _ in range(30):
+        world.step(pre)
+    x0, u0 = world.state()
+    cache = (world.t_cache_key.clone(), world.t_cache_sol.clone(), world.t_cache_count.clone())
+    stream = torch.cuda.current_stream()
+    arms = [("gauss_seidel_fp64", "rigid_gauss_seidel", "fp64"), ("gauss_seidel_fp32_refine", "rigid_gauss_seidel",
+                                                                   "fp32_refine"),
+            ("jacobi_fp64", "parallel_jacobi", "fp64")]
+    out, u_ref = {}, None
+    for name, scheme, prec in arms:
+        rp = W.make_rb_params(params, scheme=scheme, precision=prec, **kw)
+        rp.max_iterations = cap
+        times, u1 = [], None
+        for k in range(3):
+            if k == 0:
+                world.set_state(x0, u0)
+                world.t_cache_key.copy_(cache[0]); world.t_cache_sol.copy_(cache[1]); world.t_cache_count.copy_(cache[2])
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            world.step(rp)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+            st = world.stats()[0]
+            if k == 0:
+                u1 = world.state()[1]
+        if u_ref is None:
+            u_ref = u1
+        out[name] = {"ms_per_step": float(np.mean(times)), "contacts": int(st.n_contacts), "levels": int(st.n_levels),
+                     "sweeps": int(st.iterations + 1 if st.exitcode == 3 else cap), "met_tolerance": st.exitcode == 3,
+                     "residual": float(st.residual),
+                     "max_rel_velocity_error_vs_gs_fp64_step1": float(np.abs(u1 - u_ref).max() / np.abs(u_ref).max())}
+    return {"workload": "mixed_lattice_4096 (16^3 boxes / r 0.5 spheres, spacing 1.2, density 1000), SDF 64",
+            "state": "after a 30-step pre-roll; 3 steps per arm from the same state and warm-start cache",
+            "max_iterations": cap, "tolerance": args.tolerance, "arms": out}
+
+
+def config_c4(dev, steps=500, cap=100, tol=1e-6):
+    """32-high box tower, masses alternating 1 and 1000, mu 0.6, dt 0.005, `steps` steps in FP64, FP32 + FP64
+    refinement and FP32: complementarity residual per step and position drift against the FP64 run."""
+    import torch
+    from rainbow_b200 import engine_io, scenes, world as W
+    arrays = engine_io.scene_arrays(scenes.box_tower(32, device=dev))
+    params = W.params_from_vector(arrays["params"])
+    stream = torch.cuda.current_stream()
+    runs = {}
+    for mode in ("fp64", "fp32_refine", "fp32"):
+        w = W.DeviceWorld(arrays, device=dev, max_iterations=max(cap, 100))
+        rp = W.make_rb_params(params, precision=mode, termination="residual_fixed_r", residual_tolerance=tol,
+                              residual_interval=4, warm_start=True)
+        rp.max_iterations = cap
+        x_init, u_init = w.state()
+        w.step(rp)                        # sizes the work lists; the run starts from the initial state again
+        w.set_state(x_init, u_init)
+        w.reset_warm_start()
+        xs, res, ms, sw = [], [], [], []
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            w.step(rp)
+            e1.record(stream)
+            xs.append(w.state()[0][:, :3].copy())
+            s = w.stats()[0]
+            res.append(s.residual)
+            sw.append(s.fp32_sweeps)
+            ms.append(e0.elapsed_time(e1))
+        runs[mode] = (np.array(xs), np.array(res), np.array(ms), np.array(sw))
+    x64 = runs["fp64"][0]
+    every = max(1, steps // 20)
+    rep = {}
+    for mode, (xs, res, ms, sw) in runs.items():
+        drift = np.abs(xs - x64).max(axis=(1, 2))
+        rep[mode] = {"ms_per_step": float(ms[1:].mean()), "residual_median": float(np.median(res)),
+                     "residual_max": float(res.max()), "steps_meeting_tolerance": int((res <= tol).sum()),
+                     "fp32_sweeps_mean": float(sw[sw >= 0].mean()) if (sw >= 0).any() else 0.0,
+                     "drift_m_max_first_50_steps": float(drift[:50].max()), "drift_m_max": float(drift.max()),
+                     "per_step": [{"step": k + 1, "residual": float(res[k]), "drift_m": float(drift[k])}
+                                  for k in range(every - 1, steps, every)]}
+    return {"workload": "box_tower_32_mass_ratio_1e3", "bodies": 33, "dt": 0.005, "mu": 0.6, "steps": steps,
+            "termination": "residual_fixed_r", "tolerance": tol, "max_iterations": cap, "precision": rep}
+
+
+# --------------------------------------------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------------------------------------------
 def run_ours(args):
     import torch
     import torch.distributed as dist
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    # the CPU baseline pool must exist before the first CUDA call
-    cpu_pool_workers = os.cpu_count() or 1
+    cpu_pool_workers = os.cpu_count() or 1   # the CPU baseline's pool is spawned, never forked
     torch.cuda.set_device(local)
     dev = "cuda:%d" % local
     if world_size > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device(dev))
-    from rainbow_b200 import engine_io, world as W
-    from rainbow_b200.stepper import GpuStepper
+    from rainbow_b200 import world as W
     from rainbow_b200.sharding import max_over_ranks, partition_scenes, sum_over_ranks
     if world_size > 1 and args.workload == "batch1024":
         # weak scaling: world_size x --scenes scenes, split by body count so every GPU holds --scenes of them
-        arrays, params, cfg, engine = build_workload(args.workload, dev, args.scenes * world_size)
+        arrays, params, cfg, engine = build_workload(args.workload, dev, args.scenes * world_size, args.shapes)
         parts = partition_scenes([len(a["body_mass"]) for a in arrays], world_size)
         arrays = [arrays[i] for i in parts[rank]]
         cfg.update({"scenes_per_gpu": len(arrays), "scenes": args.scenes * world_size})
     else:
-        arrays, params, cfg, engine = build_workload(args.workload, dev, args.scenes)
-    max_it = int(params.max_iterations)
-    world = W.DeviceWorld(arrays, device=dev, max_iterations=max(max_it, LONG_SWEEPS))
+        arrays, params, cfg, engine = build_workload(args.workload, dev, args.scenes, args.shapes)
+    pre_cap = int(params.max_iterations)      # the configuration's own iteration limit (100)
+    cap = int(args.max_iterations)
+    world = W.DeviceWorld(arrays, device=dev, max_iterations=max(cap, pre_cap))
     kw = dict(scheme=args.scheme, termination=args.termination, residual_tolerance=args.tolerance,
               residual_interval=args.residual_interval if args.termination == "residual_fixed_r" else 1,
               ordering=args.ordering)
     warm = not args.no_warm_start
     prec = args.precision if args.termination == "residual_fixed_r" else "fp64"
-    rp = W.make_rb_params(params, warm_start=warm, precision=prec, **kw)
-    rp_prof = W.make_rb_params(params, profiling=True, warm_start=warm, precision=prec, **kw)
-    # the plain baseline: the same FP64 solver and settings, one scene per launch sequence (FP64 results are
-    # bit-identical alone and batched, tests/test_gpu_parity.py), stopping at the same residual tolerance
-    rp_plain = W.make_rb_params(params, warm_start=warm, precision="fp64", **kw)
-    rp64 = rp_plain
-    stream = torch.cuda.current_stream()
+
+    def mk(precision, it, profiling=False):
+        rp = W.make_rb_params(params, warm_start=warm, precision=precision, profiling=profiling, **kw)
+        rp.max_iterations = it
+        return rp
+    rp_pre = mk(prec, pre_cap)
     for _ in range(args.pre_roll):
-        world.step(rp)
-    # launch shapes tuned on this batch (speed only: results are the same bits for every shape)
+        world.step(rp_pre)
+    # launch shapes tuned on this batch at the 100-sweep limit (speed only: results are the same bits for every
+    # shape; the shapes mostly concern the collision kernels and the FP32 teams' slabs)
     tuning = None
     if not args.no_autotune and args.workload == "batch1024":
         from rainbow_b200 import autotune
         t0 = time.perf_counter()
-        best, info = autotune.tune(world, rp)
-        autotune.apply(rp, best)
-        autotune.apply(rp_prof, best)
+        best, info = autotune.tune(world, rp_pre)
         tuning = dict(best, seconds=time.perf_counter() - t0, **info)
+    rps = {"mode": mk(prec, cap), "fp64": mk("fp64", cap), "prof": mk(prec, cap, True),
+           "mode100": mk(prec, pre_cap), "fp64_100": mk("fp64", pre_cap)}
+    if tuning:
+        from rainbow_b200 import autotune
+        for rp in rps.values():
+            autotune.apply(rp, best)
     x0, u0 = world.state()                 # state the timed region (and every baseline) starts from
     cache = (world.t_cache_key.clone(), world.t_cache_sol.clone(), world.t_cache_count.clone())
 
@@ -412,125 +709,70 @@ def run_ours(args):
         world.set_state(x0, u0)
         world.t_cache_key.copy_(cache[0]); world.t_cache_sol.copy_(cache[1]); world.t_cache_count.copy_(cache[2])
 
-    world.step(rp_prof)                    # phase split and byte accounting (outside the timed region)
+    # the first step from the saved state in this precision mode (profiled: phase times, byte counts) and in
+    # FP64: every scene's convergence in both, and the mode's error against FP64
+    restore()
+    world.step(rps["prof"])
     phases = world.profile_times()
     stats = world.stats()
-    x_m, u_m = world.state()
-    # error of this precision mode against the FP64 step from the same state (the FP64 GPU step is
-    # bit-identical to the oracle)
+    u_m = world.state()[1]
     restore()
-    world.step(rp64)
-    x_64, u_64 = world.state()
+    world.step(rps["fp64"])
     stats64 = world.stats()
-    # the same step solved far past the iteration cap: the converged answer both are measured against
-    rp_long = W.make_rb_params(params, warm_start=warm, precision="fp64", **kw)
-    rp_long.max_iterations = LONG_SWEEPS
-    restore()
-    world.step(rp_long)
-    _, u_long = world.state()
-    stats_long = world.stats()
-    um, u6, ul = u_m.reshape(-1, 6), u_64.reshape(-1, 6), u_long.reshape(-1, 6)
-
-    def rel_err(a, b, scenes_):
-        out = []
-        for i in scenes_:
-            b0, b1 = world.scene_start[i], world.scene_start[i + 1]
-            out.append(np.abs(a[b0:b1] - b[b0:b1]).max() / max(1e-30, np.abs(b[b0:b1]).max()))
-        return np.array(out)
-
-    def pct(v):
-        return [float(np.percentile(v, 50)), float(np.percentile(v, 99)), float(v.max())] if len(v) else None
-
+    u_64 = world.state()[1]
+    um, u6 = u_m.reshape(-1, 6), u_64.reshape(-1, 6)
     active = [i for i in range(world.n_scenes) if stats64[i].n_contacts > 0]
-    conv_long = [i for i in active if stats_long[i].exitcode == 3]
-    err = {"per_scene_max_rel_velocity_error_p50_p99_max": {
-               "mode_vs_fp64_same_sweeps": pct(rel_err(um, u6, active)),
-               "mode_vs_fp64_converged": pct(rel_err(um, ul, conv_long)),
-               "fp64_vs_fp64_converged": pct(rel_err(u6, ul, conv_long))},
-           "converged_reference": "FP64, same step, up to %d sweeps; %d of %d scenes met the tolerance"
-                                  % (LONG_SWEEPS, len(conv_long), len(active)),
-           "fp64_converged_scenes": int(sum(1 for i in active if stats64[i].exitcode == 3)),
-           "mode_converged_scenes": int(sum(1 for i in active if stats[i].exitcode == 3)),
-           "fp32_sweeps_mean": float(np.mean([s_.fp32_sweeps for s_ in stats if s_.n_contacts > 0] or [0]))}
-    # sizing pass: the timed trajectory once with work-list growth, so no timed step can overflow
-    restore()
-    for _ in range(args.steps):
-        world.step(rp)
-    restore()
-    for _ in range(max(3, args.warmup)):
-        world.step(rp)
-    restore()
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    if world_size > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    world.t_status.zero_()
-    # the timed steps replay one CUDA graph of the whole step; its kernel count is taken while capturing
-    from rainbow_b200 import _native
-    lib = _native.load()
-    launches0 = lib.rb_launch_count()
-    graph = world.capture(rp)
-    per_replay = lib.rb_launch_count() - launches0
-    restore()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
-        times = timed_steps(graph.replay, args.steps, stream, flush)
-    launches = per_replay * args.steps
-    del graph
-    if world_size > 1:
-        dist.barrier()
-    status = int(world.t_status[0].item())
-    after = world.stats()
-    total_ms = max_over_ranks(float(times.sum()), dev)       # the slowest rank's device time
-    n_scenes = world.n_scenes
-    all_scenes = int(sum_over_ranks(n_scenes, dev))
-    value = all_scenes * args.steps / (total_ms / 1000.0)
-    residuals = np.array([s.residual for s in after if s.n_contacts > 0])
-    iters = np.array([s.iterations + 1 if s.exitcode == 3 else max_it for s in after if s.n_contacts > 0])
-    ncont = np.array([s.n_contacts for s in after])
-    levels = np.array([s.n_levels for s in after if s.n_contacts > 0])
-    # FP64 sweeps after the FP32 phase (scenes the FP32 phase handled)
-    refine = np.array([(s.iterations + 1 if s.exitcode == 3 else max_it) - s.fp32_sweeps
-                       for s in after if s.n_contacts > 0 and s.fp32_sweeps > 0])
-    unconverged = int(sum(1 for s in after if s.n_contacts > 0 and s.exitcode != 3)) \
-        if args.termination != "merit" else None
+    rel = []
+    for i in active:
+        b0, b1 = world.scene_start[i], world.scene_start[i + 1]
+        rel.append(np.abs(um[b0:b1] - u6[b0:b1]).max() / max(1e-30, np.abs(u6[b0:b1]).max()))
+    rel = np.array(rel)
+    both = [i for i in active if stats[i].exitcode == 3 and stats64[i].exitcode == 3]
+    rel_conv = np.array([rel[active.index(i)] for i in both])
+    pct = lambda v: [float(np.percentile(v, 50)), float(np.percentile(v, 99)), float(v.max())] if len(v) else None  # noqa: E731
+    equal = {"first_step_from_saved_state": {"mode": solve_summary(stats, cap), "fp64": solve_summary(stats64, cap)},
+             "mode_vs_fp64_per_scene_max_rel_velocity_error_p50_p99_max": pct(rel),
+             "same_on_scenes_both_met_tolerance": pct(rel_conv),
+             "fp32_sweeps_mean": float(np.mean([s.fp32_sweeps for s in stats if s.n_contacts > 0 and s.fp32_sweeps >= 0]
+                                               or [0]))}
 
-    # plain one-scene-per-launch FP64 baseline (same scheme, same tolerance, same starting states)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    times, launches, clocks, status, after = batched_arm(world, rps["mode"], args.steps, args.warmup, restore, flush,
+                                                        local, dist if world_size > 1 else None)
+    total_ms = max_over_ranks(float(times.sum()), dev)       # the slowest rank's device time
+    all_scenes = int(sum_over_ranks(world.n_scenes, dev))
+    value = all_scenes * args.steps / (total_ms / 1000.0)
+
+    sample = stratified_sample(np.diff(world.scene_start), args.plain_scenes) if world.n_scenes > 1 else []
     plain = None
-    if n_scenes > 1 and args.plain_scenes > 0 and rank == 0:
-        x0r, u0r = x0.reshape(-1, 7), u0.reshape(-1, 6)
-        pts, gts = [], []
-        for s in range(min(args.plain_scenes, n_scenes)):
-            b0, b1 = world.scene_start[s], world.scene_start[s + 1]
-            w1 = W.DeviceWorld(arrays[s], device=dev, max_iterations=max_it)
-            w1.set_state(x0r[b0:b1], u0r[b0:b1])
-            w1.step(rp_plain)              # sizes its work lists
-            w1.set_state(x0r[b0:b1], u0r[b0:b1])
-            torch.cuda.synchronize()
-            pts.append(timed_steps(lambda: w1.launch(rp_plain), args.steps, stream, flush))
-            g1 = w1.capture(rp_plain)      # the same scene-steps replayed from a CUDA graph
-            w1.set_state(x0r[b0:b1], u0r[b0:b1])
-            torch.cuda.synchronize()
-            gts.append(timed_steps(g1.replay, args.steps, stream, flush))
-            del g1
-        pt, gt = np.concatenate(pts), np.concatenate(gts)
-        plain = {"value": len(pt) / (pt.sum() / 1000.0), "unit": "scene-steps/s", "scenes_sampled": len(pts),
-                 "p50_ms": float(np.percentile(pt, 50)), "p99_ms": float(np.percentile(pt, 99)),
-                 "graph_value": len(gt) / (gt.sum() / 1000.0),
-                 "graph_p50_ms": float(np.percentile(gt, 50)), "graph_p99_ms": float(np.percentile(gt, 99)),
-                 "method": "each scene alone: one rb_step launch sequence per scene-step, FP64, same solver settings "
-                           "(bit-identical results to the batch); graph_* = the same steps replayed from a CUDA "
-                           "graph per scene"}
+    if sample and args.plain_scenes > 0 and rank == 0:
+        plain = plain_arm(world, arrays, sample, x0, u0, cache, rps["fp64"], args.plain_steps, flush, cap)
+
+    at100 = None
+    if not args.no_100 and world.n_scenes > 1 and rank == 0:
+        t100, _, c100, _, after100 = batched_arm(world, rps["mode100"], args.steps, args.warmup, restore, flush, local)
+        v100 = world.n_scenes * args.steps / (t100.sum() / 1000.0)
+        p100 = plain_arm(world, arrays, sample, x0, u0, cache, rps["fp64_100"], args.plain_steps, flush, pre_cap)
+        at100 = {"max_iterations": pre_cap, "value": v100, "unit": "scene-steps/s",
+                 "ms_per_step": float(t100.mean()), "p50_ms": float(np.percentile(t100, 50)),
+                 "p99_ms": float(np.percentile(t100, 99)), "solve_last_step": solve_summary(after100, pre_cap),
+                 "plain": p100, "speedup_vs_plain": v100 / p100["value"],
+                 "note": "the configuration's own 100-sweep limit: both arms stop at the same sweep count, most "
+                         "scenes before the 1e-6 tolerance"}
 
     # end to end through the public API, host buffers in and out every step
     e2e = None
     if not args.no_e2e:
         if engine is not None:
+            from rainbow_b200 import engine_io
+            from rainbow_b200.stepper import GpuStepper
             engine_io.write_back(engine, x0.reshape(-1, 7), u0.reshape(-1, 6))
             engine.stepper = GpuStepper(device=dev, termination=args.termination,
                                         residual_tolerance=args.tolerance)
             engine.params.proximal_solver = None if args.scheme == "rigid_gauss_seidel" else args.scheme
             engine.params.warm_start = warm
+            engine.params.solver_precision = prec
+            engine.params.max_iterations = cap
             engine.stepper.step(engine.params.time_step, engine, False)
             engine_io.write_back(engine, x0.reshape(-1, 7), u0.reshape(-1, 6))
             torch.cuda.synchronize()
@@ -541,11 +783,12 @@ def run_ours(args):
             el = time.perf_counter() - t0
             K = len(engine.contact_points)
             d2h = 13 * 8 * world.n_bodies + K * 64 + 8
+            api = "GpuStepper.step via engine"
         else:
             # the step as one CUDA graph replay; the state goes host -> device and back every step through the
             # pinned staging buffers, which the caller reads and passes back without host copies
             restore()
-            g_e2e = world.capture(rp)
+            g_e2e = world.capture(rps["mode"])
             restore()
             hx, hu = x0, u0
             torch.cuda.synchronize()
@@ -558,58 +801,68 @@ def run_ours(args):
             el = time.perf_counter() - t0
             del g_e2e
             d2h = 13 * 8 * world.n_bodies + st.numel()
+            api = "DeviceWorld set_state / graph replay / state(copy=False)"
         el = max_over_ranks(el, dev)
         e2e = {"value": all_scenes * args.steps / el, "unit": "scene-steps/s",
-               "h2d_bytes_per_step": 13 * 8 * world.n_bodies, "d2h_bytes_per_step": int(d2h),
-               "api": "GpuStepper.step via engine" if engine is not None
-               else "DeviceWorld set_state / graph replay / state(copy=False)"}
+               "h2d_bytes_per_step": 13 * 8 * world.n_bodies, "d2h_bytes_per_step": int(d2h), "api": api}
 
-    # roofline of the dominant phase from the profiled step (event times on the launching stream)
+    # rooflines of the profiled step's phases (event times on the launching stream)
     K = sum(s.n_contacts for s in stats)
-    sweeps = sum(s.n_contacts * ((s.iterations + 1) if 0 <= s.iterations < max_it else max_it) for s in stats)
-    sweeps32 = sum(s.n_contacts * min(max(s.fp32_sweeps, 0), max_it) for s in stats)   # of those, in FP32
+    sweeps = sum(s.n_contacts * ((s.iterations + 1) if 0 <= s.iterations < cap else cap) for s in stats)
+    sweeps32 = sum(s.n_contacts * min(max(s.fp32_sweeps, 0), cap) for s in stats)   # of those, in FP32
     sweeps64 = max(0, sweeps - sweeps32)
     cand = sum(s.n_candidates for s in stats)
     lookups = sum(s.n_grid_lookups for s in stats)
     npairs = sum(s.n_pairs for s in stats)
-    resid_passes = sweeps if args.termination == "residual" else 0
-    alg = {
-        "contact_search": (phases[2], cand * (72 + 64) + lookups * 64,
-                           "per candidate triangle: 3 world vertices (72 B) + result record (64 B); 8 grid values "
-                           "(64 B) per signed distance lookup, lookups counted on the device"),
-        "solve": (phases[4], sweeps64 * 137 * 8 + sweeps32 * 137 * 4 + resid_passes * 106 * 8,
-                  "per contact per sweep: J 48 + WJT 48 + b 4 + r 4 + mu 1 + x 8 + body w 24 values, 8 B each in "
-                  "FP64 sweeps (1096 B) and 4 B in FP32 sweeps (548 B); residual pass: J 48 + WJT 48 + b 4 + x 4 "
-                  "+ mu 1 + w 1 doubles"),
-        "pairs_and_candidates": (phases[1], npairs * 2 * 48 + cand * 8,
-                                 "per body pair: 2 boxes (96 B); per candidate 8 B"),
-    }
-    dom = max(alg, key=lambda k: alg[k][0])
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         peaks = {}
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    dt_s, nbytes, model = alg[dom]
-    # DRAM bytes of the solve phase's kernels per step, from the ncu capture summarised in
-    # profiles/k_solve_fp32_batch1024.md (the FP32 copies live in shared memory, so DRAM sees the copy-in and
-    # the FP64 test and refinement only)
-    traffic = PROFILED_SOLVE_DRAM_BYTES if (dom == "solve" and args.workload == "batch1024"
-                                             and prec != "fp64") else None
-    achieved = nbytes / dt_s / 1e9 if dt_s > 0 else 0.0
+    src = "of measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "of fallback 6650 GB/s"
+
+    def roof(name, dt_s, nbytes, model, kernel, bound_note):
+        achieved = nbytes / dt_s / 1e9 if dt_s > 0 else 0.0
+        prof = PROFILED_DRAM_BYTES.get(kernel)
+        traffic = prof[0] if prof and prof[1] == (cfg["workload"], prec, cap) else None
+        return {"bound": "hbm", "kernel_phase": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": int(nbytes), "bytes_model": model,
+                "phase_ms": dt_s * 1000.0, "peak_source": src, "note": bound_note}
+    solve_roof = roof("solve", phases[4], sweeps64 * 137 * 8 + sweeps32 * 137 * 4,
+                      "per contact per sweep: J 48 + WJT 48 + b 4 + r 4 + mu 1 + x 8 + body w 24 values, 8 B each in "
+                      "FP64 sweeps (1096 B) and 4 B in FP32 sweeps (548 B)", "k_solve_fp32",
+                      "latency-bound: each scene is one chain of (levels x sweeps) dependent contact updates whose "
+                      "rows sit in shared memory (FP32) or L2 (FP64); neither HBM nor the SMs are near their limit")
+    narrow_roof = roof("contact_search", phases[2], cand * (72 + 64) + lookups * 64,
+                       "per candidate triangle: 3 world vertices (72 B) + result record (64 B); 8 grid values (64 B) "
+                       "per signed distance lookup, lookups counted on the device", "k_narrow",
+                       "gathers of 8 grid nodes per lookup; with the shape pool the grids are L2-resident")
+    doms = {"solve": solve_roof, "contact_search": narrow_roof}
+    dom = max(doms, key=lambda k: doms[k]["phase_ms"])
 
     serving_rep = None
     if args.serve_seconds > 0 and args.workload == "batch1024" and world_size == 1:
-        serving_rep = run_serving(args, dev, dict(warm_start=warm, precision=prec, **kw), max_it)
+        serving_rep = run_serving(args, dev, dict(warm_start=warm, precision=prec, **kw), cap, flush,
+                                  tuning=best if tuning else None)
+
+    configs = None
+    if not args.no_configs and args.workload == "batch1024" and world_size == 1:
+        configs = {"C1": config_c1(dev, cpu=args.cpu_seconds > 0), "C2": config_c2(dev, args, flush),
+                   "C4": config_c4(dev, steps=500, cap=cap, tol=args.tolerance)}
 
     cpu = None
     if rank == 0 and args.cpu_seconds > 0:
-        cv, info = cpu_baseline(arrays, args, cpu_pool_workers if n_scenes > 1 else 1)
+        x0r, u0r = x0.reshape(-1, 7), u0.reshape(-1, 6)
+        states = {i: (x0r[world.scene_start[i]:world.scene_start[i + 1]], u0r[world.scene_start[i]:world.scene_start[i + 1]])
+                  for i in range(world.n_scenes)}
+        cv, info = cpu_baseline(arrays, args, cpu_pool_workers if world.n_scenes > 1 else 1, states=states,
+                                pre_cap=pre_cap)
         cpu = dict(value=cv, unit="scene-steps/s", **info)
 
     cfg.update({"scheme": args.scheme, "ordering": args.ordering, "termination": args.termination,
-                "tolerance": args.tolerance,
-                "precision": prec, "warm_start": warm, "residual_interval": kw["residual_interval"], "pre_roll_steps": args.pre_roll, "contacts_per_step": int(K),
+                "tolerance": args.tolerance, "max_iterations": cap,
+                "precision": prec, "warm_start": warm, "residual_interval": kw["residual_interval"],
+                "pre_roll_steps": args.pre_roll, "pre_roll_max_iterations": pre_cap, "contacts_per_step": int(K),
                 "sweeps_per_step_contacts": int(sweeps), "l2": "256 MB buffer written between timed steps",
                 "launch": "each timed step replays one CUDA graph of the whole rb_step",
                 "launch_shapes": tuning,
@@ -620,33 +873,26 @@ def run_ours(args):
         "metric": "scene-steps/s", "value": value, "unit": "scene-steps/s", "n_gpus": world_size,
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,
         "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if prec != "fp64" else "f64", "data": "synthetic",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if prec != "fp64" else "f64", "data": "synthetic",
         "config": cfg,
         "plain": plain,
-        "error_vs_fp64": err,
         "speedup_vs_plain": (value / world_size) / plain["value"] if plain else None,
-        "residual": {"max": float(residuals.max()) if len(residuals) else 0.0,
-                     "median": float(np.median(residuals)) if len(residuals) else 0.0,
-                     "unconverged_scenes": unconverged,
-                     "sweeps_p50_p90_max": [float(np.percentile(iters, 50)), float(np.percentile(iters, 90)),
-                                            int(iters.max())] if len(iters) else None,
-                     "contacts_per_scene_p50_max": [float(np.percentile(ncont, 50)), int(ncont.max())],
-                     "levels_per_scene_p50_max": [float(np.percentile(levels, 50)), int(levels.max())]
-                     if len(levels) else None,
-                     "fp64_refine_sweeps_p50_p99_max": [float(np.percentile(refine, 50)),
-                                                        float(np.percentile(refine, 99)), int(refine.max())]
-                     if len(refine) else None},
-        "roofline": {"bound": "hbm", "kernel_phase": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": int(nbytes),
-                     "bytes_model": model, "phase_ms": dt_s * 1000.0,
-                     "peak_source": "of measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "of fallback 6650 GB/s"},
+        "served_vs_plain": serving_rep.get("served_vs_plain") if serving_rep else None,
+        "residual": dict(solve_summary(after, cap) or {}, tolerance=args.tolerance, max_iterations=cap,
+                         unconverged_scenes=(solve_summary(after, cap) or {}).get("unconverged"),
+                         note="last timed step; every arm runs the same solver with the same tolerance and cap"),
+        "equal_residual": equal,
+        "at_100_sweeps": at100,
+        "roofline": doms[dom], "roofline_phases": doms,
         "phases_ms": {k: v * 1000.0 for k, v in zip(["bodies_bvh", "pairs_candidates", "contact_search", "dedup",
                                                      "contact_setup_solve", "integrate", "total"], phases)},
         "serving": serving_rep,
+        "configs": configs,
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": int(launches),
-        "clocks": clocks.summary(),
+        "clocks": clocks,
         "status": status,
     }
     if rank == 0:
@@ -656,50 +902,21 @@ def run_ours(args):
 
 
 def run_tower(args):
-    """32-high box tower, masses alternating 1 and 1000, mu 0.6, dt 0.005, --steps steps (500 by the
-    configuration) in each precision; residual and position drift against the FP64 run per step."""
     import torch
-    from rainbow_b200 import engine_io, scenes, world as W
-    arrays = engine_io.scene_arrays(scenes.box_tower(32, device="cuda:0"))
-    params = W.params_from_vector(arrays["params"])
-    out = {}
-    for mode in ("fp64", "fp32_refine", "fp32"):
-        w = W.DeviceWorld(arrays, max_iterations=100)
-        rp = W.make_rb_params(params, precision=mode, termination="residual_fixed_r", residual_tolerance=1e-6,
-                              residual_interval=4, warm_start=True)
-        xs, res, ms = [], [], []
-        stream = torch.cuda.current_stream()
-        for _ in range(args.steps):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            w.step(rp)
-            e1.record(stream)
-            xs.append(w.state()[0][:, :3].copy())
-            res.append(w.stats()[0].residual)
-            ms.append(e0.elapsed_time(e1))
-        out[mode] = (np.array(xs), np.array(res), np.array(ms))
-    x64 = out["fp64"][0]
-    every = max(1, args.steps // 20)
-    report = {}
-    for mode, (xs, res, ms) in out.items():
-        drift = np.abs(xs - x64).max(axis=(1, 2))
-        report[mode] = {"ms_per_step": float(ms.mean()), "residual_median": float(np.median(res)),
-                        "residual_max": float(res.max()),
-                        "per_step": [{"step": k + 1, "residual": float(res[k]), "drift_m": float(drift[k])}
-                                     for k in range(every - 1, args.steps, every)]}
-    line = {"metric": "scene-steps/s", "value": 1000.0 / report["fp32_refine"]["ms_per_step"],
-            "unit": "scene-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": 0,
-            "ms_per_step": report["fp32_refine"]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+    torch.cuda.set_device(0)
+    c4 = config_c4("cuda:0", steps=args.steps if args.steps > 20 else 500, cap=args.max_iterations,
+                   tol=args.tolerance)
+    ms = c4["precision"]["fp32_refine"]["ms_per_step"]
+    line = {"metric": "scene-steps/s", "value": 1000.0 / ms, "unit": "scene-steps/s", "n_gpus": 1,
+            "steps": c4["steps"], "warmup": 1, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": "box_tower_32_mass_ratio_1e3", "bodies": 33, "dt": 0.005, "mu": 0.6,
-                       "termination": "residual_fixed_r", "tolerance": 1e-6, "max_iterations": 100},
-            "precision": report}
+            "config": {k: v for k, v in c4.items() if k != "precision"}, "precision": c4["precision"]}
     print(json.dumps(line), flush=True)
 
 
 def main():
     args = parse()
-    if args.workload == "tower32":
+    if args.workload == "tower32" and args.impl == "ours":
         if int(os.environ.get("RANK", "0")) == 0:
             run_tower(args)
         return

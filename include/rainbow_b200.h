@@ -272,9 +272,13 @@ int64_t rb_launch_count(void);
    that this library keeps in device global memory, RB_NOALLOC_SCRATCH_BYTES (16 MiB) on every device that
    loads the library, held until the process exits.  Batches whose rb_workspace_bytes() exceeds that size are
    rejected with RB_ERR_WORKSPACE.  The first call on a device looks up the array's device address (with that
-   device current); make that first call before any stream capture.  All calls share the one array: calls
-   that may overlap on the GPU (different streams, or different host threads) race and must be serialised by
-   the caller.  This entry point calls no allocator.  It has no counterpart in the reference. */
+   device current) and, like the first rb_step on that device, grants the solver kernels their shared memory;
+   the first FP32-precision step on each host thread and device also creates that thread's side streams and
+   events.  Make those first calls during warm-up, outside any stream capture.  The address is kept for the
+   life of the process: after a cudaDeviceReset the array may move, so do not use this entry point across a
+   device reset.  All calls share the one array: calls that may overlap on the GPU (different streams, or
+   different host threads) race and must be serialised by the caller.  This entry point calls no allocator.
+   It has no counterpart in the reference. */
 #define RB_NOALLOC_SCRATCH_BYTES (16u << 20)
 int rb_step_noalloc(const rb_shapes* shapes, const rb_bodies* bodies, const rb_caps* caps, const rb_params* params,
                     const rb_outputs* out, void* stream);
@@ -312,6 +316,15 @@ int rb_repack(const int32_t* body_map, int32_t n_old_bodies, const double* x_old
    Unsigned distance by closest point on each triangle, sign by the generalized winding number. */
 int rb_signed_distance_grid(const double* V, int32_t n_vertices, const int32_t* T, int32_t n_triangles,
                             const double* grid_meta, double* values, void* stream);
+
+/* The grids of many shapes in one launch (grid3.py:320 create_signed_distance once per shape, for batches that
+   give every body a shape of its own).  Shape s: vertices V[3 v_off[s] ..], triangles T[3 t_off[s] ..] with
+   shape-local vertex indices, grid_meta[12 s ..] as above, values[g_off[s] ..].  block_off (n_shapes + 1) holds
+   the prefix sums of ceil(I J K / 128) over the shapes, block_off[0] = 0, and total_blocks = block_off[n_shapes].
+   Every pointer is a device pointer; the values equal rb_signed_distance_grid's, shape by shape.  Asynchronous. */
+int rb_signed_distance_grids(int32_t n_shapes, const double* V, const int32_t* v_off, const int32_t* T,
+                             const int32_t* t_off, const double* grid_meta, const int64_t* g_off,
+                             const int64_t* block_off, int64_t total_blocks, double* values, void* stream);
 
 #ifdef __cplusplus
 }

@@ -98,6 +98,7 @@ SIGNATURES = {
     "rb_step": (ctypes.c_int, [ctypes.POINTER(RbShapes), ctypes.POINTER(RbBodies), ctypes.POINTER(RbCaps),
                                ctypes.POINTER(RbParams), ctypes.POINTER(RbOutputs), _vp, ctypes.c_size_t, _vp]),
     "rb_signed_distance_grid": (ctypes.c_int, [_vp, _i32, _vp, _i32, _vp, _vp, _vp]),
+    "rb_signed_distance_grids": (ctypes.c_int, [_i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int64, _vp, _vp]),
     "rb_profile_times": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), _i32]),
     "rb_launch_count": (ctypes.c_int64, []),
     "rb_build_topology": (ctypes.c_int, [ctypes.POINTER(RbShapes), ctypes.POINTER(RbBodies), _vp, _sz, _vp]),

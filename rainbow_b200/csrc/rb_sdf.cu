@@ -52,13 +52,15 @@ __device__ d3 closest_point(d3 p, d3 a, d3 b, d3 c) {
 }
 
 constexpr int kTile = 128;
+constexpr int kSdfBlock = 128;
 
-__global__ void k_sdf(const double* __restrict__ V, const int32_t* __restrict__ T, int n_tri,
-                      const double* __restrict__ meta, double* __restrict__ values) {
+// distance and sign of node `node` of a grid (meta: min[3], max[3], spacing[3], I, J, K) around the mesh
+// (V, T with n_tri triangles); every thread of the block calls it (the triangle tiles go through shared memory)
+__device__ __forceinline__ void sdf_node(const double* __restrict__ V, const int32_t* __restrict__ T, int n_tri,
+                                         const double* __restrict__ meta, int64_t node, double* __restrict__ values) {
     __shared__ double tri[kTile][9];
     const int I = (int)meta[9], J = (int)meta[10], K = (int)meta[11];
     const int64_t n_nodes = (int64_t)I * J * K;
-    const int64_t node = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     d3 p = d3{0.0, 0.0, 0.0};
     if (node < n_nodes) {
         const int i = (int)(node % I), j = (int)((node / I) % J), k = (int)(node / ((int64_t)I * J));
@@ -91,6 +93,33 @@ __global__ void k_sdf(const double* __restrict__ V, const int32_t* __restrict__ 
     if (node < n_nodes) values[node] = (fabs(wind) / (4.0 * M_PI) > 0.5) ? -best : best;
 }
 
+__global__ void __launch_bounds__(kSdfBlock) k_sdf(const double* __restrict__ V, const int32_t* __restrict__ T,
+                                                   int n_tri, const double* __restrict__ meta,
+                                                   double* __restrict__ values) {
+    sdf_node(V, T, n_tri, meta, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, values);
+}
+
+// many grids in one launch: block b belongs to the shape s with block_off[s] <= b < block_off[s + 1]
+__global__ void __launch_bounds__(kSdfBlock) k_sdf_many(int n_shapes, const double* __restrict__ V,
+                                                        const int32_t* __restrict__ v_off,
+                                                        const int32_t* __restrict__ T,
+                                                        const int32_t* __restrict__ t_off,
+                                                        const double* __restrict__ meta,
+                                                        const int64_t* __restrict__ g_off,
+                                                        const int64_t* __restrict__ block_off,
+                                                        double* __restrict__ values) {
+    const int64_t b = blockIdx.x;
+    int lo = 0, hi = n_shapes;   // the last s with block_off[s] <= b
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (block_off[mid] <= b) lo = mid; else hi = mid;
+    }
+    const int s = lo;
+    const int64_t node = (b - block_off[s]) * kSdfBlock + threadIdx.x;
+    sdf_node(V + 3 * (size_t)v_off[s], T + 3 * (size_t)t_off[s], t_off[s + 1] - t_off[s], meta + 12 * (size_t)s,
+             node, values + g_off[s]);
+}
+
 }  // namespace
 
 extern "C" int rb_signed_distance_grid(const double* V, int32_t n_vertices, const int32_t* T, int32_t n_triangles,
@@ -112,13 +141,33 @@ extern "C" int rb_signed_distance_grid(const double* V, int32_t n_vertices, cons
         rb::g_error = "rb_signed_distance_grid: grid size out of range";
         return RB_ERR_ARG;
     }
-    const int block = 128;
+    const int block = kSdfBlock;
     k_sdf<<<(unsigned)((n_nodes + block - 1) / block), block, 0, (cudaStream_t)stream>>>(V, T, n_triangles,
                                                                                       grid_meta_dev, values);
     rb::note_launch();
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         rb::g_error = std::string("rb_signed_distance_grid: ") + cudaGetErrorString(e);
+        return RB_ERR_CUDA;
+    }
+    return RB_OK;
+}
+
+extern "C" int rb_signed_distance_grids(int32_t n_shapes, const double* V, const int32_t* v_off, const int32_t* T,
+                                        const int32_t* t_off, const double* grid_meta, const int64_t* g_off,
+                                        const int64_t* block_off, int64_t total_blocks, double* values,
+                                        void* stream) {
+    if (n_shapes <= 0 || !V || !v_off || !T || !t_off || !grid_meta || !g_off || !block_off || !values ||
+        total_blocks <= 0 || total_blocks > INT32_MAX) {
+        rb::g_error = "rb_signed_distance_grids: bad argument";
+        return RB_ERR_ARG;
+    }
+    k_sdf_many<<<(unsigned)total_blocks, kSdfBlock, 0, (cudaStream_t)stream>>>(n_shapes, V, v_off, T, t_off,
+                                                                             grid_meta, g_off, block_off, values);
+    rb::note_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        rb::g_error = std::string("rb_signed_distance_grids: ") + cudaGetErrorString(e);
         return RB_ERR_CUDA;
     }
     return RB_OK;

@@ -1720,9 +1720,14 @@ constexpr int kFp32L2Block = 512;                    // threads of the launch fo
 constexpr int kFp32LargeSmem = 224 * 1024;           // slab of a block team (one scene per SM)
 constexpr int kS32SmallSlab = 28 * 1024;             // slab of a warp team, small class (8 scenes per SM)
 constexpr int kS32MidSlab = 56 * 1024;               // slab of a warp team, mid class (4 scenes per SM)
-// relative residual below which a stalled FP32 iteration is taken to have met FP32 rounding
+// relative residual below which a stalled FP32 iteration may have met FP32 rounding
 constexpr float kFp32Floor = 1e-5f;
-constexpr int kS32Corrections = 3;   // FP64 defect corrections of one scene's FP32 problem per step
+// residual tests without a 5 % improvement after which an FP32 round ends in a defect correction (with the
+// test every 4 sweeps: 64 sweeps; Gauss-Seidel often progresses by less than 5 % in 12 sweeps near 1e-6)
+constexpr int kS32StallTests = 16;
+// a correction round that lowers the FP64 residual by less than this factor, below kFp32Floor, hands the
+// scene to FP64 sweeps: the FP32 iteration cannot take it further
+constexpr double kS32RoundGain = 0.9;
 
 struct S32Scene {
     float* c;          // kS32Floats per contact, in level order; row q at 12 q as three float4 groups
@@ -2165,7 +2170,10 @@ __global__ void __launch_bounds__(kL2 ? kFp32L2Block : kFp32BlockMax, 1) k_solve
     char* my_slab = f32_smem + (size_t)team * slab;
     const int max_it = a.pr.max_iterations;
     const int interval = a.pr.residual_interval > 1 ? a.pr.residual_interval : 1;
-    const float tol = (float)a.pr.residual_tolerance;
+    // the FP32 sweeps aim a little below the tolerance when an FP64 test follows, so that the FP32 problem
+    // rarely meets it while the FP64 one misses it
+    const float tol = (float)(a.pr.precision == RB_PRECISION_FP32_REFINE ? 0.5 * a.pr.residual_tolerance
+                                                                        : a.pr.residual_tolerance);
     // sweeps reserved for the FP64 refinement
     const int reserve = a.pr.precision == RB_PRECISION_FP32_REFINE ? min(max(a.pr.refine_iterations, 0), max_it) : 0;
     const int budget = max_it - reserve;
@@ -2206,27 +2214,32 @@ __global__ void __launch_bounds__(kL2 ? kFp32L2Block : kFp32BlockMax, 1) k_solve
         if (g.rank() == 0) a.ws.nlev[s] = L;
         float res = s32_residual(a, g, R, f);   // the warm-started iterate may already be good enough
         float best = res;
-        int sweeps = 0, stalls = 0, corrections = 0;
-        double r64 = -1.0;   // FP64 residual of the current iterate, once evaluated
+        int sweeps = 0, stalls = 0;
+        double r64 = -1.0;            // FP64 residual of the current iterate, once evaluated
+        double r64_round = INFINITY;  // FP64 residual after the previous correction round
         for (;;) {
+            const int round_start = sweeps;
             while (res > tol && sweeps < budget) {
                 s32_sweep<G, kL2>(g, f, L, rscale, bodies_global);
                 ++sweeps;
                 if (sweeps % interval == 0 || sweeps == budget) {
                     res = s32_residual(a, g, R, f);
-                    // FP32 floor: hand over once the residual, already small, stops improving.  Above the
+                    // a round ends once the residual, already small, stops improving for a while (the FP32
+                    // problem's own rounding, or slow progress a defect correction may speed up).  Above the
                     // floor a pause is the Gauss-Seidel iteration itself (it is not monotone), so go on.
                     if (res < 0.95f * best) { best = res; stalls = 0; }
-                    else if (best < kFp32Floor && ++stalls >= 3) break;
+                    else if (best < kFp32Floor && ++stalls >= kS32StallTests) break;
                 }
             }
             // FP32 + refinement: test in FP64; if the FP32 answer misses the tolerance in FP64, correct the FP32
-            // problem's b by the FP64 defect and sweep on in FP32 (a few times at most)
-            if (a.pr.precision != RB_PRECISION_FP32_REFINE || sweeps >= budget || corrections >= kS32Corrections)
-                break;
+            // problem's b by the FP64 defect and sweep on in FP32.  FP64 sweeps take over only when a round no
+            // longer lowers the FP64 residual while it is below the FP32 floor.
+            if (a.pr.precision != RB_PRECISION_FP32_REFINE || sweeps >= budget) break;
             r64 = s32_correct(a, g, R, f);
-            ++corrections;
             if (r64 <= a.pr.residual_tolerance) break;
+            if (sweeps == round_start) break;   // the FP32 problem meets the tolerance, the FP64 one does not
+            if (r64 < (double)kFp32Floor && r64 > kS32RoundGain * r64_round) break;   // r64 stays valid for x
+            r64_round = fmin(r64_round, r64);
             r64 = -1.0;   // the sweeps that follow change the iterate
             res = s32_residual(a, g, R, f);
             best = res;

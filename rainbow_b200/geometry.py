@@ -313,3 +313,34 @@ def create_signed_distance(V, T, I, J, K, boundary=0.5, device="cuda"):
                                         ctypes.c_void_p(st.cuda_stream)), "rb_signed_distance_grid")
     grid.values = out.cpu().numpy()
     return grid
+
+
+def signed_distance_grids(V_list, T_list, metas, device="cuda"):
+    """Signed distance grids of many meshes in one launch (rb_signed_distance_grids): mesh i has body-frame
+    vertices V_list[i], triangles T_list[i] and grid meta metas[i] (min[3], max[3], spacing[3], I, J, K).
+    Returns (values, g_off): one float64 device tensor holding every grid, grid i at g_off[i] .. g_off[i + 1]."""
+    import torch
+    from . import _native as N
+    dev = torch.device(device)
+    n = len(V_list)
+    nv = np.array([len(v) for v in V_list], np.int64)
+    nt = np.array([len(t) for t in T_list], np.int64)
+    metas = np.asarray(metas, np.float64).reshape(n, 12)
+    nodes = (metas[:, 9] * metas[:, 10] * metas[:, 11]).astype(np.int64)
+    g_off = np.concatenate([[0], np.cumsum(nodes)]).astype(np.int64)
+    blocks = (nodes + 127) // 128
+    block_off = np.concatenate([[0], np.cumsum(blocks)]).astype(np.int64)
+    tV = torch.from_numpy(np.ascontiguousarray(np.concatenate(V_list), np.float64).reshape(-1)).to(dev)
+    tT = torch.from_numpy(np.ascontiguousarray(np.concatenate(T_list), np.int32).reshape(-1)).to(dev)
+    tvo = torch.from_numpy(np.concatenate([[0], np.cumsum(nv)]).astype(np.int32)).to(dev)
+    tto = torch.from_numpy(np.concatenate([[0], np.cumsum(nt)]).astype(np.int32)).to(dev)
+    tM = torch.from_numpy(np.ascontiguousarray(metas).reshape(-1)).to(dev)
+    tg = torch.from_numpy(g_off).to(dev)
+    tb = torch.from_numpy(block_off).to(dev)
+    out = torch.empty(int(g_off[-1]), dtype=torch.float64, device=dev)
+    st = torch.cuda.current_stream(dev)
+    N.check(N.load().rb_signed_distance_grids(n, tV.data_ptr(), tvo.data_ptr(), tT.data_ptr(), tto.data_ptr(),
+                                              tM.data_ptr(), tg.data_ptr(), tb.data_ptr(), int(block_off[-1]),
+                                              out.data_ptr(), ctypes.c_void_p(st.cuda_stream)),
+            "rb_signed_distance_grids")
+    return out, g_off

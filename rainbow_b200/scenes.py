@@ -177,9 +177,12 @@ def batch_arrays(n_scenes=1024, seed=0, pool=64, body_range=(8, 256), resolution
     and spheres (radius U(0.25, 1), 16 x 16 sweep) with uniformly random orientations, density 1000, dropped
     onto a fixed ground box (ground x 1 x ground); friction mu U(0.2, 0.8) per scene; dt 0.01.
 
-    Shape sizes are drawn from a pool of ``pool`` boxes and ``pool`` spheres shared by all scenes, so the
-    signed distance grids are built once per pool entry.  Returns the list of per-scene arrays (sharing the
-    pool's shape arrays by ``shape_key``) and the Parameters mapping used."""
+    With ``pool`` set, shape sizes are drawn from a pool of ``pool`` boxes and ``pool`` spheres shared by all
+    scenes, so the signed distance grids are built once per pool entry; with ``pool=None`` every body gets a
+    shape and a grid of its own (:func:`batch_arrays_per_body`).  Returns the list of per-scene arrays
+    (sharing the pool's shape arrays by ``shape_key``) and the Parameters mapping used."""
+    if pool is None:
+        return batch_arrays_per_body(n_scenes, seed, body_range, resolution, device, ground)
     from . import geometry as GEO
     from .types import Parameters
     rng = np.random.default_rng(seed)
@@ -244,4 +247,94 @@ def batch_arrays(n_scenes=1024, seed=0, pool=64, body_range=(8, 256), resolution
             "material_mu": np.full((1, 1, 3), mu), "material_epsilon": np.zeros((1, 1)), "params": pvec,
         })
         out.append(scene)
+    return out, params
+
+
+def batch_arrays_per_body(n_scenes=1024, seed=0, body_range=(8, 256), resolution=32, device="cuda", ground=24.0):
+    """The batched workload with a shape and signed distance grid of its own for every body: body counts,
+    kinds (box or sphere), sizes (box side U(0.5, 2), sphere radius U(0.25, 1)), orientations and friction
+    drawn per scene from ``seed``.  A body's shape is the unit box (side 1) or unit sphere (radius 1, 16 x 16
+    sweep), taken through the reference's set-up chain once, scaled by the body's size (body-frame vertices
+    and centre of mass by s, mass by s^3, inertia by s^5); its grid (grid3.py:320: bounding box grown by
+    max(0.1 x longest side, 2 x envelope), ``resolution`` nodes per axis) is computed on the device from its
+    own mesh.  All grids live in one device tensor; each scene's ``shape_grid`` is a view of it (its ground's
+    grid first, then its bodies' in body order), so nothing of the ~18.8 GB (73k grids of 32^3 doubles) passes
+    through host memory."""
+    from . import geometry as GEO
+    from .types import Grid, Parameters
+    from .world import PARAM_FIELDS
+    rng = np.random.default_rng(seed)
+    params = Parameters()
+    params.resolution = resolution
+    params.max_iterations = 100
+    params.relative_tolerance = 1e-6
+    env = float(params.envelope)
+    unit = [_shape_arrays(*GEO.create_box(1.0, 1.0, 1.0), resolution, env, device),
+            _shape_arrays(*GEO.create_sphere(1.0, 16, 16), resolution, env, device)]
+    g = _shape_arrays(*GEO.create_box(ground, 1.0, ground), resolution, env, device)
+    unit_len = [float((u["V"].max(axis=0) - u["V"].min(axis=0)).max()) for u in unit]
+    pvec = np.array([float(getattr(params, f)) for f in PARAM_FIELDS])
+    lo, hi = np.log(body_range[0]), np.log(body_range[1])
+    V_list, T_list, metas, plans = [], [], [], []
+    for si in range(n_scenes):
+        n = int(round(np.exp(rng.uniform(lo, hi))))
+        kinds = rng.integers(0, 2, n)
+        sizes = np.where(kinds == 0, rng.uniform(0.5, 2.0, n), rng.uniform(0.25, 1.0, n))
+        quats = rng.normal(size=(n, 4))
+        quats /= np.linalg.norm(quats, axis=1, keepdims=True)
+        mu = rng.uniform(0.2, 0.8)
+        V_list.append(g["V"]); T_list.append(g["T"]); metas.append(g["meta"])
+        for b in range(n):
+            u, sz = unit[kinds[b]], float(sizes[b])
+            Vb = u["V"] * sz
+            boundary = max(0.1 * unit_len[kinds[b]] * sz, 2.0 * env)
+            V_list.append(Vb)
+            T_list.append(u["T"])
+            metas.append(Grid(Vb.min(axis=0) - boundary, Vb.max(axis=0) + boundary, resolution, resolution,
+                              resolution).meta())
+        plans.append((n, kinds, sizes, quats, mu))
+    values, g_off = GEO.signed_distance_grids(V_list, T_list, metas, device=device)
+    out = []
+    shape0 = 0
+    for si, (n, kinds, sizes, quats, mu) in enumerate(plans):
+        sh = slice(shape0, shape0 + n + 1)
+        Vs, Ts = V_list[sh], T_list[sh]
+        side = int(np.ceil(n ** (1.0 / 3.0)))
+        spacing = 2.3
+        off = -0.5 * (side - 1) * spacing
+        pos = np.zeros((n + 1, 3))
+        quat = np.zeros((n + 1, 4))
+        quat[0] = GEO.quat_prod(np.array([1.0, 0.0, 0.0, 0.0]), g["q"])
+        pos[0] = GEO.quat_rotate(np.array([1.0, 0.0, 0.0, 0.0]), g["r"]) + np.array([0.0, -0.5, 0.0])
+        mass = np.zeros(n + 1)
+        inertia = np.zeros((n + 1, 3))
+        mass[0], inertia[0] = g["mass"] * 1000.0, g["inertia"] * 1000.0
+        for b in range(n):
+            i, j, l = b % side, (b // side) % side, b // (side * side)
+            u, sz = unit[kinds[b]], float(sizes[b])
+            quat[b + 1] = GEO.quat_prod(quats[b], u["q"])
+            pos[b + 1] = GEO.quat_rotate(quats[b], u["r"] * sz) + np.array([off + i * spacing, 1.2 + j * spacing,
+                                                                         off + l * spacing])
+            mass[b + 1] = u["mass"] * sz ** 3 * 1000.0
+            inertia[b + 1] = u["inertia"] * sz ** 5 * 1000.0
+        fixed = np.zeros(n + 1, np.uint8)
+        fixed[0] = 1
+        g0, g1 = int(g_off[shape0]), int(g_off[shape0 + n + 1])
+        out.append({
+            "shape_V": np.concatenate(Vs), "shape_T": np.concatenate(Ts),
+            "shape_grid": values[g0:g1],
+            "shape_v_off": np.concatenate([[0], np.cumsum([len(v) for v in Vs])]).astype(np.int64),
+            "shape_t_off": np.concatenate([[0], np.cumsum([len(t) for t in Ts])]).astype(np.int64),
+            "shape_g_off": (g_off[shape0:shape0 + n + 2] - g_off[shape0]).astype(np.int64),
+            "shape_grid_meta": np.array(metas[sh]),
+            "shape_key": np.array(["perbody%d:%d:%g:ground" % (seed, resolution, ground)] +
+                                  ["perbody%d:%d:%d:%d" % (seed, resolution, si, b) for b in range(n)]),
+            "body_shape": np.arange(n + 1, dtype=np.int32), "body_r": pos, "body_q": quat,
+            "body_v": np.zeros((n + 1, 3)), "body_w": np.zeros((n + 1, 3)), "body_mass": mass,
+            "body_inertia": inertia, "body_fixed": fixed, "body_material": np.zeros(n + 1, np.int32),
+            "body_force_order": np.concatenate([[[-1]], np.zeros((n, 1), np.int32)]).astype(np.int32),
+            "force_kind": np.array([0], np.int32), "force_params": np.array([[9.81, 0.0, 1.0, 0.0]]),
+            "material_mu": np.full((1, 1, 3), mu), "material_epsilon": np.zeros((1, 1)), "params": pvec,
+        })
+        shape0 += n + 1
     return out, params

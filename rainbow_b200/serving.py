@@ -318,7 +318,7 @@ class ServingBatch(W.DeviceWorld):
 
 class Request:
     __slots__ = ("uid", "scene", "horizon", "arrival", "block", "admitted", "done", "tick_walls", "tick_device",
-                 "result", "slot")
+                 "result", "slot", "error")
 
     def __init__(self, uid, scene, horizon, arrival):
         self.uid, self.scene, self.horizon, self.arrival = uid, scene, int(horizon), arrival
@@ -328,6 +328,7 @@ class Request:
         self.tick_walls = []
         self.tick_device = []
         self.result = None
+        self.error = None   # why the request was rejected (it then never runs)
 
 
 class Server:
@@ -355,6 +356,7 @@ class Server:
         self.active = []
         self.batch = None
         self.finished = []
+        self.rejected = []         # requests whose scene cannot run here, with Request.error set
         self.ticks = []
         self._uid = 0
         self._dirty = False
@@ -404,7 +406,13 @@ class Server:
         while self.queue:
             r = self.queue[0]
             if r.block is None:
-                r.block = SceneBlock(r.scene, lib)
+                try:
+                    r.block = SceneBlock(r.scene, lib)
+                except ValueError as e:   # e.g. a shape beyond the triangle limit: reject it, serve the rest
+                    self.queue.popleft()
+                    r.error = str(e)
+                    self.rejected.append(r)
+                    continue
                 lib.sync()
             b = r.block
             cnt = (int(lib.nv_arr[b.shape].sum()), int(lib.nt_arr[b.shape].sum()),
@@ -550,7 +558,9 @@ class Server:
             "resident_bodies_max": int(max(t["bodies"] for t in self.ticks)),
             "finished": len(self.finished),
         }
-        if self.finished:
-            wait = np.array([r.admitted - r.arrival for r in self.finished])
+        admitted = [r for r in self.finished + self.active if r.admitted is not None]
+        if admitted:   # every request that got in so far, finished or still running
+            wait = np.array([r.admitted - r.arrival for r in admitted])
             out["queue_wait_s_p50_p99"] = [float(np.percentile(wait, 50)), float(np.percentile(wait, 99))]
+        out["rejected"] = len(self.rejected)
         return out

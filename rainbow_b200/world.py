@@ -69,7 +69,26 @@ def make_rb_params(p, dt=None, scheme="rigid_gauss_seidel", termination="merit",
 
 
 def _t(a, dtype, device):
+    if isinstance(a, torch.Tensor):   # already a tensor (grids built on the device): no host round trip
+        return a.to(device=device, dtype=dtype)
     return torch.from_numpy(np.ascontiguousarray(a)).to(device=device, dtype=dtype)
+
+
+def _cat_pieces(pieces):
+    """Concatenation of (array, start, end) pieces; device tensors stay on the device (adjacent ranges of one
+    tensor are joined first, so a scene's grids are copied in one piece)."""
+    if not any(isinstance(a, torch.Tensor) for a, _, _ in pieces):
+        return np.concatenate([np.asarray(a).ravel()[i:j] for a, i, j in pieces])
+    dev = next(a.device for a, _, _ in pieces if isinstance(a, torch.Tensor))
+    merged = []
+    for a, i, j in pieces:
+        if merged and merged[-1][0] is a and merged[-1][2] == i:
+            merged[-1][2] = j
+        else:
+            merged.append([a, i, j])
+    return torch.cat([(a.reshape(-1)[i:j] if isinstance(a, torch.Tensor)
+                       else torch.from_numpy(np.ascontiguousarray(np.asarray(a).ravel()[i:j])).to(dev))
+                      for a, i, j in merged])
 
 
 PACKED_DTYPES = {
@@ -128,7 +147,7 @@ def pack_scenes(scenes):
                 raise ValueError("shape with %d triangles exceeds %d" % (nt, MAX_TRIANGLES_PER_SHAPE))
             V.append(np.asarray(s["shape_V"])[sv[k]:sv[k + 1]])
             T.append(np.asarray(s["shape_T"])[st[k]:st[k + 1]])
-            G.append(np.asarray(s["shape_grid"]).ravel()[sg[k]:sg[k + 1]])
+            G.append((s["shape_grid"], int(sg[k]), int(sg[k + 1])))
             v_off.append(v_off[-1] + int(sv[k + 1] - sv[k]))
             t_off.append(t_off[-1] + nt)
             g_off.append(g_off[-1] + int(sg[k + 1] - sg[k]))
@@ -137,7 +156,7 @@ def pack_scenes(scenes):
     P = {"n_shapes": nshape}
     P["shape_V"] = np.concatenate(V).reshape(-1)
     P["shape_T"] = np.concatenate(T).astype(np.int32).reshape(-1)
-    P["shape_grid"] = np.concatenate(G)
+    P["shape_grid"] = _cat_pieces(G)
     P["shape_v_off"] = np.array(v_off, np.int32)
     P["shape_t_off"] = np.array(t_off, np.int32)
     P["shape_g_off"] = np.array(g_off, np.int64)

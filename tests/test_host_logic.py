@@ -114,3 +114,82 @@ def test_api_set_hinge_matches_the_reference_frames():
         A.create_hinge(engine, "h0")
     with pytest.raises(ValueError):
         A.set_hinge(engine, "h0", names[0], names[1], np.zeros(3), np.array([0.0, 0.0, 1.0]), mode="nope")
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REFERENCE, "rainbow")), reason="reference checkout not present")
+def test_mirror_api_builds_the_reference_scene(monkeypatch):
+    """The same user script through the reference's api.py:159-281 calls (create_mesh, create_shape,
+    connect_shape, set_position / set_orientation with use_model_frame, set_mass_properties, set_body_type,
+    materials, gravity) and through rainbow_b200.api gives equal body-frame meshes (vertex and triangle order),
+    shape mass, inertia and frame (shape.r, shape.q), grid extents, body placement (r, q), masses, inertias,
+    fixed flags, materials and forces.  The grid values are compared on the GPU (tests/test_gpu_sdf.py); here
+    the mirror's grid construction is replaced by its extents only, as this container has no GPU."""
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_golden as MG   # puts the reference (with its two import stand-ins) on sys.path
+    from rainbow_b200 import api as A, geometry as GEO
+    from rainbow_b200.types import Grid
+
+    def extents_only(V, T, I, J, K, boundary=0.5, device="cuda"):
+        V = np.asarray(V, np.float64)
+        return Grid(V.min(axis=0) - boundary, V.max(axis=0) + boundary, I, J, K)
+    monkeypatch.setattr(GEO, "create_signed_distance", extents_only)
+
+    rng = np.random.default_rng(3)
+    placements = [(kind, size, rng.uniform(-3, 3, 3), rng.normal(size=4))
+                  for kind, size in (("box", (1.0, 0.6, 2.0)), ("sphere", 0.7), ("box", (0.5, 0.5, 0.5)),
+                                     ("sphere", 0.3))]
+
+    def build(api, create_box, create_sphere, vec, quat_identity):
+        engine = api.create_engine() if api is MG.API else api.create_engine("cpu")
+        engine.params.resolution = 6
+        api.create_surfaces_interaction(engine, "m", "m", 0.1, vec(0.4, 0.4, 0.4))
+        api.create_surfaces_interaction(engine, "m", "w", 0.0, vec(0.3, 0.2, 0.1))
+        V, T = create_box(20.0, 1.0, 20.0)
+        api.create_shape(engine, "ground_shape", api.create_mesh(V, T))
+        api.create_rigid_body(engine, "ground")
+        api.connect_shape(engine, "ground", "ground_shape")
+        api.set_position(engine, "ground", vec(0.0, -0.5, 0.0), True)
+        api.set_orientation(engine, "ground", quat_identity(), True)
+        api.set_body_type(engine, "ground", "fixed")
+        api.set_mass_properties(engine, "ground", 1.0)
+        api.set_body_material(engine, "ground", "m")
+        api.create_gravity_force(engine, "gravity", 9.81, vec(0.0, 1.0, 0.0))
+        for k, (kind, size, r, q) in enumerate(placements):
+            V, T = create_box(*size) if kind == "box" else create_sphere(size, 8, 8)
+            api.create_shape(engine, "s%d" % k, api.create_mesh(V, T))
+            api.create_rigid_body(engine, "b%d" % k)
+            api.connect_shape(engine, "b%d" % k, "s%d" % k)
+            api.set_position(engine, "b%d" % k, vec(*r), True)
+            api.set_orientation(engine, "b%d" % k, np.asarray(q / np.linalg.norm(q)), True)
+            api.set_mass_properties(engine, "b%d" % k, 1000.0 if k % 2 else 1.0)
+            api.connect_force(engine, "b%d" % k, "gravity")
+            api.set_body_material(engine, "b%d" % k, "w" if k == 2 else "m")
+        return engine
+
+    ref = build(MG.API, MG.create_box, MG.create_sphere, MG.V3.make, MG.Q.identity)
+    mine = build(A, A.create_box, A.create_sphere, lambda *a: np.array(a, np.float64),
+                 lambda: np.array([1.0, 0.0, 0.0, 0.0]))
+    assert list(ref.shapes) == list(mine.shapes) and list(ref.bodies) == list(mine.bodies)
+    for name in ref.shapes:
+        a, b = ref.shapes[name], mine.shapes[name]
+        np.testing.assert_array_equal(b.mesh.V, a.mesh.V, err_msg=name)
+        np.testing.assert_array_equal(b.mesh.T, a.mesh.T, err_msg=name)
+        np.testing.assert_array_equal(b.mass, a.mass, err_msg=name)
+        np.testing.assert_array_equal(b.inertia, a.inertia, err_msg=name)
+        np.testing.assert_array_equal(b.r, a.r, err_msg=name)
+        np.testing.assert_array_equal(b.q, a.q, err_msg=name)
+        for f in ("min_coord", "max_coord", "spacing"):
+            np.testing.assert_array_equal(getattr(b.grid, f), getattr(a.grid, f), err_msg=name)
+        assert (b.grid.I, b.grid.J, b.grid.K) == (a.grid.I, a.grid.J, a.grid.K)
+    for name in ref.bodies:
+        a, b = ref.bodies[name], mine.bodies[name]
+        np.testing.assert_array_equal(b.r, a.r, err_msg=name)
+        np.testing.assert_array_equal(b.q, a.q, err_msg=name)
+        np.testing.assert_array_equal(b.mass, a.mass, err_msg=name)
+        np.testing.assert_array_equal(b.inertia, a.inertia, err_msg=name)
+        assert (b.is_fixed, b.material, [f.name for f in b.forces]) == (a.is_fixed, a.material,
+                                                                        [f.name for f in a.forces])
+    for key in (("m", "m"), ("m", "w")):
+        ia, ib = ref.surfaces_interactions.get_interaction(*key), mine.surfaces_interactions.get_interaction(*key)
+        np.testing.assert_array_equal(ib.mu, ia.mu)
+        assert ib.epsilon == ia.epsilon

@@ -2,11 +2,11 @@
 
 Such a caller (an application that owns all device memory through its own pool, a real-time loop that must
 not allocate once running) has no way to hand rb_step a workspace, so this variant keeps the step's
-temporaries in a fixed scratch array inside the library.  The test steps one scene through the C ABI with
-both entry points, twice in a row, and demands identical results (the FP64 step is bit-exact, so the
-tolerance is zero).  The second call also shows that what the first call left in the shared scratch does not
-leak into the next step.  This file is collected last so that a failure here stops a run only after every
-other test has run.
+temporaries in a fixed scratch array inside the library.  The test first steps a larger, different scene
+through the scratch (so it holds another scene's lists and counters), then steps one scene through the C ABI
+with both entry points, twice in a row, and demands identical results (the FP64 step is bit-exact, so the
+tolerance is zero): whatever a call leaves in the shared scratch must not leak into the next step.  This file
+is collected last so that a failure here stops a run only after every other test has run.
 """
 import ctypes
 
@@ -33,6 +33,21 @@ def test_noalloc_step_matches_workspace_step_twice():
     N.check(lib.rb_workspace_bytes(ctypes.byref(no_ws.rb_bodies), ctypes.byref(no_ws.caps), ctypes.byref(need)),
             "rb_workspace_bytes")
     assert need.value <= (16 << 20), "fixture scene must fit the 16 MiB scratch"
+
+    # dirty the scratch: a few steps of the 64-box lattice (more bodies, pairs and contacts) through it
+    big = load_fixture("c1_boxes64")
+    other = W.DeviceWorld(big)
+    N.check(lib.rb_workspace_bytes(ctypes.byref(other.rb_bodies), ctypes.byref(other.caps), ctypes.byref(need)),
+            "rb_workspace_bytes")
+    assert need.value <= (16 << 20)
+    for _ in range(3):
+        other.t_status.zero_()
+        N.check(lib.rb_step_noalloc(ctypes.byref(other.rb_shapes), ctypes.byref(other.rb_bodies),
+                                    ctypes.byref(other.caps), ctypes.byref(W.make_rb_params(W.params_from_vector(big["params"]))),
+                                    ctypes.byref(other.rb_outputs), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)),
+                "rb_step_noalloc")
+    torch.cuda.synchronize()
+    assert other.n_contacts_total() > 0
 
     for _ in range(2):
         with_ws.t_status.zero_()
