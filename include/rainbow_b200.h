@@ -24,7 +24,7 @@
 extern "C" {
 #endif
 
-#define RB_ABI_VERSION 1
+#define RB_ABI_VERSION 2
 
 /* return codes */
 #define RB_OK 0
@@ -79,6 +79,11 @@ typedef struct rb_shapes {
     const int64_t* g_off;       /* n_shapes+1 value offsets */
     const double* grid_meta;    /* 12 doubles per shape: min[3], max[3], spacing[3], I, J, K (grid3.py:16) */
     int32_t max_shape_triangles; /* triangles of the largest shape (at most 16384) */
+    const float* grid32;        /* optional FP32 copy of grid (same offsets), or NULL.  With it, the FP32
+                                   precision modes run the contact search's signed distance lookups (the seed
+                                   and Frank-Wolfe iterations, collision_detection.py:134-165) in FP32; the
+                                   acceptance tests and the contact's point, normal and gap (:172-188) stay
+                                   FP64, evaluated at the point the FP32 search found */
 } rb_shapes;
 
 /* Bodies of one or more independent scenes; scene s owns bodies scene_start[s] .. scene_start[s+1]-1 in the
@@ -206,6 +211,12 @@ typedef struct rb_scene_stats {
     double max_penetration;       /* contacts.py:222 */
     double solve_start_us;        /* device clock (%globaltimer, microseconds) when the scene's solve started (profiling only) */
     double solve_us;              /* device time of the scene's contact solve, FP32 and FP64 phases (profiling only) */
+    int32_t n_search_flips;       /* FP32 contact search (profiling only): candidates whose seed, Frank-Wolfe vertex
+                                     choices or iteration count differ from the FP64 search's */
+    int32_t n_accept_flips;       /* ... candidates the FP32 search accepts as a contact and the FP64 search does
+                                     not, or the other way round */
+    int32_t n_grid_lookups32;     /* signed distance lookups of the contact search made on grid32 (profiling only;
+                                     n_grid_lookups counts the FP64 ones) */
 } rb_scene_stats;
 
 /* Outputs: device buffers sized by rb_caps.contact_capacity / n_scenes / max_iterations. */

@@ -32,7 +32,7 @@ _i32 = ctypes.c_int32
 
 class RbShapes(ctypes.Structure):
     _fields_ = [("n_shapes", _i32), ("V", _vp), ("v_off", _vp), ("T", _vp), ("t_off", _vp), ("grid", _vp),
-                ("g_off", _vp), ("grid_meta", _vp), ("max_shape_triangles", _i32)]
+                ("g_off", _vp), ("grid_meta", _vp), ("max_shape_triangles", _i32), ("grid32", _vp)]
 
 
 class RbBodies(ctypes.Structure):
@@ -78,6 +78,7 @@ class RbSceneStats(ctypes.Structure):
         ("n_levels", _i32), ("fp32_sweeps", _i32), ("merit", ctypes.c_double), ("residual", ctypes.c_double), ("kinetic_energy", ctypes.c_double),
         ("potential_energy", ctypes.c_double), ("max_penetration", ctypes.c_double),
         ("solve_start_us", ctypes.c_double), ("solve_us", ctypes.c_double),
+        ("n_search_flips", _i32), ("n_accept_flips", _i32), ("n_grid_lookups32", _i32),
     ]
 
 
@@ -127,7 +128,7 @@ def load():
             fn = getattr(lib, name)
             fn.restype = res
             fn.argtypes = args
-        if lib.rb_abi_version() != 1:
+        if lib.rb_abi_version() != 2:
             raise NativeError("rainbow_b200 ABI version mismatch")
         _lib = lib
     return _lib

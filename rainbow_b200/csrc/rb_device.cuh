@@ -216,6 +216,51 @@ __device__ __forceinline__ bool grid_is_inside(const GridView& g, d3 p, double b
     return true;
 }
 
+// FP32 copies of the lookups above for the contact search of the FP32 precision modes: the same cell choice,
+// interpolation and gradient expressions (the min_coord divisor included) on an FP32 copy of the grid
+struct GridView32 {
+    const float* values;
+    float mn[3], mx[3], sp[3];
+    int I, J, K;
+};
+__device__ __forceinline__ GridView32 load_grid32(const double* meta, const float* values) {
+    GridView32 g;
+    g.values = values;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) { g.mn[a] = (float)meta[a]; g.mx[a] = (float)meta[3 + a]; g.sp[a] = (float)meta[6 + a]; }
+    g.I = (int)meta[9]; g.J = (int)meta[10]; g.K = (int)meta[11];
+    return g;
+}
+__device__ __forceinline__ int cell_index32(float p, float mn, float sp, int n) {
+    const float f = floorf((p - mn) / sp);
+    const int lim = n - 2;
+    if (!(f >= 0.0f)) return 0;
+    if (f > (float)lim) return lim;
+    return (int)f;
+}
+__device__ __forceinline__ float3 grid_gradient32(const GridView32& g, float3 p) {
+    const int i = cell_index32(p.x, g.mn[0], g.sp[0], g.I);
+    const int j = cell_index32(p.y, g.mn[1], g.sp[1], g.J);
+    const int k = cell_index32(p.z, g.mn[2], g.sp[2], g.K);
+    const int64_t I = g.I, IJ = (int64_t)g.I * g.J;
+    const float* v = g.values + i + I * j + IJ * k;
+    const float d000 = __ldg(v), d100 = __ldg(v + 1), d010 = __ldg(v + I), d110 = __ldg(v + I + 1);
+    const float d001 = __ldg(v + IJ), d101 = __ldg(v + IJ + 1), d011 = __ldg(v + IJ + I), d111 = __ldg(v + IJ + I + 1);
+    const float s = (p.x - ((float)i * g.sp[0] + g.mn[0])) / g.mn[0];
+    const float t = (p.y - ((float)j * g.sp[1] + g.mn[1])) / g.mn[1];
+    const float u = (p.z - ((float)k * g.sp[2] + g.mn[2])) / g.mn[2];
+    const float x00 = (d100 - d000) * s + d000, x01 = (d101 - d001) * s + d001;
+    const float x10 = (d110 - d010) * s + d010, x11 = (d111 - d011) * s + d011;
+    const float y0 = (x10 - x00) * t + x00, y1 = (x11 - x01) * t + x01;
+    const float dx00 = d100 - d000, dx01 = d101 - d001, dx10 = d110 - d010, dx11 = d111 - d011;
+    const float dy0_ds = (dx10 - dx00) * t + dx00, dy1_ds = (dx11 - dx01) * t + dx01;
+    const float dy0_dt = x10 - x00, dy1_dt = x11 - x01;
+    const float dp_ds = (dy1_ds - dy0_ds) * u + dy0_ds;
+    const float dp_dt = (dy1_dt - dy0_dt) * u + dy0_dt;
+    const float dp_du = y1 - y0;
+    return make_float3(dp_ds * (1.0f / g.sp[0]), dp_dt * (1.0f / g.sp[1]), dp_du * (1.0f / g.sp[2]));
+}
+
 // NumPy np.add.reduceat over one segment: a[0] + pairwise_sum(a[1:]) (8 interleaved partial sums once the
 // remainder holds at least 8 values).  Used for the Delassus diagonal (contacts.py:49).
 __device__ __forceinline__ double np_reduce_sum(const double* a, int m) {

@@ -228,7 +228,11 @@ __global__ void k_bodies(const StepArgs a) {
 
 __global__ void k_zero_stats(const StepArgs a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < a.bd.n_scenes) { a.out.stats[s].n_grid_lookups = 0; a.out.stats[s].n_leaf_overlaps = 0; }
+    if (s < a.bd.n_scenes) {
+        rb_scene_stats* st = a.out.stats + s;
+        st->n_grid_lookups = 0; st->n_leaf_overlaps = 0;
+        st->n_grid_lookups32 = 0; st->n_search_flips = 0; st->n_accept_flips = 0;
+    }
 }
 
 // collision_detection.py:32 V_world = rotate_array(q, V) + r
@@ -498,6 +502,78 @@ __global__ void __launch_bounds__(kBlock) k_mid(const StepArgs a, int max_cluste
 // ---------------------------------------------------------------------------------------------------------
 // narrow phase (collision_detection.py:87 _compute_contacts): one thread per candidate triangle
 // ---------------------------------------------------------------------------------------------------------
+// seed and Frank-Wolfe search on one triangle (ps: its corners in the SDF owner's frame) in FP64
+// (collision_detection.py:134-165).  Returns the point; n_fw = iterations, trace = the seed (bits 0-1) and
+// each iteration's vertex (2 bits each from bit 2)
+__device__ __forceinline__ d3 fw_search64(const GridView& g, const d3* ps, int max_it, double tol, int& n_fw,
+                                          uint32_t& trace) {
+    // seed: corner with the smallest gradient norm (:136-140); norm(list, axis=1) sums squares unfused
+    double gn[3];
+    for (int c = 0; c < 3; ++c) {
+        const d3 gr = grid_gradient(g, ps[c]);
+        gn[c] = sqrt((gr.x * gr.x + gr.y * gr.y) + gr.z * gr.z);
+    }
+    int best = 0;
+    if (gn[1] < gn[best]) best = 1;
+    if (gn[2] < gn[best]) best = 2;
+    trace = (uint32_t)best;
+    d3 x = best == 0 ? ps[0] : (best == 1 ? ps[1] : ps[2]);   // selects keep ps in registers
+    n_fw = 0;
+    for (int i = 0; i < max_it; ++i) {   // Frank-Wolfe (:144-165)
+        ++n_fw;
+        // the reference evaluates the same gradient once per corner; one evaluation gives identical values
+        const d3 gr = grid_gradient(g, x);
+        const double o0 = dot3_np(ps[0], gr), o1 = dot3_np(ps[1], gr), o2 = dot3_np(ps[2], gr);
+        int v = 0;
+        double ov = o0;
+        if (o1 < ov) { v = 1; ov = o1; }
+        if (o2 < ov) { v = 2; ov = o2; }
+        if (i < 15) trace |= (uint32_t)v << (2 + 2 * i);
+        const double alpha = 2.0 / (double)(i + 2);
+        const d3 s = v == 0 ? ps[0] : (v == 1 ? ps[1] : ps[2]);
+        x = d3{x.x + alpha * (s.x - x.x), x.y + alpha * (s.y - x.y), x.z + alpha * (s.z - x.z)};
+        if (ov > tol) break;
+    }
+    return x;
+}
+
+// the same search in FP32 on the FP32 grid (the FP32 precision modes): the same decisions, FP32 arithmetic
+__device__ __forceinline__ float3 fw_search32(const GridView32& g, const float3* ps, int max_it, float tol, int& n_fw,
+                                              uint32_t& trace) {
+    float gn[3];
+    for (int c = 0; c < 3; ++c) {
+        const float3 gr = grid_gradient32(g, ps[c]);
+        gn[c] = (gr.x * gr.x + gr.y * gr.y) + gr.z * gr.z;   // squared norms order the corners as the norms do
+    }
+    int best = 0;
+    if (gn[1] < gn[best]) best = 1;
+    if (gn[2] < gn[best]) best = 2;
+    trace = (uint32_t)best;
+    float3 x = best == 0 ? ps[0] : (best == 1 ? ps[1] : ps[2]);
+    n_fw = 0;
+    for (int i = 0; i < max_it; ++i) {
+        ++n_fw;
+        const float3 gr = grid_gradient32(g, x);
+        const float o0 = fmaf(ps[0].z, gr.z, fmaf(ps[0].y, gr.y, ps[0].x * gr.x));
+        const float o1 = fmaf(ps[1].z, gr.z, fmaf(ps[1].y, gr.y, ps[1].x * gr.x));
+        const float o2 = fmaf(ps[2].z, gr.z, fmaf(ps[2].y, gr.y, ps[2].x * gr.x));
+        int v = 0;
+        float ov = o0;
+        if (o1 < ov) { v = 1; ov = o1; }
+        if (o2 < ov) { v = 2; ov = o2; }
+        if (i < 15) trace |= (uint32_t)v << (2 + 2 * i);
+        const float alpha = 2.0f / (float)(i + 2);
+        const float3 s = v == 0 ? ps[0] : (v == 1 ? ps[1] : ps[2]);
+        x = make_float3(fmaf(alpha, s.x - x.x, x.x), fmaf(alpha, s.y - x.y, x.y), fmaf(alpha, s.z - x.z, x.z));
+        if (ov > tol) break;
+    }
+    return x;
+}
+
+// kF32: the seed and Frank-Wolfe lookups on the FP32 grid copy; the acceptance tests (is_inside, phi <=
+// envelope) and the contact's point, normal and gap in FP64 at the point found.  A profiled step also runs
+// the FP64 search and counts, per scene, the candidates whose search decisions or acceptance differ.
+template <bool kF32>
 __global__ void __launch_bounds__(256, 2) k_narrow(const StepArgs a) {
     if (a.ws.counters[kAbort]) return;
     const int n_items = a.ws.counters[kNItems];
@@ -523,33 +599,22 @@ __global__ void __launch_bounds__(256, 2) k_narrow(const StepArgs a) {
             ps[c] = quat_rotate_row(cqB, sub(pw, rB));   // :120-121
         }
         const GridView g = load_grid(a.sh.grid_meta + 12 * ss, a.sh.grid + a.sh.g_off[ss]);
-        // seed: corner with the smallest gradient norm (:136-140); norm(list, axis=1) sums squares unfused
-        double gn[3];
-        for (int c = 0; c < 3; ++c) {
-            const d3 gr = grid_gradient(g, ps[c]);
-            gn[c] = sqrt((gr.x * gr.x + gr.y * gr.y) + gr.z * gr.z);
-        }
-        int best = 0;
-        if (gn[1] < gn[best]) best = 1;
-        if (gn[2] < gn[best]) best = 2;
-        d3 x = best == 0 ? ps[0] : (best == 1 ? ps[1] : ps[2]);   // selects keep ps in registers
-        int n_fw = 0;
-        for (int i = 0; i < max_it; ++i) {   // Frank-Wolfe (:144-165)
-            ++n_fw;
-            // the reference evaluates the same gradient once per corner; one evaluation gives identical values
-            const d3 gr = grid_gradient(g, x);
-            const double o0 = dot3_np(ps[0], gr), o1 = dot3_np(ps[1], gr), o2 = dot3_np(ps[2], gr);
-            int v = 0;
-            double ov = o0;
-            if (o1 < ov) { v = 1; ov = o1; }
-            if (o2 < ov) { v = 2; ov = o2; }
-            const double alpha = 2.0 / (double)(i + 2);
-            const d3 s = v == 0 ? ps[0] : (v == 1 ? ps[1] : ps[2]);
-            x = d3{x.x + alpha * (s.x - x.x), x.y + alpha * (s.y - x.y), x.z + alpha * (s.z - x.z)};
-            if (ov > tol) break;
+        int n_fw = 0, lookups = 0, lookups32 = 0;
+        uint32_t trace = 0u;
+        d3 x;
+        if (kF32) {
+            const GridView32 g32 = load_grid32(a.sh.grid_meta + 12 * ss, a.sh.grid32 + a.sh.g_off[ss]);
+            const float3 ps32[3] = {make_float3((float)ps[0].x, (float)ps[0].y, (float)ps[0].z),
+                                    make_float3((float)ps[1].x, (float)ps[1].y, (float)ps[1].z),
+                                    make_float3((float)ps[2].x, (float)ps[2].y, (float)ps[2].z)};
+            const float3 x32 = fw_search32(g32, ps32, max_it, (float)tol, n_fw, trace);
+            x = d3{(double)x32.x, (double)x32.y, (double)x32.z};
+            lookups32 = 3 + n_fw;
+        } else {
+            x = fw_search64(g, ps, max_it, tol, n_fw, trace);
+            lookups = 3 + n_fw;   // seed gradients + one gradient per Frank-Wolfe iteration
         }
         int flag = 0;
-        int lookups = 3 + n_fw;   // seed gradients + one gradient per Frank-Wolfe iteration
         if (grid_is_inside(g, x, 0.5)) {   // :172 (is_inside default boundary 0.5)
             lookups += 1;
             const double phi = grid_value(g, x);
@@ -570,9 +635,20 @@ __global__ void __launch_bounds__(256, 2) k_narrow(const StepArgs a) {
             }
         }
         a.ws.item_flag[it] = flag;
-        if (a.pr.profiling) {   // statistic for the bandwidth accounting: lookups per scene
+        if (a.pr.profiling) {   // statistics for the bandwidth accounting (lookups per scene) and decision flips
             const int s = scene_of(a.bd.scene_start, a.bd.n_scenes, A);
             atomicAdd(&a.out.stats[s].n_grid_lookups, lookups);
+            if (kF32) {
+                atomicAdd(&a.out.stats[s].n_grid_lookups32, lookups32);
+                int n64 = 0;
+                uint32_t trace64 = 0u;
+                const d3 x64 = fw_search64(g, ps, max_it, tol, n64, trace64);
+                int accept64 = 0;
+                if (grid_is_inside(g, x64, 0.5) && grid_value(g, x64) <= envelope)
+                    accept64 = norm3_np(quat_rotate(qB, grid_gradient(g, x64))) > 0.0;
+                if (n64 != n_fw || trace64 != trace) atomicAdd(&a.out.stats[s].n_search_flips, 1);
+                if (accept64 != flag) atomicAdd(&a.out.stats[s].n_accept_flips, 1);
+            }
         }
     }
 }
@@ -1723,10 +1799,12 @@ constexpr int kS32MidSlab = 56 * 1024;               // slab of a warp team, mid
 // relative residual below which a stalled FP32 iteration may have met FP32 rounding
 constexpr float kFp32Floor = 1e-5f;
 // residual tests without a 5 % improvement after which an FP32 round ends in a defect correction (with the
-// test every 4 sweeps: 64 sweeps; Gauss-Seidel often progresses by less than 5 % in 12 sweeps near 1e-6)
+// test every 4 sweeps: 64 sweeps; Gauss-Seidel often progresses by less than 5 % in 12 sweeps near 1e-6).
+// A round that did not lower the FP64 residual by kS32RoundGain doubles the next round's window (up to
+// kS32StallTestsMax): a scene whose Gauss-Seidel iteration itself has stalled keeps sweeping in FP32 with
+// rare corrections, as FP64 sweeps would stall on it just the same
 constexpr int kS32StallTests = 16;
-// a correction round that lowers the FP64 residual by less than this factor, below kFp32Floor, hands the
-// scene to FP64 sweeps: the FP32 iteration cannot take it further
+constexpr int kS32StallTestsMax = 512;
 constexpr double kS32RoundGain = 0.9;
 
 struct S32Scene {
@@ -1848,11 +1926,10 @@ __device__ __forceinline__ int s32_load(const StepArgs& a, const G& g, const Sce
     return L;
 }
 
-// w = W J^T x (each body sums its contacts in ascending order), then the FP32 residual
-// ||x - prox(x - D^-1 (A x + b))||_inf / max(1, ||x||_inf)
+// w = W J^T x (each body sums its contacts in ascending order)
 template <class G>
-__device__ __forceinline__ float s32_residual(const StepArgs& a, const G& g, const SceneRange& R, const S32Scene& f) {
-    const int K = R.c1 - R.c0, nb = R.b1 - R.b0;
+__device__ __forceinline__ void s32_rebuild_w(const G& g, const SceneRange& R, const S32Scene& f) {
+    const int nb = R.b1 - R.b0;
     for (int bl = g.rank(); bl < nb; bl += g.size()) {
         float* B = f.body + kS32BodyFloats * bl;
         float P[3] = {0.f, 0.f, 0.f}, T[3] = {0.f, 0.f, 0.f};
@@ -1879,6 +1956,13 @@ __device__ __forceinline__ float s32_residual(const StepArgs& a, const G& g, con
         B[3] = om[0]; B[4] = om[1]; B[5] = om[2];
     }
     g.sync();
+}
+
+// w = W J^T x, then the FP32 residual ||x - prox(x - D^-1 (A x + b))||_inf / max(1, ||x||_inf)
+template <class G>
+__device__ __forceinline__ float s32_residual(const StepArgs& a, const G& g, const SceneRange& R, const S32Scene& f) {
+    const int K = R.c1 - R.c0;
+    s32_rebuild_w(g, R, f);
     float m = 0.0f, xm = 0.0f;
     for (int i = g.rank(); i < K; i += g.size()) {
         const float4* C4 = reinterpret_cast<const float4*>(f.c + kS32Floats * i);
@@ -2009,6 +2093,44 @@ __device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, 
         start = end;
         end = next_end;
     }
+}
+
+// One proximal Jacobi sweep (proximal_contact/jacobi_solver.py:41-57) on the FP32 copy: every contact's new
+// impulse from the accumulators w = W J^T x of the previous iterate, four lanes per contact as in the
+// Gauss-Seidel sweep (any order: no contact reads another's new impulse), then w rebuilt from the new
+// impulses.  hybrid (jacobi_solver.py:60-79): the friction ball's radius uses the new normal impulse instead
+// of the previous one.
+template <class G>
+__device__ __forceinline__ void s32_sweep_jacobi(const G& g, const SceneRange& R, const S32Scene& f, float rscale,
+                                                 bool hybrid) {
+    const int K = R.c1 - R.c0;
+    const int q = g.rank() & 3, slot = g.rank() >> 2, nslot = g.size() >> 2;
+    const int base = (threadIdx.x & 31) & ~3;
+    const unsigned qm = 0xfu << base;
+    for (int i = slot; i < K; i += nslot) {   // the four lanes of a quad take the same contacts
+        const float4* C4 = reinterpret_cast<const float4*>(f.c + kS32Floats * i);
+        const uint32_t lh = f.lohi[i];
+        const float* Bl = f.body + kS32BodyFloats * (int)(lh & 0xffffu);
+        const float* Bh = f.body + kS32BodyFloats * (int)(lh >> 16);
+        const float4 r0 = C4[3 * q], r1 = C4[3 * q + 1], r2 = C4[3 * q + 2];   // own row
+        const float4 l0 = *reinterpret_cast<const float4*>(Bl), l1 = *reinterpret_cast<const float4*>(Bl + 4);
+        const float4 h0 = *reinterpret_cast<const float4*>(Bh), h1 = *reinterpret_cast<const float4*>(Bh + 4);
+        float lin = fmaf(r0.x, l0.x - h0.x, fmaf(r0.y, l0.y - h0.y, r0.z * (l0.z - h0.z)));
+        if (q == 3) lin = 0.0f;
+        const float alo = fmaf(r1.x, l0.w, fmaf(r1.y, l1.x, r1.z * l1.y));
+        const float ahi = fmaf(r2.x, h0.w, fmaf(r2.y, h1.x, r2.z * h1.y));
+        const float z = r2.w - rscale * r1.w * (((lin + alo) + ahi) + r0.w);
+        float zz[4];
+        for (int j = 0; j < 4; ++j) zz[j] = __shfl_sync(qm, z, base | j);
+        const float mu = __shfl_sync(qm, r0.x, base | 3);
+        const float xn_old = __shfl_sync(qm, r2.w, base);   // every read of the old impulses is done here
+        const float xn = fmaxf(zz[0], 0.0f);
+        float fr[3];
+        f32_prox(zz[1], zz[2], zz[3], mu, hybrid ? xn : xn_old, fr);
+        f.c[kS32Floats * i + 12 * q + 11] = q == 0 ? xn : fr[q - 1];
+    }
+    g.sync();
+    s32_rebuild_w(g, R, f);
 }
 
 // FP64 check of the FP32 iterate and defect correction of the FP32 problem.  With x the current FP32 iterate,
@@ -2181,6 +2303,8 @@ __global__ void __launch_bounds__(kL2 ? kFp32L2Block : kFp32BlockMax, 1) k_solve
     if (a.pr.relaxation > 0.0) rs *= a.pr.relaxation;
     const float rscale = (float)rs;
     const bool coloured = a.pr.scheme == RB_SCHEME_COLOURED_GS || a.pr.ordering == RB_ORDER_COLOURED;
+    const bool jacobi = a.pr.scheme == RB_SCHEME_JACOBI || a.pr.scheme == RB_SCHEME_JACOBI_HYBRID;
+    const bool hybrid = a.pr.scheme == RB_SCHEME_JACOBI_HYBRID;
     const int cls = queue - kQueueFp32;
     const int list0 = cls == 0 ? 0 : a.ws.counters[kClassEnd32 + cls - 1];
     const int list1 = a.ws.counters[kClassEnd32 + cls];
@@ -2214,13 +2338,14 @@ __global__ void __launch_bounds__(kL2 ? kFp32L2Block : kFp32BlockMax, 1) k_solve
         if (g.rank() == 0) a.ws.nlev[s] = L;
         float res = s32_residual(a, g, R, f);   // the warm-started iterate may already be good enough
         float best = res;
-        int sweeps = 0, stalls = 0;
+        int sweeps = 0, stalls = 0, window = kS32StallTests;
         double r64 = -1.0;            // FP64 residual of the current iterate, once evaluated
         double r64_round = INFINITY;  // FP64 residual after the previous correction round
         for (;;) {
             const int round_start = sweeps;
             while (res > tol && sweeps < budget) {
-                s32_sweep<G, kL2>(g, f, L, rscale, bodies_global);
+                if (jacobi) s32_sweep_jacobi(g, R, f, rscale, hybrid);
+                else s32_sweep<G, kL2>(g, f, L, rscale, bodies_global);
                 ++sweeps;
                 if (sweeps % interval == 0 || sweeps == budget) {
                     res = s32_residual(a, g, R, f);
@@ -2228,17 +2353,17 @@ __global__ void __launch_bounds__(kL2 ? kFp32L2Block : kFp32BlockMax, 1) k_solve
                     // problem's own rounding, or slow progress a defect correction may speed up).  Above the
                     // floor a pause is the Gauss-Seidel iteration itself (it is not monotone), so go on.
                     if (res < 0.95f * best) { best = res; stalls = 0; }
-                    else if (best < kFp32Floor && ++stalls >= kS32StallTests) break;
+                    else if (best < kFp32Floor && ++stalls >= window) break;
                 }
             }
             // FP32 + refinement: test in FP64; if the FP32 answer misses the tolerance in FP64, correct the FP32
-            // problem's b by the FP64 defect and sweep on in FP32.  FP64 sweeps take over only when a round no
-            // longer lowers the FP64 residual while it is below the FP32 floor.
+            // problem's b by the FP64 defect and sweep on in FP32.  FP64 sweeps take over only when the FP32
+            // problem meets the tolerance and the FP64 one does not (the FP32 sweeps can do no more).
             if (a.pr.precision != RB_PRECISION_FP32_REFINE || sweeps >= budget) break;
             r64 = s32_correct(a, g, R, f);
             if (r64 <= a.pr.residual_tolerance) break;
-            if (sweeps == round_start) break;   // the FP32 problem meets the tolerance, the FP64 one does not
-            if (r64 < (double)kFp32Floor && r64 > kS32RoundGain * r64_round) break;   // r64 stays valid for x
+            if (sweeps == round_start) break;   // r64 stays valid for x
+            if (r64 > kS32RoundGain * r64_round) window = min(2 * window, kS32StallTestsMax);
             r64_round = fmin(r64_round, r64);
             r64 = -1.0;   // the sweeps that follow change the iterate
             res = s32_residual(a, g, R, f);
@@ -2668,10 +2793,8 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     if (pr->max_iterations < 0 || pr->max_iterations > caps->max_iterations)
         return fail(RB_ERR_ARG, "rb_step: max_iterations exceeds rb_caps.max_iterations");
     if (!(pr->dt > 0.0)) return fail(RB_ERR_ARG, "rb_step: dt must be positive");
-    if (pr->precision != RB_PRECISION_FP64 &&
-        (pr->termination != RB_TERMINATE_RESIDUAL_FIXED_R ||
-         !(pr->scheme == RB_SCHEME_RIGID_GS || pr->scheme == RB_SCHEME_GS || pr->scheme == RB_SCHEME_COLOURED_GS)))
-        return fail(RB_ERR_UNSUPPORTED, "rb_step: FP32 precision needs the fixed-r residual rule and a Gauss-Seidel scheme");
+    if (pr->precision != RB_PRECISION_FP64 && pr->termination != RB_TERMINATE_RESIDUAL_FIXED_R)
+        return fail(RB_ERR_UNSUPPORTED, "rb_step: FP32 precision needs the fixed-r residual rule");
     if (pr->precision < RB_PRECISION_FP64 || pr->precision > RB_PRECISION_FP32)
         return fail(RB_ERR_ARG, "rb_step: unknown precision");
     if (sh->max_shape_triangles <= 0 || sh->max_shape_triangles > 32 * kMaxClustersPerShape)
@@ -2718,7 +2841,11 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     k_check<<<1, 1, 0, st>>>(a.ws.counters, kNItems, caps->item_capacity, RB_STATUS_ITEM_OVERFLOW, out->status); note_launch();
     prof_mark(prof, 2, st);
     // narrow phase
-    k_narrow<<<narrow_blocks, narrow_threads, 0, st>>>(a); note_launch();
+    if (pr->precision != RB_PRECISION_FP64 && sh->grid32) {
+        k_narrow<true><<<narrow_blocks, narrow_threads, 0, st>>>(a); note_launch();
+    } else {
+        k_narrow<false><<<narrow_blocks, narrow_threads, 0, st>>>(a); note_launch();
+    }
     prof_mark(prof, 3, st);
     // reduction and compaction
     k_dedup<false><<<G, kBlock, 0, st>>>(a); note_launch();

@@ -88,11 +88,13 @@ class ShapeLibrary:
             "g_off": off([len(g) for g in self.G], np.int64).to(dev),
             "grid_meta": torch.from_numpy(np.concatenate(self.meta)).to(dev, torch.float64),
         }
+        self.t["grid32"] = self.t["grid"].float()   # the FP32 modes' contact search reads this copy
         sh = N.RbShapes()
         sh.n_shapes = len(self.V)
         for f in ("V", "v_off", "T", "t_off", "grid", "g_off", "grid_meta"):
             setattr(sh, f, self.t[f].data_ptr())
         sh.max_shape_triangles = max(self.nt)
+        sh.grid32 = self.t["grid32"].data_ptr()
         self.rb_shapes = sh
         self._dirty = False
 

@@ -297,6 +297,9 @@ class DeviceWorld:
             setattr(sh, f, T["shape_" + f].data_ptr())
         sh.grid_meta = T["shape_grid_meta"].data_ptr()
         sh.max_shape_triangles = int(np.diff(P["shape_t_off"]).max())
+        # FP32 copy of the grids for the contact search of the FP32 precision modes (FP64 steps ignore it)
+        T["shape_grid32"] = T["shape_grid"].float()
+        sh.grid32 = T["shape_grid32"].data_ptr()
         self.rb_shapes = sh
         bd = N.RbBodies()
         bd.n_bodies, bd.n_scenes = self.n_bodies, self.n_scenes

@@ -32,7 +32,7 @@ def test_library_loads_and_exports_every_declared_symbol():
     for name in declared_functions():
         assert hasattr(lib, name), name
         assert name in N.SIGNATURES, "no ctypes signature for %s" % name
-    assert lib.rb_abi_version() == 1
+    assert lib.rb_abi_version() == 2
 
 
 STRUCTS = {

@@ -68,7 +68,7 @@ def test_server_rejects_a_request_it_cannot_run_and_serves_the_rest():
     assert srv.report()["rejected"] == 1
     done = {r.uid: r for r in srv.finished}
     for r, d in ((done[u1], good1), (done[u2], good2)):
-        w = W.DeviceWorld(d, max_iterations=100)
+        w = W.DeviceWorld(d, max_iterations=int(rp.max_iterations))
         for _ in range(r.horizon):
             w.step(rp)
         np.testing.assert_array_equal(r.result[0], w.state()[0])
@@ -91,7 +91,7 @@ def test_server_holds_requests_beyond_its_memory_budget():
     assert sorted(done) == [ua, ub]
     assert done[ub].admitted >= done[ua].admitted
     for uid, d, h in ((ua, a, 3), (ub, b, 2)):
-        w = W.DeviceWorld(d, max_iterations=100)
+        w = W.DeviceWorld(d, max_iterations=int(rp.max_iterations))
         for _ in range(h):
             w.step(rp)
         np.testing.assert_array_equal(done[uid].result[0], w.state()[0])

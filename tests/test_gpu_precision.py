@@ -100,3 +100,72 @@ def test_fp32_solve_of_scenes_whose_rows_live_in_l2():
         assert s32[i].fp32_sweeps > 0
         assert np.abs(u32[b0:b1] - u64[b0:b1]).max() <= 1e-3 * np.abs(u64[b0:b1]).max()
         assert s32[i].residual <= 2.0 * s64[i].residual + 1e-6
+
+
+def test_fp32_contact_search_reports_its_decision_flips():
+    """The FP32 modes run the contact search's lookups on the FP32 grid copy and accept contacts in FP64 at the
+    point found.  On 16 scenes of the batched workload after a 20-step pre-roll, a profiled step counts the
+    candidates whose search decisions or acceptance differ from the FP64 search: few of them, and in scenes
+    without a flip the contacts of both searches lie within 1e-5 m of each other."""
+    from rainbow_b200 import scenes
+    from rainbow_b200 import world as W
+    arrays, params = scenes.batch_arrays(n_scenes=16, seed=0, pool=64, resolution=32, device="cuda:0")
+    w = W.DeviceWorld(arrays, max_iterations=100)
+    kw = dict(termination="residual_fixed_r", residual_tolerance=1e-6, residual_interval=4, profiling=True)
+    for _ in range(20):
+        w.step(W.make_rb_params(params, **dict(kw, profiling=False)))
+    x0, u0 = w.state()
+    out = {}
+    for mode in ("fp64", "fp32_refine"):
+        w.set_state(x0, u0)
+        w.step(W.make_rb_params(params, precision=mode, **kw))
+        out[mode] = (w.stats(), w.contacts())
+    (s64, c64), (s32, c32) = out["fp64"], out["fp32_refine"]
+    cand = sum(s.n_candidates for s in s32)
+    assert cand > 0 and sum(s.n_grid_lookups32 for s in s32) > 0 and sum(s.n_grid_lookups32 for s in s64) == 0
+    search = sum(s.n_search_flips for s in s32)
+    accept = sum(s.n_accept_flips for s in s32)
+    assert search <= 0.05 * cand and accept <= 0.01 * cand, (search, accept, cand)
+    assert sum(s.n_search_flips + s.n_accept_flips for s in s64) == 0
+    checked = 0
+    for a, b in zip(s64, s32):
+        if a.n_contacts != b.n_contacts or a.n_contacts == 0 or b.n_search_flips or b.n_accept_flips:
+            continue
+        ka, kb = slice(a.contact_start, a.contact_start + a.n_contacts), slice(b.contact_start, b.contact_start + b.n_contacts)
+        if not np.array_equal(c64["ids"][ka], c32["ids"][kb]):
+            continue
+        assert np.abs(c64["p"][ka] - c32["p"][kb]).max() <= 1e-5
+        checked += 1
+    assert checked >= 8
+
+
+@pytest.mark.parametrize("scheme", ["parallel_jacobi", "parallel_jacobi_hybrid"])
+def test_fp32_jacobi_agrees_with_fp64_jacobi(scheme):
+    """Proximal Jacobi (jacobi_solver.py:41-79) in FP32 + FP64 refinement against the FP64 Jacobi solve of the
+    same step: the same share of steps meets the 1e-6 residual, and the velocities agree to 1e-4 of their scale
+    on the 64-box lattice over 10 steps from the same states."""
+    from rainbow_b200 import world as W
+    from conftest import load_fixture
+    d = load_fixture("c1_boxes64")
+    p = W.params_from_vector(d["params"])
+    p["max_iterations"] = 3000
+    w = W.DeviceWorld(d, max_iterations=3000)
+    kw = dict(scheme=scheme, termination="residual_fixed_r", residual_tolerance=1e-6, residual_interval=4,
+              warm_start=True)
+    met = {"fp64": 0, "fp32_refine": 0}
+    for _ in range(10):
+        x0, u0 = w.state()
+        cache = (w.t_cache_key.clone(), w.t_cache_sol.clone(), w.t_cache_count.clone())
+        out = {}
+        for mode in ("fp32_refine", "fp64"):      # FP64 last: the trajectory follows FP64
+            w.set_state(x0, u0)
+            w.t_cache_key.copy_(cache[0]); w.t_cache_sol.copy_(cache[1]); w.t_cache_count.copy_(cache[2])
+            w.step(W.make_rb_params(p, precision=mode, **kw))
+            st = w.stats()[0]
+            met[mode] += st.exitcode == 3
+            out[mode] = (w.state()[1], st)
+        (u32, s32), (u64, s64) = out["fp32_refine"], out["fp64"]
+        if s64.n_contacts:
+            assert s32.fp32_sweeps > 0
+            assert np.abs(u32 - u64).max() <= 1e-4 * max(1e-3, np.abs(u64).max())
+    assert met["fp32_refine"] >= met["fp64"] - 1

@@ -36,18 +36,20 @@ def test_noalloc_step_matches_workspace_step_twice():
 
     # dirty the scratch: a few steps of the 64-box lattice (more bodies, pairs and contacts) through it
     big = load_fixture("c1_boxes64")
+    big_params = W.make_rb_params(W.params_from_vector(big["params"]))
     other = W.DeviceWorld(big)
+    other.step(big_params)   # with a workspace: grows the work lists to this scene's needs
     N.check(lib.rb_workspace_bytes(ctypes.byref(other.rb_bodies), ctypes.byref(other.caps), ctypes.byref(need)),
             "rb_workspace_bytes")
     assert need.value <= (16 << 20)
     for _ in range(3):
         other.t_status.zero_()
         N.check(lib.rb_step_noalloc(ctypes.byref(other.rb_shapes), ctypes.byref(other.rb_bodies),
-                                    ctypes.byref(other.caps), ctypes.byref(W.make_rb_params(W.params_from_vector(big["params"]))),
-                                    ctypes.byref(other.rb_outputs), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)),
+                                    ctypes.byref(other.caps), ctypes.byref(big_params), ctypes.byref(other.rb_outputs),
+                                    ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)),
                 "rb_step_noalloc")
-    torch.cuda.synchronize()
-    assert other.n_contacts_total() > 0
+        torch.cuda.synchronize()
+        assert int(other.t_status[0].item()) == 0 and other.n_contacts_total() > 0
 
     for _ in range(2):
         with_ws.t_status.zero_()
