@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batch1024", choices=["batch1024", "mixed4096", "boxes64", "tower32"])
-    ap.add_argument("--shapes", default="pool", choices=["pool", "per-body"],
+    ap.add_argument("--shapes", default="per-body", choices=["pool", "per-body"],
                     help="batch1024: sizes from a shared pool of 64 + 64 shapes, or a shape and SDF per body")
     ap.add_argument("--scheme", default="rigid_gauss_seidel")
     ap.add_argument("--termination", default="residual_fixed_r", choices=["residual_fixed_r", "residual", "merit"])
@@ -696,7 +696,7 @@ def run_ours(args):
         t0 = time.perf_counter()
         best, info = autotune.tune(world, rp_pre)
         tuning = dict(best, seconds=time.perf_counter() - t0, **info)
-    rps = {"mode": mk(prec, cap), "fp64": mk("fp64", cap), "prof": mk(prec, cap, True),
+    rps = {"mode": mk(prec, cap), "fp64": mk("fp64", cap), "prof": mk(prec, cap, True), "check": mk(prec, cap, 3),
            "mode100": mk(prec, pre_cap), "fp64_100": mk("fp64", pre_cap)}
     if tuning:
         from rainbow_b200 import autotune
@@ -716,6 +716,9 @@ def run_ours(args):
     phases = world.profile_times()
     stats = world.stats()
     u_m = world.state()[1]
+    restore()
+    world.step(rps["check"])               # the FP32 contact search checked against the FP64 search
+    stats_check = world.stats()
     restore()
     world.step(rps["fp64"])
     stats64 = world.stats()
@@ -815,10 +818,12 @@ def run_ours(args):
     lookups = sum(s.n_grid_lookups for s in stats)
     lookups32 = sum(s.n_grid_lookups32 for s in stats)
     equal["contact_search_decision_flips"] = {
-        "candidates": int(cand), "search_flips": int(sum(s.n_search_flips for s in stats)),
-        "accept_flips": int(sum(s.n_accept_flips for s in stats)),
-        "note": "profiled step: candidates whose FP32 search (seed, Frank-Wolfe choices, iterations) or acceptance "
-                "differs from the FP64 search on the same candidate"}
+        "candidates": int(cand), "search_flips": int(sum(s.n_search_flips for s in stats_check)),
+        "accept_flips": int(sum(s.n_accept_flips for s in stats_check)),
+        "fp32_lookups": int(lookups32), "fp64_lookups": int(lookups),
+        "note": "first step from the saved state: candidates whose FP32 search (seed, Frank-Wolfe choices, "
+                "iterations) or acceptance differs from the plain FP64 search on the same candidate; FP64 lookups "
+                "are the acceptance tests, the contact data and the near-ties decided in FP64"}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
@@ -842,9 +847,29 @@ def run_ours(args):
                        "per candidate triangle: 3 world vertices (72 B) + result record (64 B); 8 grid values per "
                        "signed distance lookup, 64 B on the FP64 grid and 32 B on the FP32 copy, lookups counted on "
                        "the device", "k_narrow",
-                       "gathers of 8 grid nodes per lookup; with the shape pool the grids are L2-resident")
+                       "gathers of 8 grid nodes per lookup; " + ("a grid per body: the gathers go to HBM"
+                                                                 if args.shapes == "per-body" and
+                                                                 args.workload == "batch1024"
+                                                                 else "with a shape pool the grids are L2-resident"))
     doms = {"solve": solve_roof, "contact_search": narrow_roof}
     dom = max(doms, key=lambda k: doms[k]["phase_ms"])
+
+    cpu = None
+    if rank == 0 and args.cpu_seconds > 0:
+        x0r, u0r = x0.reshape(-1, 7), u0.reshape(-1, 6)
+        states = {i: (x0r[world.scene_start[i]:world.scene_start[i + 1]], u0r[world.scene_start[i]:world.scene_start[i + 1]])
+                  for i in range(world.n_scenes)}
+        cv, info = cpu_baseline(arrays, args, cpu_pool_workers if world.n_scenes > 1 else 1, states=states,
+                                pre_cap=pre_cap)
+        cpu = dict(value=cv, unit="scene-steps/s", **info)
+
+    # the batch's device memory (with a grid per body ~48 GB) is released before the serving run admits scenes
+    # by its own memory budget
+    n_bodies_world = world.n_bodies
+    del world, arrays
+    import gc
+    gc.collect()
+    torch.cuda.empty_cache()
 
     serving_rep = None
     if args.serve_seconds > 0 and args.workload == "batch1024" and world_size == 1:
@@ -856,14 +881,6 @@ def run_ours(args):
         configs = {"C1": config_c1(dev, cpu=args.cpu_seconds > 0), "C2": config_c2(dev, args, flush),
                    "C4": config_c4(dev, steps=500, cap=pre_cap, tol=args.tolerance)}
 
-    cpu = None
-    if rank == 0 and args.cpu_seconds > 0:
-        x0r, u0r = x0.reshape(-1, 7), u0.reshape(-1, 6)
-        states = {i: (x0r[world.scene_start[i]:world.scene_start[i + 1]], u0r[world.scene_start[i]:world.scene_start[i + 1]])
-                  for i in range(world.n_scenes)}
-        cv, info = cpu_baseline(arrays, args, cpu_pool_workers if world.n_scenes > 1 else 1, states=states,
-                                pre_cap=pre_cap)
-        cpu = dict(value=cv, unit="scene-steps/s", **info)
 
     cfg.update({"scheme": args.scheme, "ordering": args.ordering, "termination": args.termination,
                 "tolerance": args.tolerance, "max_iterations": cap,

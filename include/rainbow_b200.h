@@ -164,7 +164,9 @@ typedef struct rb_params {
     int32_t scheme;               /* RB_SCHEME_* */
     int32_t termination;          /* RB_TERMINATE_* */
     double residual_tolerance;    /* used by RB_TERMINATE_RESIDUAL */
-    int32_t profiling;            /* nonzero: fill energies and residual histories */
+    int32_t profiling;            /* nonzero: phase times, energies and residual histories; bit 2 (value 2) also
+                                     checks the FP32 modes' contact search against the plain FP64 search
+                                     (rb_scene_stats.n_search_flips / n_accept_flips) */
     double relaxation;            /* RB_TERMINATE_RESIDUAL_FIXED_R: r = relaxation / diag (over-relaxation of the
                                      projected Gauss-Seidel update; values <= 0 mean 1) */
     int32_t residual_interval;    /* RB_TERMINATE_RESIDUAL_FIXED_R: test the residual every this many sweeps
@@ -211,7 +213,7 @@ typedef struct rb_scene_stats {
     double max_penetration;       /* contacts.py:222 */
     double solve_start_us;        /* device clock (%globaltimer, microseconds) when the scene's solve started (profiling only) */
     double solve_us;              /* device time of the scene's contact solve, FP32 and FP64 phases (profiling only) */
-    int32_t n_search_flips;       /* FP32 contact search (profiling only): candidates whose seed, Frank-Wolfe vertex
+    int32_t n_search_flips;       /* FP32 contact search (profiling bit 2): candidates whose seed, Frank-Wolfe vertex
                                      choices or iteration count differ from the FP64 search's */
     int32_t n_accept_flips;       /* ... candidates the FP32 search accepts as a contact and the FP64 search does
                                      not, or the other way round */

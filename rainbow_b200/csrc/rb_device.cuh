@@ -216,39 +216,24 @@ __device__ __forceinline__ bool grid_is_inside(const GridView& g, d3 p, double b
     return true;
 }
 
-// FP32 copies of the lookups above for the contact search of the FP32 precision modes: the same cell choice,
-// interpolation and gradient expressions (the min_coord divisor included) on an FP32 copy of the grid
-struct GridView32 {
-    const float* values;
-    float mn[3], mx[3], sp[3];
-    int I, J, K;
-};
-__device__ __forceinline__ GridView32 load_grid32(const double* meta, const float* values) {
-    GridView32 g;
-    g.values = values;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) { g.mn[a] = (float)meta[a]; g.mx[a] = (float)meta[3 + a]; g.sp[a] = (float)meta[6 + a]; }
-    g.I = (int)meta[9]; g.J = (int)meta[10]; g.K = (int)meta[11];
-    return g;
-}
-__device__ __forceinline__ int cell_index32(float p, float mn, float sp, int n) {
-    const float f = floorf((p - mn) / sp);
-    const int lim = n - 2;
-    if (!(f >= 0.0f)) return 0;
-    if (f > (float)lim) return lim;
-    return (int)f;
-}
-__device__ __forceinline__ float3 grid_gradient32(const GridView32& g, float3 p) {
-    const int i = cell_index32(p.x, g.mn[0], g.sp[0], g.I);
-    const int j = cell_index32(p.y, g.mn[1], g.sp[1], g.J);
-    const int k = cell_index32(p.z, g.mn[2], g.sp[2], g.K);
+// Gradient from the FP32 copy of a grid (the contact search of the FP32 precision modes): the cell and the
+// fractions s, t, u in FP64 exactly as grid_gradient computes them (so the cell is always the FP64 lookup's,
+// grid3.py:107, and the min_coord divisor of :209-211 is kept), the eight corner values and their trilinear
+// combination in FP32.  err bounds the absolute difference of each component from grid_gradient's: the FP32
+// rounding of the values (at most 2^-24 |v|) and of the combination, amplified by the weights (1 - s, s) ...,
+// which the min_coord divisor can take outside [0, 1].
+__device__ __forceinline__ d3 grid_gradient_f32(const GridView& g, const float* values32, d3 p, double& err) {
+    const int i = cell_index(p.x, g.mn[0], g.sp[0], g.I);
+    const int j = cell_index(p.y, g.mn[1], g.sp[1], g.J);
+    const int k = cell_index(p.z, g.mn[2], g.sp[2], g.K);
     const int64_t I = g.I, IJ = (int64_t)g.I * g.J;
-    const float* v = g.values + i + I * j + IJ * k;
+    const float* v = values32 + i + I * j + IJ * k;
     const float d000 = __ldg(v), d100 = __ldg(v + 1), d010 = __ldg(v + I), d110 = __ldg(v + I + 1);
     const float d001 = __ldg(v + IJ), d101 = __ldg(v + IJ + 1), d011 = __ldg(v + IJ + I), d111 = __ldg(v + IJ + I + 1);
-    const float s = (p.x - ((float)i * g.sp[0] + g.mn[0])) / g.mn[0];
-    const float t = (p.y - ((float)j * g.sp[1] + g.mn[1])) / g.mn[1];
-    const float u = (p.z - ((float)k * g.sp[2] + g.mn[2])) / g.mn[2];
+    const double sd = (p.x - ((double)i * g.sp[0] + g.mn[0])) / g.mn[0];
+    const double td = (p.y - ((double)j * g.sp[1] + g.mn[1])) / g.mn[1];
+    const double ud = (p.z - ((double)k * g.sp[2] + g.mn[2])) / g.mn[2];
+    const float s = (float)sd, t = (float)td, u = (float)ud;
     const float x00 = (d100 - d000) * s + d000, x01 = (d101 - d001) * s + d001;
     const float x10 = (d110 - d010) * s + d010, x11 = (d111 - d011) * s + d011;
     const float y0 = (x10 - x00) * t + x00, y1 = (x11 - x01) * t + x01;
@@ -258,7 +243,12 @@ __device__ __forceinline__ float3 grid_gradient32(const GridView32& g, float3 p)
     const float dp_ds = (dy1_ds - dy0_ds) * u + dy0_ds;
     const float dp_dt = (dy1_dt - dy0_dt) * u + dy0_dt;
     const float dp_du = y1 - y0;
-    return make_float3(dp_ds * (1.0f / g.sp[0]), dp_dt * (1.0f / g.sp[1]), dp_du * (1.0f / g.sp[2]));
+    float vmax = fmaxf(fmaxf(fmaxf(fabsf(d000), fabsf(d100)), fmaxf(fabsf(d010), fabsf(d110))),
+                       fmaxf(fmaxf(fabsf(d001), fabsf(d101)), fmaxf(fabsf(d011), fabsf(d111))));
+    const double amp = (1.0 + 2.0 * fabs(sd)) * (1.0 + 2.0 * fabs(td)) * (1.0 + 2.0 * fabs(ud));
+    const double sp_min = fmin(g.sp[0], fmin(g.sp[1], g.sp[2]));
+    err = 64.0 * 5.9604644775390625e-8 * (double)vmax * amp / sp_min;   // 64 x 2^-24 x ...
+    return d3{(double)dp_ds * (1.0 / g.sp[0]), (double)dp_dt * (1.0 / g.sp[1]), (double)dp_du * (1.0 / g.sp[2])};
 }
 
 // NumPy np.add.reduceat over one segment: a[0] + pairwise_sum(a[1:]) (8 interleaved partial sums once the

@@ -537,42 +537,81 @@ __device__ __forceinline__ d3 fw_search64(const GridView& g, const d3* ps, int m
     return x;
 }
 
-// the same search in FP32 on the FP32 grid (the FP32 precision modes): the same decisions, FP32 arithmetic
-__device__ __forceinline__ float3 fw_search32(const GridView32& g, const float3* ps, int max_it, float tol, int& n_fw,
-                                              uint32_t& trace) {
-    float gn[3];
+// the same search with its lookups on the FP32 copy of the grid (the FP32 precision modes).  The point x and
+// the objectives stay FP64; a decision whose margin lies within the FP32 lookups' error bound (an exact tie of
+// coplanar corners, a near-tie, an objective next to the tolerance) is taken again on FP64 lookups, so every
+// decision, and x, equal fw_search64's.  l64 / l32 count the FP64 and FP32 lookups made.
+__device__ __forceinline__ d3 fw_search_f32(const GridView& g, const float* values32, const d3* ps, int max_it,
+                                            double tol, int& n_fw, uint32_t& trace, int& l64, int& l32) {
+    double scale = 0.0;   // max over corners of |p|_1: an objective's error is at most err x scale
+    for (int c = 0; c < 3; ++c) scale = fmax(scale, fabs(ps[c].x) + fabs(ps[c].y) + fabs(ps[c].z));
+    double gn[3], err = 0.0;
     for (int c = 0; c < 3; ++c) {
-        const float3 gr = grid_gradient32(g, ps[c]);
-        gn[c] = (gr.x * gr.x + gr.y * gr.y) + gr.z * gr.z;   // squared norms order the corners as the norms do
+        double e;
+        const d3 gr = grid_gradient_f32(g, values32, ps[c], e);
+        gn[c] = sqrt((gr.x * gr.x + gr.y * gr.y) + gr.z * gr.z);
+        err = fmax(err, e);
+    }
+    l32 += 3;
+    {   // a seed whose gradient norms lie within 2 sqrt(3) err of another's is chosen on FP64 lookups
+        const double lo = fmin(gn[0], fmin(gn[1], gn[2]));
+        int close = 0;
+        for (int c = 0; c < 3; ++c) close += gn[c] - lo <= 4.0 * 1.7320508075688772 * err;
+        if (close > 1) {
+            for (int c = 0; c < 3; ++c) {
+                const d3 gr = grid_gradient(g, ps[c]);
+                gn[c] = sqrt((gr.x * gr.x + gr.y * gr.y) + gr.z * gr.z);
+            }
+            l64 += 3;
+        }
     }
     int best = 0;
     if (gn[1] < gn[best]) best = 1;
     if (gn[2] < gn[best]) best = 2;
     trace = (uint32_t)best;
-    float3 x = best == 0 ? ps[0] : (best == 1 ? ps[1] : ps[2]);
+    d3 x = best == 0 ? ps[0] : (best == 1 ? ps[1] : ps[2]);
     n_fw = 0;
     for (int i = 0; i < max_it; ++i) {
         ++n_fw;
-        const float3 gr = grid_gradient32(g, x);
-        const float o0 = fmaf(ps[0].z, gr.z, fmaf(ps[0].y, gr.y, ps[0].x * gr.x));
-        const float o1 = fmaf(ps[1].z, gr.z, fmaf(ps[1].y, gr.y, ps[1].x * gr.x));
-        const float o2 = fmaf(ps[2].z, gr.z, fmaf(ps[2].y, gr.y, ps[2].x * gr.x));
+        double e;
+        d3 gr = grid_gradient_f32(g, values32, x, e);
+        ++l32;
+        double o0 = dot3_np(ps[0], gr), o1 = dot3_np(ps[1], gr), o2 = dot3_np(ps[2], gr);
+        const double margin = 4.0 * e * scale;
+        const double lo = fmin(o0, fmin(o1, o2));
+        const int close = (o0 - lo <= margin) + (o1 - lo <= margin) + (o2 - lo <= margin);
+        if (close > 1 || fabs(lo - tol) <= margin) {   // decide on the FP64 gradient
+            gr = grid_gradient(g, x);
+            ++l64;
+            o0 = dot3_np(ps[0], gr); o1 = dot3_np(ps[1], gr); o2 = dot3_np(ps[2], gr);
+        }
         int v = 0;
-        float ov = o0;
+        double ov = o0;
         if (o1 < ov) { v = 1; ov = o1; }
         if (o2 < ov) { v = 2; ov = o2; }
         if (i < 15) trace |= (uint32_t)v << (2 + 2 * i);
-        const float alpha = 2.0f / (float)(i + 2);
-        const float3 s = v == 0 ? ps[0] : (v == 1 ? ps[1] : ps[2]);
-        x = make_float3(fmaf(alpha, s.x - x.x, x.x), fmaf(alpha, s.y - x.y, x.y), fmaf(alpha, s.z - x.z, x.z));
+        const double alpha = 2.0 / (double)(i + 2);
+        const d3 s = v == 0 ? ps[0] : (v == 1 ? ps[1] : ps[2]);
+        x = d3{x.x + alpha * (s.x - x.x), x.y + alpha * (s.y - x.y), x.z + alpha * (s.z - x.z)};
         if (ov > tol) break;
     }
     return x;
 }
 
-// kF32: the seed and Frank-Wolfe lookups on the FP32 grid copy; the acceptance tests (is_inside, phi <=
-// envelope) and the contact's point, normal and gap in FP64 at the point found.  A profiled step also runs
-// the FP64 search and counts, per scene, the candidates whose search decisions or acceptance differ.
+// the plain FP64 search's trace and acceptance for a profiled step's check of the FP32 search (a call of its
+// own, so that it does not raise the registers of the search itself)
+__device__ __noinline__ void fw_check64(const GridView& g, const d3* ps, const double* qB, int max_it, double tol,
+                                        double envelope, int& n64, uint32_t& trace64, int& accept64) {
+    const d3 x64 = fw_search64(g, ps, max_it, tol, n64, trace64);
+    accept64 = 0;
+    if (grid_is_inside(g, x64, 0.5) && grid_value(g, x64) <= envelope)
+        accept64 = norm3_np(quat_rotate(qB, grid_gradient(g, x64))) > 0.0;
+}
+
+// kF32: the seed and Frank-Wolfe lookups on the FP32 grid copy (near-ties decided on FP64 lookups); the
+// acceptance tests (is_inside, phi <= envelope) and the contact's point, normal and gap in FP64 at the point
+// found.  A step profiled with bit 2 set also runs the plain FP64 search and counts, per scene, the candidates
+// whose search decisions or acceptance differ (a check of the error bound: zero when it holds).
 template <bool kF32>
 __global__ void __launch_bounds__(256, 2) k_narrow(const StepArgs a) {
     if (a.ws.counters[kAbort]) return;
@@ -603,13 +642,7 @@ __global__ void __launch_bounds__(256, 2) k_narrow(const StepArgs a) {
         uint32_t trace = 0u;
         d3 x;
         if (kF32) {
-            const GridView32 g32 = load_grid32(a.sh.grid_meta + 12 * ss, a.sh.grid32 + a.sh.g_off[ss]);
-            const float3 ps32[3] = {make_float3((float)ps[0].x, (float)ps[0].y, (float)ps[0].z),
-                                    make_float3((float)ps[1].x, (float)ps[1].y, (float)ps[1].z),
-                                    make_float3((float)ps[2].x, (float)ps[2].y, (float)ps[2].z)};
-            const float3 x32 = fw_search32(g32, ps32, max_it, (float)tol, n_fw, trace);
-            x = d3{(double)x32.x, (double)x32.y, (double)x32.z};
-            lookups32 = 3 + n_fw;
+            x = fw_search_f32(g, a.sh.grid32 + a.sh.g_off[ss], ps, max_it, tol, n_fw, trace, lookups, lookups32);
         } else {
             x = fw_search64(g, ps, max_it, tol, n_fw, trace);
             lookups = 3 + n_fw;   // seed gradients + one gradient per Frank-Wolfe iteration
@@ -638,14 +671,11 @@ __global__ void __launch_bounds__(256, 2) k_narrow(const StepArgs a) {
         if (a.pr.profiling) {   // statistics for the bandwidth accounting (lookups per scene) and decision flips
             const int s = scene_of(a.bd.scene_start, a.bd.n_scenes, A);
             atomicAdd(&a.out.stats[s].n_grid_lookups, lookups);
-            if (kF32) {
-                atomicAdd(&a.out.stats[s].n_grid_lookups32, lookups32);
-                int n64 = 0;
+            if (kF32) atomicAdd(&a.out.stats[s].n_grid_lookups32, lookups32);
+            if (kF32 && (a.pr.profiling & 2)) {   // the check against the plain FP64 search, on request
+                int n64 = 0, accept64 = 0;
                 uint32_t trace64 = 0u;
-                const d3 x64 = fw_search64(g, ps, max_it, tol, n64, trace64);
-                int accept64 = 0;
-                if (grid_is_inside(g, x64, 0.5) && grid_value(g, x64) <= envelope)
-                    accept64 = norm3_np(quat_rotate(qB, grid_gradient(g, x64))) > 0.0;
+                fw_check64(g, ps, qB, max_it, tol, envelope, n64, trace64, accept64);
                 if (n64 != n_fw || trace64 != trace) atomicAdd(&a.out.stats[s].n_search_flips, 1);
                 if (accept64 != flag) atomicAdd(&a.out.stats[s].n_accept_flips, 1);
             }

@@ -57,7 +57,7 @@ def make_rb_params(p, dt=None, scheme="rigid_gauss_seidel", termination="merit",
     rp.termination = {"merit": N.TERMINATE_MERIT, "residual": N.TERMINATE_RESIDUAL,
                       "residual_fixed_r": N.TERMINATE_RESIDUAL_FIXED_R}[termination]
     rp.residual_tolerance = float(residual_tolerance)
-    rp.profiling = int(bool(profiling))
+    rp.profiling = int(profiling)   # bit 2 (value 2): also check the FP32 contact search against the FP64 one
     rp.warm_start = int(bool(warm_start))
     rp.residual_interval = int(residual_interval)
     rp.relaxation = float(relaxation)

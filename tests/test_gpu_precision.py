@@ -102,41 +102,31 @@ def test_fp32_solve_of_scenes_whose_rows_live_in_l2():
         assert s32[i].residual <= 2.0 * s64[i].residual + 1e-6
 
 
-def test_fp32_contact_search_reports_its_decision_flips():
-    """The FP32 modes run the contact search's lookups on the FP32 grid copy and accept contacts in FP64 at the
-    point found.  On 16 scenes of the batched workload after a 20-step pre-roll, a profiled step counts the
-    candidates whose search decisions or acceptance differ from the FP64 search: few of them, and in scenes
-    without a flip the contacts of both searches lie within 1e-5 m of each other."""
+def test_fp32_contact_search_finds_the_fp64_contacts():
+    """The FP32 modes run the contact search's lookups on the FP32 grid copy, decide near-ties (exact ties of
+    coplanar box corners included) on FP64 lookups and accept contacts in FP64.  On 16 scenes of the batched
+    workload after a 20-step pre-roll, a profiled step finds exactly the FP64 step's contacts (ids, points,
+    normals, gaps), most of its lookups are FP32, and the self-check against the plain FP64 search counts no
+    flipped decision."""
     from rainbow_b200 import scenes
     from rainbow_b200 import world as W
     arrays, params = scenes.batch_arrays(n_scenes=16, seed=0, pool=64, resolution=32, device="cuda:0")
     w = W.DeviceWorld(arrays, max_iterations=100)
-    kw = dict(termination="residual_fixed_r", residual_tolerance=1e-6, residual_interval=4, profiling=True)
+    kw = dict(termination="residual_fixed_r", residual_tolerance=1e-6, residual_interval=4)
     for _ in range(20):
-        w.step(W.make_rb_params(params, **dict(kw, profiling=False)))
+        w.step(W.make_rb_params(params, **kw))
     x0, u0 = w.state()
     out = {}
     for mode in ("fp64", "fp32_refine"):
         w.set_state(x0, u0)
-        w.step(W.make_rb_params(params, precision=mode, **kw))
+        w.step(W.make_rb_params(params, precision=mode, profiling=3, **kw))
         out[mode] = (w.stats(), w.contacts())
     (s64, c64), (s32, c32) = out["fp64"], out["fp32_refine"]
-    cand = sum(s.n_candidates for s in s32)
-    assert cand > 0 and sum(s.n_grid_lookups32 for s in s32) > 0 and sum(s.n_grid_lookups32 for s in s64) == 0
-    search = sum(s.n_search_flips for s in s32)
-    accept = sum(s.n_accept_flips for s in s32)
-    assert search <= 0.05 * cand and accept <= 0.01 * cand, (search, accept, cand)
-    assert sum(s.n_search_flips + s.n_accept_flips for s in s64) == 0
-    checked = 0
-    for a, b in zip(s64, s32):
-        if a.n_contacts != b.n_contacts or a.n_contacts == 0 or b.n_search_flips or b.n_accept_flips:
-            continue
-        ka, kb = slice(a.contact_start, a.contact_start + a.n_contacts), slice(b.contact_start, b.contact_start + b.n_contacts)
-        if not np.array_equal(c64["ids"][ka], c32["ids"][kb]):
-            continue
-        assert np.abs(c64["p"][ka] - c32["p"][kb]).max() <= 1e-5
-        checked += 1
-    assert checked >= 8
+    for key in ("ids", "p", "n", "g"):
+        np.testing.assert_array_equal(c32[key], c64[key], err_msg=key)
+    l32, l64 = sum(s.n_grid_lookups32 for s in s32), sum(s.n_grid_lookups for s in s32)
+    assert sum(s.n_grid_lookups32 for s in s64) == 0 and l32 > l64
+    assert sum(s.n_search_flips + s.n_accept_flips for s in s32) == 0
 
 
 @pytest.mark.parametrize("scheme", ["parallel_jacobi", "parallel_jacobi_hybrid"])
