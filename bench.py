@@ -43,9 +43,14 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM bytes per launch of the dominant kernels, from ncu captures of this build (see the profile summaries):
-# kernel -> (bytes, workload the capture ran on)
-PROFILED_DRAM_BYTES = {}
+# DRAM bytes of a phase's kernels per step, from ncu captures of this build (dram__bytes_read.sum +
+# dram__bytes_write.sum), keyed by the phase's kernel and the (workload, precision, sweep cap) they hold for.
+# k_solve_fp32: 8.8 MB for the four size-class launches of one step of the first 128 scenes (3343 contacts),
+# scaled by contacts to the 1024-scene step (83,158 contacts): the traffic is the per-contact copy-in, the FP64
+# corrections and the write-back, all proportional to the contacts.
+PROFILED_DRAM_BYTES = {
+    "k_solve_fp32": (219_000_000, ("batch_1024_scenes", "fp32_refine", 4000)),
+}
 EQUAL_RESIDUAL_SWEEPS = 4000   # default sweep cap of the equal-residual measurement
 
 
@@ -93,12 +98,20 @@ def parse():
 # --------------------------------------------------------------------------------------------------------------
 # workloads
 # --------------------------------------------------------------------------------------------------------------
-def build_workload(name, device, n_scenes=1024, shapes="pool"):
+def build_workload(name, device, n_scenes=1024, shapes="pool", select=None):
+    """The workload's scene arrays (for batch1024 only the scenes in `select`, when given)."""
     from rainbow_b200 import engine_io, scenes
     if name == "batch1024":
         pool = 64 if shapes == "pool" else None
-        arrays, params = scenes.batch_arrays(n_scenes=n_scenes, seed=0, pool=pool, resolution=32, device=device)
-        bodies = sum(len(a["body_mass"]) for a in arrays)
+        if pool is None:
+            arrays, params = scenes.batch_arrays_per_body(n_scenes=n_scenes, seed=0, resolution=32, device=device,
+                                                          select=select)
+            bodies = sum(scenes.per_body_counts(n_scenes, 0))
+        else:
+            arrays, params = scenes.batch_arrays(n_scenes=n_scenes, seed=0, pool=pool, resolution=32, device=device)
+            bodies = sum(len(a["body_mass"]) for a in arrays)
+            if select is not None:
+                arrays = [arrays[i] for i in select]
         cfg = {"workload": "batch_%d_scenes" % n_scenes, "scenes": n_scenes, "bodies": int(bodies),
                "bodies_per_scene": "8..256",
                "shapes": ("boxes side U(0.5,2), spheres r U(0.25,1) 16x16, "
@@ -665,11 +678,18 @@ def run_ours(args):
     from rainbow_b200 import world as W
     from rainbow_b200.sharding import max_over_ranks, partition_scenes, sum_over_ranks
     if world_size > 1 and args.workload == "batch1024":
-        # weak scaling: world_size x --scenes scenes, split by body count so every GPU holds --scenes of them
-        arrays, params, cfg, engine = build_workload(args.workload, dev, args.scenes * world_size, args.shapes)
-        parts = partition_scenes([len(a["body_mass"]) for a in arrays], world_size)
-        arrays = [arrays[i] for i in parts[rank]]
-        cfg.update({"scenes_per_gpu": len(arrays), "scenes": args.scenes * world_size})
+        # weak scaling: world_size x --scenes scenes, split by body count so every GPU holds --scenes of them;
+        # each rank builds only its own share (the body counts come from the seeded draws alone)
+        from rainbow_b200 import scenes as SC
+        n_all = args.scenes * world_size
+        if args.shapes == "per-body":
+            counts = SC.per_body_counts(n_all, 0)
+        else:
+            counts = [len(a["body_mass"]) for a in SC.batch_arrays(n_scenes=n_all, seed=0, pool=64, resolution=32,
+                                                                   device=dev)[0]]
+        parts = partition_scenes(counts, world_size)
+        arrays, params, cfg, engine = build_workload(args.workload, dev, n_all, args.shapes, select=parts[rank])
+        cfg.update({"scenes_per_gpu": len(arrays), "scenes": n_all})
     else:
         arrays, params, cfg, engine = build_workload(args.workload, dev, args.scenes, args.shapes)
     pre_cap = int(params.max_iterations)      # the configuration's own iteration limit (100)

@@ -250,7 +250,26 @@ def batch_arrays(n_scenes=1024, seed=0, pool=64, body_range=(8, 256), resolution
     return out, params
 
 
-def batch_arrays_per_body(n_scenes=1024, seed=0, body_range=(8, 256), resolution=32, device="cuda", ground=24.0):
+def _per_body_draws(rng, lo, hi):
+    """One scene's draws of the per-body workload: body count, kinds, sizes, orientations, friction."""
+    n = int(round(np.exp(rng.uniform(lo, hi))))
+    kinds = rng.integers(0, 2, n)
+    sizes = np.where(kinds == 0, rng.uniform(0.5, 2.0, n), rng.uniform(0.25, 1.0, n))
+    quats = rng.normal(size=(n, 4))
+    quats /= np.linalg.norm(quats, axis=1, keepdims=True)
+    mu = rng.uniform(0.2, 0.8)
+    return n, kinds, sizes, quats, mu
+
+
+def per_body_counts(n_scenes=1024, seed=0, body_range=(8, 256)):
+    """Bodies (ground included) of each scene of :func:`batch_arrays_per_body`, without building anything."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(body_range[0]), np.log(body_range[1])
+    return [_per_body_draws(rng, lo, hi)[0] + 1 for _ in range(n_scenes)]
+
+
+def batch_arrays_per_body(n_scenes=1024, seed=0, body_range=(8, 256), resolution=32, device="cuda", ground=24.0,
+                          select=None):
     """The batched workload with a shape and signed distance grid of its own for every body: body counts,
     kinds (box or sphere), sizes (box side U(0.5, 2), sphere radius U(0.25, 1)), orientations and friction
     drawn per scene from ``seed``.  A body's shape is the unit box (side 1) or unit sphere (radius 1, 16 x 16
@@ -259,7 +278,8 @@ def batch_arrays_per_body(n_scenes=1024, seed=0, body_range=(8, 256), resolution
     max(0.1 x longest side, 2 x envelope), ``resolution`` nodes per axis) is computed on the device from its
     own mesh.  All grids live in one device tensor; each scene's ``shape_grid`` is a view of it (its ground's
     grid first, then its bodies' in body order), so nothing of the ~18.8 GB (73k grids of 32^3 doubles) passes
-    through host memory."""
+    through host memory.  ``select``: build only these scene indices (every scene's draws are still made, so a
+    scene is the same whichever others are built; ranks of a multi-GPU run build their own share)."""
     from . import geometry as GEO
     from .types import Grid, Parameters
     from .world import PARAM_FIELDS
@@ -276,13 +296,11 @@ def batch_arrays_per_body(n_scenes=1024, seed=0, body_range=(8, 256), resolution
     pvec = np.array([float(getattr(params, f)) for f in PARAM_FIELDS])
     lo, hi = np.log(body_range[0]), np.log(body_range[1])
     V_list, T_list, metas, plans = [], [], [], []
+    wanted = set(range(n_scenes)) if select is None else set(int(i) for i in select)
     for si in range(n_scenes):
-        n = int(round(np.exp(rng.uniform(lo, hi))))
-        kinds = rng.integers(0, 2, n)
-        sizes = np.where(kinds == 0, rng.uniform(0.5, 2.0, n), rng.uniform(0.25, 1.0, n))
-        quats = rng.normal(size=(n, 4))
-        quats /= np.linalg.norm(quats, axis=1, keepdims=True)
-        mu = rng.uniform(0.2, 0.8)
+        n, kinds, sizes, quats, mu = _per_body_draws(rng, lo, hi)
+        if si not in wanted:
+            continue
         V_list.append(g["V"]); T_list.append(g["T"]); metas.append(g["meta"])
         for b in range(n):
             u, sz = unit[kinds[b]], float(sizes[b])
@@ -292,11 +310,11 @@ def batch_arrays_per_body(n_scenes=1024, seed=0, body_range=(8, 256), resolution
             T_list.append(u["T"])
             metas.append(Grid(Vb.min(axis=0) - boundary, Vb.max(axis=0) + boundary, resolution, resolution,
                               resolution).meta())
-        plans.append((n, kinds, sizes, quats, mu))
+        plans.append((si, n, kinds, sizes, quats, mu))
     values, g_off = GEO.signed_distance_grids(V_list, T_list, metas, device=device)
     out = []
     shape0 = 0
-    for si, (n, kinds, sizes, quats, mu) in enumerate(plans):
+    for si, n, kinds, sizes, quats, mu in plans:
         sh = slice(shape0, shape0 + n + 1)
         Vs, Ts = V_list[sh], T_list[sh]
         side = int(np.ceil(n ** (1.0 / 3.0)))

@@ -91,3 +91,18 @@ def test_per_body_workload_steps_like_the_oracle(oracle_lib):
             b0, b1 = world.scene_start[i], world.scene_start[i + 1]
             np.testing.assert_array_equal(x[b0:b1].ravel(), o["x"], err_msg="step %d scene %d" % (s, i))
             np.testing.assert_array_equal(u[b0:b1].ravel(), o["u"], err_msg="step %d scene %d" % (s, i))
+
+
+def test_per_body_scenes_do_not_depend_on_which_others_are_built():
+    """A multi-GPU rank builds only its share of the per-body workload: a selected scene's arrays (shapes,
+    grids, bodies) equal the same scene built with all the others, and the counts without building match."""
+    from rainbow_b200 import scenes
+    every, _ = scenes.batch_arrays_per_body(n_scenes=5, seed=2, body_range=(8, 16), resolution=8, device="cuda:0")
+    some, _ = scenes.batch_arrays_per_body(n_scenes=5, seed=2, body_range=(8, 16), resolution=8, device="cuda:0",
+                                           select=[1, 4])
+    assert [len(a["body_mass"]) for a in every] == scenes.per_body_counts(5, 2, (8, 16))
+    for a, b in zip([every[1], every[4]], some):
+        for k in a:
+            va = a[k].cpu().numpy() if hasattr(a[k], "cpu") else np.asarray(a[k])
+            vb = b[k].cpu().numpy() if hasattr(b[k], "cpu") else np.asarray(b[k])
+            np.testing.assert_array_equal(va, vb, err_msg=k)
