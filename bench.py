@@ -45,11 +45,14 @@ sys.path.insert(0, ROOT)
 
 # DRAM bytes of a phase's kernels per step, from ncu captures of this build (dram__bytes_read.sum +
 # dram__bytes_write.sum), keyed by the phase's kernel and the (workload, precision, sweep cap) they hold for.
-# k_solve_fp32: 8.8 MB for the four size-class launches of one step of the first 128 scenes (3343 contacts),
-# scaled by contacts to the 1024-scene step (83,158 contacts): the traffic is the per-contact copy-in, the FP64
+# k_solve_fp32: 6.22 MB for the four size-class launches of one step of the first 128 scenes (2624 contacts),
+# scaled by contacts to the 1024-scene step (78,787 contacts): the traffic is the per-contact copy-in, the FP64
 # corrections and the write-back, all proportional to the contacts.
+# k_narrow: 66.1 MB for one launch on the first 128 scenes (152,968 candidates) with a grid per body, scaled by
+# candidates to the 1024-scene step (4,374,974 candidates).
 PROFILED_DRAM_BYTES = {
-    "k_solve_fp32": (219_000_000, ("batch_1024_scenes", "fp32_refine", 4000)),
+    "k_solve_fp32": (187_000_000, ("batch_1024_scenes_shape_per_body", "fp32_refine", 4000)),
+    "k_narrow": (1_890_000_000, ("batch_1024_scenes_shape_per_body", "fp32_refine", 4000)),
 }
 EQUAL_RESIDUAL_SWEEPS = 4000   # default sweep cap of the equal-residual measurement
 
@@ -112,7 +115,8 @@ def build_workload(name, device, n_scenes=1024, shapes="pool", select=None):
             bodies = sum(len(a["body_mass"]) for a in arrays)
             if select is not None:
                 arrays = [arrays[i] for i in select]
-        cfg = {"workload": "batch_%d_scenes" % n_scenes, "scenes": n_scenes, "bodies": int(bodies),
+        cfg = {"workload": "batch_%d_scenes_%s" % (n_scenes, "shape_pool" if pool else "shape_per_body"),
+               "scenes": n_scenes, "bodies": int(bodies),
                "bodies_per_scene": "8..256",
                "shapes": ("boxes side U(0.5,2), spheres r U(0.25,1) 16x16, "
                           + ("sizes from a pool of 64+64 shapes" if pool else "a shape and SDF per body")),

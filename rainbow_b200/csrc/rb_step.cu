@@ -2125,6 +2125,96 @@ __device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, 
     }
 }
 
+// The same Gauss-Seidel sweep with one lane per contact: the lane loads the contact's twelve row groups,
+// computes the four rows' J w as independent chains, applies the prox and updates both bodies.  A warp takes
+// 32 contacts of a level per pass instead of 8, and no shuffle lies on the chain.  Every expression is the
+// four-lane sweep's (the same operands, the same fmaf order), so both give the same bits.
+template <class G, bool kL2>
+__device__ __forceinline__ void s32_sweep_lane(const G& g, const S32Scene& f, int L, float rscale, bool bodies_global) {
+    int start = f.lptr[0], end = f.lptr[1];
+    for (int l = 1; l <= L; ++l) {
+        const int next_end = l < L ? f.lptr[l + 1] : end;
+        if (kL2) {   // rows in L2: pull the next level's rows (contiguous in level order) into L1 meanwhile
+            const char* p0 = reinterpret_cast<const char*>(f.c + kS32Floats * (size_t)end);
+            const int lines = (int)(((size_t)(next_end - end) * kS32Floats * sizeof(float) + 127) / 128);
+            for (int t = g.rank(); t < lines; t += g.size())
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(p0 + 128 * (size_t)t));
+            if (bodies_global)
+                for (int i = end + g.rank(); i < next_end; i += g.size()) {
+                    const uint32_t lh = f.lohi[i];
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(f.body + kS32BodyFloats * (size_t)(lh & 0xffffu)));
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(f.body + kS32BodyFloats * (size_t)(lh >> 16)));
+                }
+        }
+        for (int i = start + g.rank(); i < end; i += g.size()) {
+            const float4* C4 = reinterpret_cast<const float4*>(f.c + kS32Floats * i);
+            const uint32_t lh = f.lohi[i];
+            float* Bl = f.body + kS32BodyFloats * (int)(lh & 0xffffu);
+            float* Bh = f.body + kS32BodyFloats * (int)(lh >> 16);
+            float4 R[12];
+            for (int k = 0; k < 12; ++k) R[k] = C4[k];
+            const float4 l0 = *reinterpret_cast<const float4*>(Bl), l1 = *reinterpret_cast<const float4*>(Bl + 4);
+            const float4 h0 = *reinterpret_cast<const float4*>(Bh), h1 = *reinterpret_cast<const float4*>(Bh + 4);
+            float z[4];
+            for (int q = 0; q < 4; ++q) {
+                const float4 r0 = R[3 * q], r1 = R[3 * q + 1], r2 = R[3 * q + 2];
+                float lin = fmaf(r0.x, l0.x - h0.x, fmaf(r0.y, l0.y - h0.y, r0.z * (l0.z - h0.z)));
+                if (q == 3) lin = 0.0f;
+                const float alo = fmaf(r1.x, l0.w, fmaf(r1.y, l1.x, r1.z * l1.y));
+                const float ahi = fmaf(r2.x, h0.w, fmaf(r2.y, h1.x, r2.z * h1.y));
+                z[q] = r2.w - rscale * r1.w * (((lin + alo) + ahi) + r0.w);
+            }
+            const float mu = R[9].x;
+            const float xn = fmaxf(z[0], 0.0f);
+            const float radius = mu * xn;
+            const float sqr = fmaf(z[1], z[1], fmaf(z[2], z[2], z[3] * z[3]));
+            float scale = sqr > radius * radius ? radius * rsqrtf(sqr) : 1.0f;
+            if (xn <= 0.0f) scale = 0.0f;
+            const float f1 = z[1] * scale, f2 = z[2] * scale, f3 = z[3] * scale;
+            const float d0 = xn - R[2].w, d1 = f1 - R[5].w, d2 = f2 - R[8].w, d3 = f3 - R[11].w;
+            f.c[kS32Floats * i + 11] = xn;
+            f.c[kS32Floats * i + 23] = f1;
+            f.c[kS32Floats * i + 35] = f2;
+            f.c[kS32Floats * i + 47] = f3;
+            // the three sums of the update (the torsion row has no linear columns: d3 enters as 0 there)
+            const float L0 = fmaf(R[9].x, 0.0f, fmaf(R[6].x, d2, fmaf(R[3].x, d1, R[0].x * d0)));
+            const float L1 = fmaf(R[9].y, 0.0f, fmaf(R[6].y, d2, fmaf(R[3].y, d1, R[0].y * d0)));
+            const float L2 = fmaf(R[9].z, 0.0f, fmaf(R[6].z, d2, fmaf(R[3].z, d1, R[0].z * d0)));
+            const float A0 = fmaf(R[10].x, d3, fmaf(R[7].x, d2, fmaf(R[4].x, d1, R[1].x * d0)));
+            const float A1 = fmaf(R[10].y, d3, fmaf(R[7].y, d2, fmaf(R[4].y, d1, R[1].y * d0)));
+            const float A2 = fmaf(R[10].z, d3, fmaf(R[7].z, d2, fmaf(R[4].z, d1, R[1].z * d0)));
+            const float H0 = fmaf(R[11].x, d3, fmaf(R[8].x, d2, fmaf(R[5].x, d1, R[2].x * d0)));
+            const float H1 = fmaf(R[11].y, d3, fmaf(R[8].y, d2, fmaf(R[5].y, d1, R[2].y * d0)));
+            const float H2 = fmaf(R[11].z, d3, fmaf(R[8].z, d2, fmaf(R[5].z, d1, R[2].z * d0)));
+            if (l1.w == 0.0f) {   // lo body not fixed: +m^-1 on the linear sums, I_lo^-1 on the angular ones
+                const float m = l1.z;
+                const float4 I0 = *reinterpret_cast<const float4*>(Bl + 8);
+                const float2 I1 = *reinterpret_cast<const float2*>(Bl + 12);
+                Bl[0] = l0.x + fmaf(m, L0, fmaf(0.0f, L1, 0.0f * L2));
+                Bl[1] = l0.y + fmaf(0.0f, L0, fmaf(m, L1, 0.0f * L2));
+                Bl[2] = l0.z + fmaf(0.0f, L0, fmaf(0.0f, L1, m * L2));
+                Bl[3] = l0.w + fmaf(I0.x, A0, fmaf(I0.y, A1, I0.z * A2));
+                Bl[4] = l1.x + fmaf(I0.y, A0, fmaf(I0.w, A1, I1.x * A2));
+                Bl[5] = l1.y + fmaf(I0.z, A0, fmaf(I1.x, A1, I1.y * A2));
+            }
+            if (h1.w == 0.0f) {   // hi body: -m^-1 on the linear sums, I_hi^-1 on its angular ones
+                const float m = -h1.z;
+                const float4 I0 = *reinterpret_cast<const float4*>(Bh + 8);
+                const float2 I1 = *reinterpret_cast<const float2*>(Bh + 12);
+                Bh[0] = h0.x + fmaf(m, L0, fmaf(0.0f, L1, 0.0f * L2));
+                Bh[1] = h0.y + fmaf(0.0f, L0, fmaf(m, L1, 0.0f * L2));
+                Bh[2] = h0.z + fmaf(0.0f, L0, fmaf(0.0f, L1, m * L2));
+                Bh[3] = h0.w + fmaf(I0.x, H0, fmaf(I0.y, H1, I0.z * H2));
+                Bh[4] = h1.x + fmaf(I0.y, H0, fmaf(I0.w, H1, I1.x * H2));
+                Bh[5] = h1.y + fmaf(I0.z, H0, fmaf(I1.x, H1, I1.y * H2));
+            }
+        }
+        g.sync();
+        start = end;
+        end = next_end;
+    }
+}
+
 // One proximal Jacobi sweep (proximal_contact/jacobi_solver.py:41-57) on the FP32 copy: every contact's new
 // impulse from the accumulators w = W J^T x of the previous iterate, four lanes per contact as in the
 // Gauss-Seidel sweep (any order: no contact reads another's new impulse), then w rebuilt from the new
@@ -2375,7 +2465,11 @@ __global__ void __launch_bounds__(kL2 ? kFp32L2Block : kFp32BlockMax, 1) k_solve
             const int round_start = sweeps;
             while (res > tol && sweeps < budget) {
                 if (jacobi) s32_sweep_jacobi(g, R, f, rscale, hybrid);
+#ifdef RB_SWEEP_LANE
+                else s32_sweep_lane<G, kL2>(g, f, L, rscale, bodies_global);
+#else
                 else s32_sweep<G, kL2>(g, f, L, rscale, bodies_global);
+#endif
                 ++sweeps;
                 if (sweeps % interval == 0 || sweeps == budget) {
                     res = s32_residual(a, g, R, f);
