@@ -91,7 +91,7 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=20.0,
                     help="wall time of the serving run (Poisson arrivals, continuous batching); 0 skips it")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="request arrival rate (requests/s)")
-    ap.add_argument("--serve-max-bodies", type=int, default=131072,
+    ap.add_argument("--serve-max-bodies", type=int, default=393216,
                     help="resident-body cap of the server (its step-latency target)")
     ap.add_argument("--serve-templates", type=int, default=192, help="distinct scenes the requests draw from")
     ap.add_argument("--serve-plain-scenes", type=int, default=8)
@@ -569,9 +569,9 @@ def config_c1(dev, cpu=True):
 
 
 def config_c2(dev, args, flush):
-    """4097-body box/sphere lattice (SDF resolution 64), after a 30-step pre-roll: Gauss-Seidel FP64,
-    Gauss-Seidel FP32 + FP64 refinement and proximal Jacobi FP64, each for a few steps from the same state at
-    the equal-residual settings; error of each against Gauss-Seidel FP64 after the first step."""
+    """4097-body box/sphere lattice (SDF resolution 64), after a 30-step pre-roll: Gauss-Seidel and proximal
+    Jacobi, each in FP64 and in FP32 + FP64 refinement, for a few steps from the same state at the
+    equal-residual settings; error of each against Gauss-Seidel FP64 after the first step."""
     import torch
     from rainbow_b200 import engine_io, scenes, world as W
     arrays = engine_io.scene_arrays(scenes.mixed_lattice(n=16, spacing=1.2, resolution=64, seed=0, device=dev))
@@ -588,7 +588,7 @@ def config_c2(dev, args, flush):
     stream = torch.cuda.current_stream()
     arms = [("gauss_seidel_fp64", "rigid_gauss_seidel", "fp64"), ("gauss_seidel_fp32_refine", "rigid_gauss_seidel",
                                                                    "fp32_refine"),
-            ("jacobi_fp64", "parallel_jacobi", "fp64")]
+            ("jacobi_fp64", "parallel_jacobi", "fp64"), ("jacobi_fp32_refine", "parallel_jacobi", "fp32_refine")]
     out, u_ref = {}, None
     for name, scheme, prec in arms:
         rp = W.make_rb_params(params, scheme=scheme, precision=prec, **kw)

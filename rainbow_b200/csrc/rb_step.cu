@@ -2465,11 +2465,8 @@ __global__ void __launch_bounds__(kL2 ? kFp32L2Block : kFp32BlockMax, 1) k_solve
             const int round_start = sweeps;
             while (res > tol && sweeps < budget) {
                 if (jacobi) s32_sweep_jacobi(g, R, f, rscale, hybrid);
-#ifdef RB_SWEEP_LANE
-                else s32_sweep_lane<G, kL2>(g, f, L, rscale, bodies_global);
-#else
+                else if (!block_team) s32_sweep_lane<G, kL2>(g, f, L, rscale, bodies_global);
                 else s32_sweep<G, kL2>(g, f, L, rscale, bodies_global);
-#endif
                 ++sweeps;
                 if (sweeps % interval == 0 || sweeps == budget) {
                     res = s32_residual(a, g, R, f);
