@@ -12,7 +12,8 @@ work-list growth, the warm-start cache):
 * the 32-box tower with mass ratio 1e3 (dt 0.005) over 60 steps;
 * the 4096-body box/sphere lattice at SDF resolution 64;
 * a 2048-body scene of the serving workload (the top of its 16..2048 body range);
-* the 64-box lattice run freely for 100 steps with the reference's parameters.
+* the 64-box lattice run freely for 100 steps with the reference's parameters;
+* four scenes of the default benchmark workload, which gives every body a shape and grid of its own.
 
 Every compared step asserts equal contact ids, positions, normals, gaps, impulses, iteration counts, exit
 codes and body states.  The reference steps these scenes through steppers.py:47-106; the oracle restates that
@@ -142,3 +143,26 @@ def test_c1_free_run_100_steps_matches_oracle(oracle_lib):
         if s % 10 == 9:
             _check(world, o, 0, "C1 step %d" % s)
     assert o["n_contacts"] > 0
+
+
+def test_per_body_workload_scenes_match_oracle(oracle_lib):
+    """The default benchmark workload gives every body a shape and grid of its own.  Four of its scenes --
+    the largest of all 1024 (257 bodies) and three of the first twenty (179, 145 and 11 bodies) -- built alone
+    (the draws of the other scenes replayed, their shapes not built), batched together and stepped 20 steps
+    with the bench's FP64 settings: bit-identical to the oracle on host copies at every step."""
+    from rainbow_b200 import scenes, world as W
+    pick = [3, 9, 11, 419]
+    arrays, params = scenes.batch_arrays_per_body(n_scenes=1024, seed=0, resolution=32, device="cuda:0", select=pick)
+    assert sorted(len(a["body_mass"]) for a in arrays) == [11, 145, 179, 257]
+    host = [{k: (v.cpu().numpy() if hasattr(v, "cpu") else v) for k, v in a.items()} for a in arrays]
+    world = W.DeviceWorld(arrays, device="cuda:0", max_iterations=100)
+    ors = [oracle_lib.OracleScene(h) for h in host]
+    rp = _rb(params, True)
+    contacts = 0
+    for s in range(20):
+        assert world.step(rp) == 0
+        for i, sc in enumerate(ors):
+            o = sc.step(**BENCH_ORACLE)
+            contacts += o["n_contacts"]
+            _check(world, o, i, "per-body step %d scene %d" % (s, i))
+    assert contacts > 0
