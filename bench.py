@@ -85,6 +85,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     ap.add_argument("--cpu-scenes", type=int, default=64, help="scenes in the CPU baseline sample (stratified)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plugin", action="store_true",
+                    help="skip the e2e run through api.simulate_batch on engine objects")
     ap.add_argument("--no-autotune", action="store_true", help="keep the built-in launch shapes")
     ap.add_argument("--no-100", action="store_true", help="skip the 100-sweep block")
     ap.add_argument("--no-configs", action="store_true", help="skip the C1 / C2 / C4 sub-results")
@@ -447,6 +449,56 @@ def plain_arm(world, arrays, idx, x0, u0, cache, rp, steps, flush, max_it):
             "method": "scenes stratified by body count, each alone: one rb_step launch sequence per scene-step, "
                       "FP64, same solver settings, from the batch's state and warm-start cache (bit-identical to "
                       "the batch's FP64 step); graph_* = the same steps replayed from a CUDA graph per scene"}
+
+
+def plugin_arm(arrays, x0, u0, args, dev, flush, prec, warm, cap):
+    """The batch through the reference-style drop-in: one engine object per scene (grids kept on the device
+    as views of the workload's tensor), stepped by api.simulate_batch with a BatchStepper.  Every step reads
+    the bodies' r, q, v, w from the engine objects (host), uploads them, steps, and writes the new state and
+    each engine's contact points back into the objects.  Starts from the batch's saved state; the warm-start
+    cache fills during the warm-up steps."""
+    import torch
+    from rainbow_b200 import api as API, engine_io
+    from rainbow_b200.stepper import BatchStepper
+    t_build = time.perf_counter()
+    engines = [engine_io.engine_from_arrays(a) for a in arrays]
+    x0r, u0r = x0.reshape(-1, 7), u0.reshape(-1, 6)
+    k = 0
+    for e in engines:
+        e.params.proximal_solver = None if args.scheme == "rigid_gauss_seidel" else args.scheme
+        e.params.warm_start = warm
+        e.params.solver_precision = prec
+        e.params.contact_ordering = args.ordering
+        e.params.max_iterations = cap
+        for b in e.bodies.values():
+            b.r, b.q, b.v, b.w = x0r[k, :3].copy(), x0r[k, 3:].copy(), u0r[k, :3].copy(), u0r[k, 3:].copy()
+            k += 1
+    stepper = BatchStepper(device=dev, termination=args.termination, residual_tolerance=args.tolerance,
+                           residual_interval=args.residual_interval)
+    dt = engines[0].params.time_step
+    API.simulate_batch(engines, dt, stepper)       # builds the batch
+    t_build = time.perf_counter() - t_build
+    for _ in range(max(0, args.warmup - 1)):
+        API.simulate_batch(engines, dt, stepper)
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        API.simulate_batch(engines, dt, stepper)
+        times.append(time.perf_counter() - t0)
+    t = np.array(times)
+    nb = sum(len(e.bodies) for e in engines)
+    K = sum(len(e.contact_points) for e in engines)
+    out = {"value": len(engines) * len(t) / t.sum(), "unit": "scene-steps/s",
+           "p50_ms": float(np.percentile(t, 50) * 1e3), "p99_ms": float(np.percentile(t, 99) * 1e3),
+           "h2d_bytes_per_step": 13 * 8 * nb, "d2h_bytes_per_step": 13 * 8 * nb + 64 * K,
+           "engines": len(engines), "bodies": nb, "build_s": t_build,
+           "api": "api.simulate_batch(engines, dt, BatchStepper) over one engine object per scene: r, q, v, w read "
+                  "from and written back to every body, contact points per engine, every step"}
+    del stepper, engines
+    torch.cuda.empty_cache()
+    return out
 
 
 # --------------------------------------------------------------------------------------------------------------
@@ -832,6 +884,8 @@ def run_ours(args):
         el = max_over_ranks(el, dev)
         e2e = {"value": all_scenes * args.steps / el, "unit": "scene-steps/s",
                "h2d_bytes_per_step": 13 * 8 * world.n_bodies, "d2h_bytes_per_step": int(d2h), "api": api}
+        if engine is None and world_size == 1 and not args.no_plugin:
+            e2e["plugin"] = plugin_arm(arrays, x0, u0, args, dev, flush, prec, warm, cap)
 
     # rooflines of the profiled step's phases (event times on the launching stream)
     K = sum(s.n_contacts for s in stats)

@@ -13,7 +13,7 @@ host exactly as the reference API does, so scripts written against the reference
 import numpy as np
 
 from . import geometry as GEO
-from .stepper import GpuStepper
+from .stepper import BatchStepper, GpuStepper   # noqa: F401 (BatchStepper drives simulate_batch)
 from .types import Damping, Engine, Gravity, Hinge, RigidBody, Shape, SurfacesInteraction
 
 create_box = GEO.create_box
@@ -256,6 +256,23 @@ def simulate(engine, T, profiling_on=False):
     while T_left:
         dt = min(T_left, engine.params.time_step)
         engine.stepper.step(dt, engine, profiling_on)
+        T_left -= dt
+
+
+def simulate_batch(engines, T, stepper, profiling_on=False):
+    """Advance every engine by T, all of them in one batch per time step (the many-scene form of
+    :func:`simulate`, api.py:676): ``stepper`` is a :class:`rainbow_b200.stepper.BatchStepper`, and the
+    engines share ``params.time_step`` and the other step parameters."""
+    if T <= 0:
+        raise ValueError("Time must be positive")
+    engines = list(engines)
+    if not engines:
+        return
+    time_step = engines[0].params.time_step
+    T_left = T
+    while T_left:
+        dt = min(T_left, time_step)
+        stepper.step(dt, engines, profiling_on)
         T_left -= dt
 
 

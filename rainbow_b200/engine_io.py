@@ -18,17 +18,28 @@ def _force_kind(force):
     raise NotImplementedError("force type %r is not supported by the GPU stepper" % (kind,))
 
 
-def scene_arrays(engine, shape_cache=None):
-    """Flat arrays of one scene.  ``shape_cache`` (dict) reuses the packed arrays of unchanged shapes."""
+def _is_device_tensor(a):
+    return type(a).__module__.startswith("torch") and getattr(a, "is_cuda", False)
+
+
+def scene_arrays(engine):
+    """Flat arrays of one scene.  Grids held as CUDA tensors stay on the device (``shape_grid`` is then a
+    device tensor); everything else is a host array."""
     out = {}
     shapes = list(engine.shapes.values())
     shape_index = {id(s): i for i, s in enumerate(shapes)}
     Vs, Ts, Gs, meta = [], [], [], []
     v_off, t_off, g_off = [0], [0], [0]
+    on_device = False
     for s in shapes:
         V = np.ascontiguousarray(s.mesh.V, dtype=np.float64)
         T = np.ascontiguousarray(s.mesh.T, dtype=np.int32)
-        vals = np.ascontiguousarray(s.grid.values, dtype=np.float64).ravel()
+        vals = s.grid.values
+        if _is_device_tensor(vals):   # a grid built on (or kept on) the device stays there
+            vals = vals.reshape(-1)
+            on_device = True
+        else:
+            vals = np.ascontiguousarray(vals, dtype=np.float64).ravel()
         Vs.append(V)
         Ts.append(T)
         Gs.append(vals)
@@ -40,7 +51,13 @@ def scene_arrays(engine, shape_cache=None):
                                     [g.I, g.J, g.K]]).astype(np.float64))
     out["shape_V"] = np.concatenate(Vs) if Vs else np.zeros((0, 3))
     out["shape_T"] = np.concatenate(Ts) if Ts else np.zeros((0, 3), np.int32)
-    out["shape_grid"] = np.concatenate(Gs) if Gs else np.zeros(0)
+    if on_device:
+        import torch
+        dev = next(g.device for g in Gs if _is_device_tensor(g))
+        out["shape_grid"] = torch.cat([g.to(torch.float64) if _is_device_tensor(g) else
+                                       torch.from_numpy(g).to(dev) for g in Gs])
+    else:
+        out["shape_grid"] = np.concatenate(Gs) if Gs else np.zeros(0)
     out["shape_v_off"] = np.array(v_off, dtype=np.int64)
     out["shape_t_off"] = np.array(t_off, dtype=np.int64)
     out["shape_g_off"] = np.array(g_off, dtype=np.int64)
@@ -163,7 +180,10 @@ def engine_from_arrays(arrays, names=None):
         m = meta[k]
         g = TY.Grid(m[0:3], m[3:6], int(m[9]), int(m[10]), int(m[11]))
         g.spacing = m[6:9].copy()
-        g.values = np.asarray(a["shape_grid"]).ravel()[sg[k]:sg[k + 1]].copy()
+        if _is_device_tensor(a["shape_grid"]):   # grids built on the device: views of the one tensor
+            g.values = a["shape_grid"].reshape(-1)[sg[k]:sg[k + 1]]
+        else:
+            g.values = np.asarray(a["shape_grid"]).ravel()[sg[k]:sg[k + 1]].copy()
         s.grid = g
         engine.shapes[s.name] = s
         shape_objs.append(s)

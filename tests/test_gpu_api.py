@@ -68,3 +68,44 @@ def test_api_scene_matches_oracle(oracle_lib):
     np.testing.assert_array_equal(x.ravel(), o["x"])
     np.testing.assert_array_equal(u.ravel(), o["u"])
     assert o["n_contacts"] > 0
+
+
+def test_simulate_batch_matches_each_engine_stepped_alone():
+    """api.simulate_batch over three engines (random boxes and spheres on a ground; 6, 12 and 20 bodies) gives
+    every engine the body states and contact points that a GpuStepper of its own gives it through
+    api.simulate, bit for bit, also after one body's velocity is edited in place and another body's spin array
+    is replaced between two calls."""
+    from rainbow_b200 import api as API, scenes
+    from rainbow_b200.stepper import BatchStepper, GpuStepper
+
+    def make():
+        return [scenes.random_scene(n, np.random.default_rng(seed), resolution=16)
+                for n, seed in ((6, 1), (12, 2), (20, 3))]
+
+    def edit(engines):
+        list(engines[1].bodies.values())[2].v[1] += 0.5
+        list(engines[2].bodies.values())[3].w = np.array([0.0, 1.0, 0.0])
+
+    batch, alone = make(), make()
+    for e in alone:
+        e.stepper = GpuStepper()
+    stepper = BatchStepper()
+    dt = batch[0].params.time_step
+    contacts = 0
+    for k in range(8):
+        if k == 4:
+            edit(batch)
+            edit(alone)
+        API.simulate_batch(batch, dt, stepper)
+        for e in alone:
+            API.simulate(e, dt)
+        for eb, ea in zip(batch, alone):
+            for b1, b2 in zip(eb.bodies.values(), ea.bodies.values()):
+                for f in ("r", "q", "v", "w"):
+                    np.testing.assert_array_equal(getattr(b1, f), getattr(b2, f), err_msg="step %d %s" % (k, f))
+            for x1, x2 in zip(eb.contact_points.arrays(), ea.contact_points.arrays()):
+                np.testing.assert_array_equal(x1, x2)
+            assert ([(c.bodyA.name, c.bodyB.name) for c in eb.contact_points] ==
+                    [(c.bodyA.name, c.bodyB.name) for c in ea.contact_points])
+            contacts += len(eb.contact_points)
+    assert contacts > 0

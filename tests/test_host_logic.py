@@ -193,3 +193,21 @@ def test_mirror_api_builds_the_reference_scene(monkeypatch):
         ia, ib = ref.surfaces_interactions.get_interaction(*key), mine.surfaces_interactions.get_interaction(*key)
         np.testing.assert_array_equal(ib.mu, ia.mu)
         assert ib.epsilon == ia.epsilon
+
+
+def test_simulate_batch_refuses_engines_with_different_parameters():
+    """The batched drop-in steps engines that share the step's parameters; a differing one is named before any
+    device work (api.simulate_batch, BatchStepper)."""
+    from rainbow_b200 import api as A
+    from rainbow_b200.stepper import BatchStepper
+    a, b = (engine_io.engine_from_arrays(load_fixture("boxes8")) for _ in range(2))
+    b.params.time_step = 0.005
+    with pytest.raises(ValueError, match="time_step"):
+        A.simulate_batch([a, b], 0.01, BatchStepper())
+    b.params.time_step = a.params.time_step
+    b.params.solver_precision = "fp32_refine"
+    with pytest.raises(ValueError, match="solver_precision"):
+        A.simulate_batch([a, b], 0.01, BatchStepper())
+    with pytest.raises(ValueError):
+        A.simulate_batch([a, b], 0.0, BatchStepper())
+
