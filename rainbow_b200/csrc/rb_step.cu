@@ -1949,8 +1949,9 @@ __device__ __forceinline__ int s32_load(const StepArgs& a, const G& g, const Sce
         const double* Wi = a.ws.Winv + 9 * (size_t)b;
         B[6] = fx ? 0.0f : (float)(1.0 / a.bd.mass[b]);
         B[7] = fx ? 1.0f : 0.0f;
-        B[8] = (float)Wi[0]; B[9] = (float)Wi[1]; B[10] = (float)Wi[2];
-        B[11] = (float)Wi[4]; B[12] = (float)Wi[5]; B[13] = (float)Wi[8];
+        // a fixed body's update is zero (m^-1 = I^-1 = 0); the sweeps still only store to free bodies
+        B[8] = fx ? 0.0f : (float)Wi[0]; B[9] = fx ? 0.0f : (float)Wi[1]; B[10] = fx ? 0.0f : (float)Wi[2];
+        B[11] = fx ? 0.0f : (float)Wi[4]; B[12] = fx ? 0.0f : (float)Wi[5]; B[13] = fx ? 0.0f : (float)Wi[8];
     }
     g.sync();
     return L;
@@ -2094,18 +2095,20 @@ __device__ __forceinline__ void s32_sweep(const G& g, const S32Scene& f, int L, 
                 const float d3 = linear ? 0.0f : f3 - xo[3];   // the torsion row has no linear columns
                 const float xq = q == 0 ? xn : (q == 1 ? f1 : (q == 2 ? f2 : f3));
                 f.c[kS32Floats * i + 12 * q + 11] = xq;
-                const float S0 = fmaf(v[3].x, d3, fmaf(v[2].x, d2, fmaf(v[1].x, d1, v[0].x * d0)));
-                const float S1 = fmaf(v[3].y, d3, fmaf(v[2].y, d2, fmaf(v[1].y, d1, v[0].y * d0)));
-                const float S2 = fmaf(v[3].z, d3, fmaf(v[2].z, d2, fmaf(v[1].z, d1, v[0].z * d0)));
+                const float T0 = fmaf(v[2].x, d2, fmaf(v[1].x, d1, v[0].x * d0));
+                const float T1 = fmaf(v[2].y, d2, fmaf(v[1].y, d1, v[0].y * d0));
+                const float T2 = fmaf(v[2].z, d2, fmaf(v[1].z, d1, v[0].z * d0));
+                // the torsion row has no linear columns: linear lanes sum three rows
+                const float S0 = linear ? T0 : fmaf(v[3].x, d3, T0);
+                const float S1 = linear ? T1 : fmaf(v[3].y, d3, T1);
+                const float S2 = linear ? T2 : fmaf(v[3].z, d3, T2);
                 // the lane's body: w, m^-1 and fixed flag were loaded above
                 const float4 w0 = on_hi ? h0 : l0;
                 const float4 w1 = on_hi ? h1 : l1;
                 const float m = on_hi ? -w1.z : w1.z;
-                const float i0 = linear ? m : I0.x, i1 = linear ? 0.0f : I0.y, i2 = linear ? 0.0f : I0.z;
-                const float i3 = linear ? m : I0.w, i4 = linear ? 0.0f : I1.x, i5 = linear ? m : I1.y;
-                const float dw0 = fmaf(i0, S0, fmaf(i1, S1, i2 * S2));
-                const float dw1 = fmaf(i1, S0, fmaf(i3, S1, i4 * S2));
-                const float dw2 = fmaf(i2, S0, fmaf(i4, S1, i5 * S2));
+                const float dw0 = linear ? m * S0 : fmaf(I0.x, S0, fmaf(I0.y, S1, I0.z * S2));
+                const float dw1 = linear ? m * S1 : fmaf(I0.y, S0, fmaf(I0.w, S1, I1.x * S2));
+                const float dw2 = linear ? m * S2 : fmaf(I0.z, S0, fmaf(I1.x, S1, I1.y * S2));
                 // the lane's three components of w: linear (0-2) or angular (3-5), without a branch
                 const int off = linear ? 0 : 3;
                 const float o0 = linear ? w0.x : w0.w, o1 = linear ? w0.y : w1.x, o2 = linear ? w0.z : w1.y;
@@ -2176,38 +2179,33 @@ __device__ __forceinline__ void s32_sweep_lane(const G& g, const S32Scene& f, in
             f.c[kS32Floats * i + 23] = f1;
             f.c[kS32Floats * i + 35] = f2;
             f.c[kS32Floats * i + 47] = f3;
-            // the three sums of the update (the torsion row has no linear columns: d3 enters as 0 there)
-            const float L0 = fmaf(R[9].x, 0.0f, fmaf(R[6].x, d2, fmaf(R[3].x, d1, R[0].x * d0)));
-            const float L1 = fmaf(R[9].y, 0.0f, fmaf(R[6].y, d2, fmaf(R[3].y, d1, R[0].y * d0)));
-            const float L2 = fmaf(R[9].z, 0.0f, fmaf(R[6].z, d2, fmaf(R[3].z, d1, R[0].z * d0)));
+            // the three sums of the update (the torsion row has no linear columns)
+            const float L0 = fmaf(R[6].x, d2, fmaf(R[3].x, d1, R[0].x * d0));
+            const float L1 = fmaf(R[6].y, d2, fmaf(R[3].y, d1, R[0].y * d0));
+            const float L2 = fmaf(R[6].z, d2, fmaf(R[3].z, d1, R[0].z * d0));
             const float A0 = fmaf(R[10].x, d3, fmaf(R[7].x, d2, fmaf(R[4].x, d1, R[1].x * d0)));
             const float A1 = fmaf(R[10].y, d3, fmaf(R[7].y, d2, fmaf(R[4].y, d1, R[1].y * d0)));
             const float A2 = fmaf(R[10].z, d3, fmaf(R[7].z, d2, fmaf(R[4].z, d1, R[1].z * d0)));
             const float H0 = fmaf(R[11].x, d3, fmaf(R[8].x, d2, fmaf(R[5].x, d1, R[2].x * d0)));
             const float H1 = fmaf(R[11].y, d3, fmaf(R[8].y, d2, fmaf(R[5].y, d1, R[2].y * d0)));
             const float H2 = fmaf(R[11].z, d3, fmaf(R[8].z, d2, fmaf(R[5].z, d1, R[2].z * d0)));
-            if (l1.w == 0.0f) {   // lo body not fixed: +m^-1 on the linear sums, I_lo^-1 on the angular ones
-                const float m = l1.z;
-                const float4 I0 = *reinterpret_cast<const float4*>(Bl + 8);
-                const float2 I1 = *reinterpret_cast<const float2*>(Bl + 12);
-                Bl[0] = l0.x + fmaf(m, L0, fmaf(0.0f, L1, 0.0f * L2));
-                Bl[1] = l0.y + fmaf(0.0f, L0, fmaf(m, L1, 0.0f * L2));
-                Bl[2] = l0.z + fmaf(0.0f, L0, fmaf(0.0f, L1, m * L2));
-                Bl[3] = l0.w + fmaf(I0.x, A0, fmaf(I0.y, A1, I0.z * A2));
-                Bl[4] = l1.x + fmaf(I0.y, A0, fmaf(I0.w, A1, I1.x * A2));
-                Bl[5] = l1.y + fmaf(I0.z, A0, fmaf(I1.x, A1, I1.y * A2));
-            }
-            if (h1.w == 0.0f) {   // hi body: -m^-1 on the linear sums, I_hi^-1 on its angular ones
-                const float m = -h1.z;
-                const float4 I0 = *reinterpret_cast<const float4*>(Bh + 8);
-                const float2 I1 = *reinterpret_cast<const float2*>(Bh + 12);
-                Bh[0] = h0.x + fmaf(m, L0, fmaf(0.0f, L1, 0.0f * L2));
-                Bh[1] = h0.y + fmaf(0.0f, L0, fmaf(m, L1, 0.0f * L2));
-                Bh[2] = h0.z + fmaf(0.0f, L0, fmaf(0.0f, L1, m * L2));
-                Bh[3] = h0.w + fmaf(I0.x, H0, fmaf(I0.y, H1, I0.z * H2));
-                Bh[4] = h1.x + fmaf(I0.y, H0, fmaf(I0.w, H1, I1.x * H2));
-                Bh[5] = h1.y + fmaf(I0.z, H0, fmaf(I1.x, H1, I1.y * H2));
-            }
+            // lo body: +m^-1 on the linear sums, I_lo^-1 on the angular ones; hi body: -m^-1 and I_hi^-1.
+            // Both are computed without a branch; only free bodies are written (a fixed body's is zero).
+            const float4 Il0 = *reinterpret_cast<const float4*>(Bl + 8);
+            const float2 Il1 = *reinterpret_cast<const float2*>(Bl + 12);
+            const float4 Ih0 = *reinterpret_cast<const float4*>(Bh + 8);
+            const float2 Ih1 = *reinterpret_cast<const float2*>(Bh + 12);
+            const float ml = l1.z, mh = -h1.z;
+            const float nl0 = l0.x + ml * L0, nl1 = l0.y + ml * L1, nl2 = l0.z + ml * L2;
+            const float nl3 = l0.w + fmaf(Il0.x, A0, fmaf(Il0.y, A1, Il0.z * A2));
+            const float nl4 = l1.x + fmaf(Il0.y, A0, fmaf(Il0.w, A1, Il1.x * A2));
+            const float nl5 = l1.y + fmaf(Il0.z, A0, fmaf(Il1.x, A1, Il1.y * A2));
+            const float nh0 = h0.x + mh * L0, nh1 = h0.y + mh * L1, nh2 = h0.z + mh * L2;
+            const float nh3 = h0.w + fmaf(Ih0.x, H0, fmaf(Ih0.y, H1, Ih0.z * H2));
+            const float nh4 = h1.x + fmaf(Ih0.y, H0, fmaf(Ih0.w, H1, Ih1.x * H2));
+            const float nh5 = h1.y + fmaf(Ih0.z, H0, fmaf(Ih1.x, H1, Ih1.y * H2));
+            if (l1.w == 0.0f) { Bl[0] = nl0; Bl[1] = nl1; Bl[2] = nl2; Bl[3] = nl3; Bl[4] = nl4; Bl[5] = nl5; }
+            if (h1.w == 0.0f) { Bh[0] = nh0; Bh[1] = nh1; Bh[2] = nh2; Bh[3] = nh3; Bh[4] = nh4; Bh[5] = nh5; }
         }
         g.sync();
         start = end;
@@ -2464,9 +2462,19 @@ __global__ void __launch_bounds__(kL2 ? kFp32L2Block : kFp32BlockMax, 1) k_solve
         for (;;) {
             const int round_start = sweeps;
             while (res > tol && sweeps < budget) {
-                if (jacobi) s32_sweep_jacobi(g, R, f, rscale, hybrid);
-                else if (!block_team) s32_sweep_lane<G, kL2>(g, f, L, rscale, bodies_global);
-                else s32_sweep<G, kL2>(g, f, L, rscale, bodies_global);
+                if (jacobi) {
+                    s32_sweep_jacobi(g, R, f, rscale, hybrid);
+                } else if (!block_team) {
+                    s32_sweep_lane<G, kL2>(g, f, L, rscale, bodies_global);
+                } else if (!kL2) {
+                    // a block team's slab scene: its levels rarely hold more contacts than a warp has lanes,
+                    // so warp 0 sweeps it one lane per contact (the same bits as four lanes per contact) with
+                    // warp barriers between levels, and the block meets once per sweep
+                    if (threadIdx.x < 32) s32_sweep_lane<WarpGroup, false>(WarpGroup{}, f, L, rscale, false);
+                    g.sync();
+                } else {
+                    s32_sweep<G, kL2>(g, f, L, rscale, bodies_global);
+                }
                 ++sweeps;
                 if (sweeps % interval == 0 || sweeps == budget) {
                     res = s32_residual(a, g, R, f);
