@@ -76,7 +76,9 @@ def tune(world, rb_params, steps=4, rounds=2, memo=True, repeats=3):
     saved state (warm-start cache included) `repeats` times and keeps the median.  The world is left in its
     saved state."""
     import torch
-    key = signature(world) if memo else None
+    # the best shapes depend on the solve's length too (a 100-sweep step is throughput-bound, a long one is
+    # bound by its longest scene), so the memo key holds the sweep cap and the precision
+    key = (signature(world), int(rb_params.max_iterations), int(rb_params.precision)) if memo else None
     if key is not None and key in _memo:
         return dict(_memo[key][0]), _memo[key][1]
     x0, u0 = world.state()

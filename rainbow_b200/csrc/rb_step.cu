@@ -2330,47 +2330,55 @@ __host__ __device__ inline int s32_class(int K, int nb, size_t small_slab, size_
     return s32_bytes(K, nb, true, bodies_global) <= (size_t)kFp32LargeSmem ? 3 : -1;
 }
 
-// Per-scene FP32 bookkeeping of the step, and the scene list of each size class with the larger contact
-// counts first, so that every team's next scene is one of its class and the longest chains start first.
-// One block.
+// Per-scene FP32 bookkeeping of the step, and the scene list of each size class, longest expected chain
+// first, so that every team's next scene is one of its class and the scenes that bound the step start first.
+// The expected chain of a scene is its previous step's levels x sweeps (the solve length in level steps),
+// read before this step resets them; without a plausible history (first step, a scene new to its slot) it is
+// estimated from the contact count.  The order decides only which team takes which scene and when, never a
+// result.  One block.
+constexpr int kClassBuckets = 64;
 __global__ void __launch_bounds__(1024) k_fp32_classes(const StepArgs a, size_t small_slab, size_t mid_slab) {
-    __shared__ int cnt[4 * 32];
+    __shared__ int cnt[4 * kClassBuckets];
     const int S = a.bd.n_scenes;
     // no lists after an overflow: the contact ranges are not valid then, and the solvers do not run
     const bool fp32 = a.pr.precision != RB_PRECISION_FP64 && !a.ws.counters[kAbort];
-    for (int t = threadIdx.x; t < 4 * 32; t += blockDim.x) cnt[t] = 0;
+    const int max_it = a.pr.max_iterations;
+    for (int t = threadIdx.x; t < 4 * kClassBuckets; t += blockDim.x) cnt[t] = 0;
     __syncthreads();
-    auto slot = [&](int s) -> int {   // class x 32 + contact-count bucket (descending), or -1
+    auto slot = [&](int s) -> int {   // class x buckets + expected-chain bucket (descending), or -1
         const SceneRange R = scene_range(a, s);
         const int K = R.c1 - R.c0;
         const int c = s32_class(K, R.b1 - R.b0, small_slab, mid_slab);
         if (c < 0) return -1;
-        const int lg = (int)(3.0f * log2f((float)K + 1.0f));   // buckets of a factor 2^(1/3)
-        return 32 * c + 31 - min(lg, 31);
+        const int Lp = a.ws.nlev[s], Sp = a.ws.sweeps32[s];
+        const bool known = Lp > 0 && Lp <= K && Sp > 0 && Sp <= max_it;
+        const float w = known ? (float)Lp * (float)Sp : 500.0f * (float)K;
+        const int lg = (int)(2.0f * log2f(w + 1.0f));   // buckets of a factor 2^(1/2)
+        return kClassBuckets * c + kClassBuckets - 1 - min(lg, kClassBuckets - 1);
     };
-    for (int s = threadIdx.x; s < S; s += blockDim.x) {
-        a.ws.sweeps32[s] = -1;
-        a.ws.fin32[s] = 0;
-        if (fp32) {
+    if (fp32)
+        for (int s = threadIdx.x; s < S; s += blockDim.x) {
             const int t = slot(s);
             if (t >= 0) atomicAdd(&cnt[t], 1);
         }
-    }
     __syncthreads();
-    if (!fp32) return;
-    if (threadIdx.x == 0) {   // counts -> starts; class ends to the counters
+    if (fp32 && threadIdx.x == 0) {   // counts -> starts; class ends to the counters
         int run = 0;
-        for (int t = 0; t < 4 * 32; ++t) {
+        for (int t = 0; t < 4 * kClassBuckets; ++t) {
             const int n = cnt[t];
             cnt[t] = run;
             run += n;
-            if ((t & 31) == 31) a.ws.counters[kClassEnd32 + (t >> 5)] = run;
+            if ((t % kClassBuckets) == kClassBuckets - 1) a.ws.counters[kClassEnd32 + t / kClassBuckets] = run;
         }
     }
     __syncthreads();
-    for (int s = threadIdx.x; s < S; s += blockDim.x) {
-        const int t = slot(s);
-        if (t >= 0) a.ws.list32[atomicAdd(&cnt[t], 1)] = s;
+    for (int s = threadIdx.x; s < S; s += blockDim.x) {   // the thread that keyed scene s places and resets it
+        if (fp32) {
+            const int t = slot(s);
+            if (t >= 0) a.ws.list32[atomicAdd(&cnt[t], 1)] = s;
+        }
+        a.ws.sweeps32[s] = -1;
+        a.ws.fin32[s] = 0;
     }
 }
 

@@ -179,11 +179,13 @@ class BatchStepper:
     body's shape, mass, inertia, material or forces call :meth:`invalidate`.
     """
 
-    def __init__(self, device="cuda", termination="merit", residual_tolerance=1e-6, residual_interval=1):
+    def __init__(self, device="cuda", termination="merit", residual_tolerance=1e-6, residual_interval=1,
+                 launch_shapes=None):
         self.device = device
         self.termination = termination
         self.residual_tolerance = residual_tolerance
         self.residual_interval = residual_interval
+        self.launch_shapes = launch_shapes   # optional autotune setting (speed only; see rainbow_b200.autotune)
         self.log = []
         self.invalidate()
 
@@ -254,6 +256,9 @@ class BatchStepper:
         t0 = time.perf_counter()
         rp = _step_params(engines[0].params, dt, self.termination, self.residual_tolerance, profiling_on,
                           self.residual_interval)
+        if self.launch_shapes:
+            from .autotune import DEFAULTS, apply
+            apply(rp, {k: v for k, v in self.launch_shapes.items() if k in DEFAULTS})
         world.set_state(self._x, self._u)
         _check_status(world.step(rp))
         x, u = world.state()
