@@ -539,15 +539,16 @@ def run_serving(args, dev, rp_kw, max_it, flush, tuning=None):
                 "workload": "Poisson requests, scenes of 16..2048 bodies (log-uniform; %d distinct), horizons "
                             "U[50,500], boxes/spheres as the batch workload on a 40 x 1 x 40 ground"
                             % len(templates)})
-    # plain: scenes resident at the end of the run (seeded pick), each stepped alone from its current state and
-    # warm-start cache, one rb_step per scene-step, FP64, same solver settings
+    # plain: scenes resident at the end of the run, spread evenly over their body counts (so that the sample's
+    # sizes, and with them its rate, do not depend on which scenes happen to be resident), each stepped alone
+    # from its current state and warm-start cache, one rb_step per scene-step, FP64, same solver settings
     rp64 = W.make_rb_params(params, **dict(rp_kw, precision="fp64"))
     rp64.max_iterations = max_it
     stream = torch.cuda.current_stream()
     b = srv.batch
     resident = sorted([r for r in srv.active if r.done < r.horizon], key=lambda r: r.uid)
-    pick = np.random.default_rng(11).choice(len(resident), size=min(args.serve_plain_scenes, len(resident)),
-                                            replace=False) if resident else []
+    pick = stratified_sample([len(r.scene["body_mass"]) for r in resident], args.serve_plain_scenes) \
+        if resident and args.serve_plain_scenes > 0 else []
     times, last = [], []
     for i in sorted(int(v) for v in pick):
         r = resident[i]
@@ -572,8 +573,9 @@ def run_serving(args, dev, rp_kw, max_it, flush, tuning=None):
         rep["plain"] = {"value": len(times) / (times.sum() / 1000.0), "unit": "scene-steps/s",
                         "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
                         "solve_last_step": solve_summary(last, max_it),
-                        "sample": "%d scenes resident at the end of the run (seeded pick), %d steps each from their "
-                                  "state and warm-start cache, one rb_step per scene-step, FP64"
+                        "bodies_sampled": [len(resident[int(i)].scene["body_mass"]) for i in sorted(pick)],
+                        "sample": "%d scenes resident at the end of the run, stratified by body count, %d steps each "
+                                  "from their state and warm-start cache, one rb_step per scene-step, FP64"
                                   % (len(pick), args.plain_steps)}
         rep["served_vs_plain"] = rep["scene_steps_per_s"] / rep["plain"]["value"] if rep.get("scene_steps_per_s") else None
     return rep
@@ -774,7 +776,7 @@ def run_ours(args):
         best100, info100 = autotune.tune(world, rp_pre)
         t1 = time.perf_counter()
         if cap != pre_cap:
-            best, info = autotune.tune(world, mk(prec, cap), steps=3, repeats=1, rounds=1)
+            best, info = autotune.tune(world, mk(prec, cap), steps=6, repeats=1, rounds=1)
         else:
             best, info = best100, info100
         tuning = dict(best, seconds=time.perf_counter() - t1, **info)

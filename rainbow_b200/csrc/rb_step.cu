@@ -3013,9 +3013,9 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
     const int bg = bd->n_scenes < 148 * 16 ? bd->n_scenes : 148 * 16;
     k_fp32_classes<<<1, 1024, 0, st>>>(a, small_slab, mid_slab); note_launch();
     if (pr->precision != RB_PRECISION_FP64) {
-        // FP32 phase, four size classes side by side: warp teams with 28 KB slabs (8 scenes per SM), warp
-        // teams with 56 KB slabs (4 per SM), block teams with 224 KB (1 per SM), and 512-thread block teams
-        // for the scenes beyond that, whose contact rows stay in L2
+        // FP32 phase, four size classes side by side: warp teams with small slabs (28 KB unless tuned), warp
+        // teams with mid slabs (56 KB), block teams with 224 KB (1 per SM), and 512-thread block teams for the
+        // scenes beyond that, whose contact rows stay in L2
         SideStreams* ss = nullptr;
         rc = side_streams(st, &ss);
         if (rc != RB_OK) return rc;
@@ -3025,12 +3025,14 @@ int rb_step(const rb_shapes* sh, const rb_bodies* bd, const rb_caps* caps, const
             a, kQueueFp32 + 3, kFp32LargeSmem, kFp32LargeSmem); note_launch();
         k_solve_fp32<BlockGroup, false><<<148, kFp32Block, (size_t)kFp32LargeSmem, ss->s[2]>>>(
             a, kQueueFp32 + 2, mid_slab, kFp32LargeSmem); note_launch();
-        // blocks per SM that the shared memory (227 KB) and the threads (2048) allow
-        const int small_per_sm = std::min(16, (227 * 1024) / (4 * small_slab));
-        const int mid_per_sm = std::max(1, std::min(16, (227 * 1024) / (4 * mid_slab)));
-        k_solve_fp32<WarpGroup, false><<<148 * mid_per_sm, kFp32Block, 4 * (size_t)mid_slab, ss->s[1]>>>(
+        // warp teams as one-warp blocks: a team's slab is released as soon as the team finds its queue empty
+        // (in blocks of four teams the slowest held all four slabs), so the small class fills the room the mid
+        // class leaves; as many blocks per SM as the shared memory (227 KB) allows, up to 32
+        const int small_per_sm = std::min(32, (227 * 1024) / small_slab);
+        const int mid_per_sm = std::max(1, std::min(32, (227 * 1024) / mid_slab));
+        k_solve_fp32<WarpGroup, false><<<148 * mid_per_sm, 32, (size_t)mid_slab, ss->s[1]>>>(
             a, kQueueFp32 + 1, small_slab, mid_slab); note_launch();
-        k_solve_fp32<WarpGroup, false><<<148 * small_per_sm, kFp32Block, 4 * (size_t)small_slab, ss->s[0]>>>(
+        k_solve_fp32<WarpGroup, false><<<148 * small_per_sm, 32, (size_t)small_slab, ss->s[0]>>>(
             a, kQueueFp32, 0, small_slab); note_launch();
         for (int c = 0; c < kSideStreams; ++c) {
             cudaEventRecord(ss->join[c], ss->s[c]);
