@@ -2332,9 +2332,9 @@ __host__ __device__ inline int s32_class(int K, int nb, size_t small_slab, size_
 
 // Per-scene FP32 bookkeeping of the step, and the scene list of each size class, longest expected chain
 // first, so that every team's next scene is one of its class and the scenes that bound the step start first.
-// The expected chain of a scene is its previous step's levels x sweeps (the solve length in level steps),
-// read before this step resets them; without a plausible history (first step, a scene new to its slot) it is
-// estimated from the contact count.  The order decides only which team takes which scene and when, never a
+// The expected chain of a scene is its previous step's levels x sweeps (the solve length in level steps,
+// the sweeps floored at half the cap), read before this step resets them; without a plausible history (first
+// step, a scene new to its slot) it is estimated from the contact count.  The order decides only which team takes which scene and when, never a
 // result.  One block.
 constexpr int kClassBuckets = 64;
 __global__ void __launch_bounds__(1024) k_fp32_classes(const StepArgs a, size_t small_slab, size_t mid_slab) {
@@ -2350,9 +2350,11 @@ __global__ void __launch_bounds__(1024) k_fp32_classes(const StepArgs a, size_t 
         const int K = R.c1 - R.c0;
         const int c = s32_class(K, R.b1 - R.b0, small_slab, mid_slab);
         if (c < 0) return -1;
+        // previous levels x sweeps, the sweeps floored at half the cap: whether a scene converges early varies
+        // from step to step, and one that converged last step may run to the cap in this one
         const int Lp = a.ws.nlev[s], Sp = a.ws.sweeps32[s];
         const bool known = Lp > 0 && Lp <= K && Sp > 0 && Sp <= max_it;
-        const float w = known ? (float)Lp * (float)Sp : 500.0f * (float)K;
+        const float w = known ? (float)Lp * (float)max(Sp, max_it / 2) : 0.25f * (float)K * (float)max_it;
         const int lg = (int)(2.0f * log2f(w + 1.0f));   // buckets of a factor 2^(1/2)
         return kClassBuckets * c + kClassBuckets - 1 - min(lg, kClassBuckets - 1);
     };
