@@ -1833,6 +1833,7 @@ constexpr float kFp32Floor = 1e-5f;
 // A round that did not lower the FP64 residual by kS32RoundGain doubles the next round's window (up to
 // kS32StallTestsMax): a scene whose Gauss-Seidel iteration itself has stalled keeps sweeping in FP32 with
 // rare corrections, as FP64 sweeps would stall on it just the same
+constexpr float kS32FarFactor = 100.0f;   // residual / tolerance above which tests are spaced twice as far
 constexpr int kS32StallTests = 16;
 constexpr int kS32StallTestsMax = 512;
 constexpr double kS32RoundGain = 0.9;
@@ -2467,6 +2468,10 @@ __global__ void __launch_bounds__(kL2 ? kFp32L2Block : kFp32BlockMax, 1) k_solve
         float res = s32_residual(a, g, R, f);   // the warm-started iterate may already be good enough
         float best = res;
         int sweeps = 0, stalls = 0, window = kS32StallTests;
+        // far above the tolerance (and the stall floor) the residual is tested half as often: no stop and no
+        // stall can be decided there, and each test rebuilds w
+        auto gap = [&](float r) { return r > kS32FarFactor * tol ? 2 * interval : interval; };
+        int next_test = gap(res);
         double r64 = -1.0;            // FP64 residual of the current iterate, once evaluated
         double r64_round = INFINITY;  // FP64 residual after the previous correction round
         for (;;) {
@@ -2486,8 +2491,9 @@ __global__ void __launch_bounds__(kL2 ? kFp32L2Block : kFp32BlockMax, 1) k_solve
                     s32_sweep<G, kL2>(g, f, L, rscale, bodies_global);
                 }
                 ++sweeps;
-                if (sweeps % interval == 0 || sweeps == budget) {
+                if (--next_test == 0 || sweeps == budget) {
                     res = s32_residual(a, g, R, f);
+                    next_test = gap(res);
                     // a round ends once the residual, already small, stops improving for a while (the FP32
                     // problem's own rounding, or slow progress a defect correction may speed up).  Above the
                     // floor a pause is the Gauss-Seidel iteration itself (it is not monotone), so go on.
@@ -2506,6 +2512,7 @@ __global__ void __launch_bounds__(kL2 ? kFp32L2Block : kFp32BlockMax, 1) k_solve
             r64_round = fmin(r64_round, r64);
             r64 = -1.0;   // the sweeps that follow change the iterate
             res = s32_residual(a, g, R, f);
+            next_test = gap(res);
             best = res;
             stalls = 0;
         }
