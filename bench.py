@@ -775,8 +775,9 @@ def run_ours(args):
         t0 = time.perf_counter()
         best100, info100 = autotune.tune(world, rp_pre)
         t1 = time.perf_counter()
-        if cap != pre_cap:
-            best, info = autotune.tune(world, mk(prec, cap), steps=6, repeats=1, rounds=1)
+        if cap != pre_cap:   # at the cap only the FP32 slabs matter: tuned over the timed horizon
+            best, info = autotune.tune(world, mk(prec, cap), steps=args.steps, repeats=1, rounds=1,
+                                       start=best100, knobs=("fp32_small_slab", "fp32_mid_slab"))
         else:
             best, info = best100, info100
         tuning = dict(best, seconds=time.perf_counter() - t1, **info)

@@ -71,14 +71,16 @@ def signature(world):
     return (world.n_scenes, int(round(np.log(max(world.n_bodies, 1)) * 100)), int(nb.max()))
 
 
-def tune(world, rb_params, steps=4, rounds=2, memo=True, repeats=3):
+def tune(world, rb_params, steps=4, rounds=2, memo=True, repeats=3, start=None, knobs=None):
     """Fastest launch shapes for `world` stepped with `rb_params`: a trial times `steps` steps from the same
-    saved state (warm-start cache included) `repeats` times and keeps the median.  The world is left in its
-    saved state."""
+    saved state (warm-start cache included) `repeats` times and keeps the median.  ``start`` is the setting
+    the descent starts from (the defaults otherwise) and ``knobs`` the knobs it varies (all otherwise).  The
+    world is left in its saved state."""
     import torch
     # the best shapes depend on the solve's length too (a 100-sweep step is throughput-bound, a long one is
     # bound by its longest scene), so the memo key holds the sweep cap and the precision
-    key = (signature(world), int(rb_params.max_iterations), int(rb_params.precision)) if memo else None
+    key = (signature(world), int(rb_params.max_iterations), int(rb_params.precision), steps,
+           tuple(sorted((start or {}).items())), tuple(knobs or ())) if memo else None
     if key is not None and key in _memo:
         return dict(_memo[key][0]), _memo[key][1]
     x0, u0 = world.state()
@@ -113,7 +115,8 @@ def tune(world, rb_params, steps=4, rounds=2, memo=True, repeats=3):
             times.append(e0.elapsed_time(e1) / steps)
         return float(np.median(times))
 
-    best, best_ms, n = coordinate_descent(cost, rounds=rounds)
+    cands = {k: v for k, v in CANDIDATES.items() if knobs is None or k in knobs}
+    best, best_ms, n = coordinate_descent(cost, start=start, candidates=cands, rounds=rounds)
     restore()
     info = {"ms_per_step": best_ms, "default_ms_per_step": cost(DEFAULTS), "trials": n}
     restore()
