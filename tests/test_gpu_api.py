@@ -109,3 +109,30 @@ def test_simulate_batch_matches_each_engine_stepped_alone():
                     [(c.bodyA.name, c.bodyB.name) for c in ea.contact_points])
             contacts += len(eb.contact_points)
     assert contacts > 0
+
+
+def test_engines_with_device_grids_step_like_their_arrays():
+    """Scenes whose grids live on the device (the per-body workload builds them there) go through
+    engine_io.engine_from_arrays and api.simulate_batch without a host copy of the grids (each engine's grids
+    are views of the workload's tensor) and step bit for bit like the same arrays given to DeviceWorld."""
+    import torch
+    from rainbow_b200 import api as API, engine_io, scenes, world as W
+    from rainbow_b200.stepper import BatchStepper
+    arrays, params = scenes.batch_arrays_per_body(n_scenes=1024, seed=0, resolution=32, device="cuda:0",
+                                                  select=[3, 11])
+    engines = [engine_io.engine_from_arrays(a) for a in arrays]
+    grid = next(iter(engines[0].shapes.values())).grid.values
+    assert isinstance(grid, torch.Tensor) and grid.is_cuda
+    back = engine_io.scene_arrays(engines[0])
+    assert isinstance(back["shape_grid"], torch.Tensor) and back["shape_grid"].is_cuda
+    world = W.DeviceWorld(arrays, device="cuda:0", max_iterations=100)
+    rp = W.make_rb_params(params)
+    stepper = BatchStepper()
+    for _ in range(5):
+        assert world.step(rp) == 0
+        API.simulate_batch(engines, engines[0].params.time_step, stepper)
+    x, u = world.state()
+    xb = np.concatenate([engine_io.body_state(e)[0] for e in engines])
+    ub = np.concatenate([engine_io.body_state(e)[1] for e in engines])
+    np.testing.assert_array_equal(xb, x)
+    np.testing.assert_array_equal(ub, u)
