@@ -1,7 +1,7 @@
 """GPU step (through the C ABI) against the reference's recorded steps and against the oracle.
 
 FP64 parity target: bit-identical contact sets (body indices, positions, normals, gaps), solver impulses,
-iteration counts and body states.  The north-star bound is 1e-9 relative; the kernels reproduce NumPy's
+iteration counts and body states.  The required bound is 1e-9 relative; the kernels reproduce NumPy's
 rounding sequence, so the tests demand exact equality."""
 import numpy as np
 import pytest
