@@ -211,3 +211,78 @@ def test_simulate_batch_refuses_engines_with_different_parameters():
     with pytest.raises(ValueError):
         A.simulate_batch([a, b], 0.0, BatchStepper())
 
+
+
+def test_batch_stepper_host_state_traffic(monkeypatch):
+    """BatchStepper's host side against a stand-in world: the state it uploads holds every body's current
+    r, q, v, w (arrays edited in place and arrays replaced since the last step alike), the bodies receive the
+    world's new state as their own arrays, each engine gets its own contact points (scene-local body indices),
+    and adding a body to an engine rebuilds the batch."""
+    from rainbow_b200 import api as A, stepper as ST, world as W
+
+    class FakeWorld:
+        built = 0
+
+        def __init__(self, arrays, device=None, max_iterations=None):
+            FakeWorld.built += 1
+            self.scene_start = np.concatenate([[0], np.cumsum([len(a["body_mass"]) for a in arrays])])
+            self.n = int(self.scene_start[-1])
+            self.uploaded = None
+
+        def set_state(self, x, u):
+            self.uploaded = (np.array(x, copy=True), np.array(u, copy=True))
+
+        def step(self, rp):
+            return 0
+
+        def state(self):
+            x, u = self.uploaded
+            return x + 1.0, u + 2.0   # a recognisable "new" state
+
+        def contacts(self):
+            # one contact in each scene, between its first two bodies
+            ids = np.array([[int(s0), int(s0) + 1] for s0 in self.scene_start[:-1]], dtype=np.int32)
+            K = len(ids)
+            return dict(ids=ids, p=np.zeros((K, 3)), n=np.tile([0.0, 1.0, 0.0], (K, 1)), g=np.zeros(K),
+                        sol=np.zeros(4 * K))
+
+    monkeypatch.setattr(W, "DeviceWorld", FakeWorld)
+    monkeypatch.setattr(ST, "_check_status", lambda s: s)
+    engines = [engine_io.engine_from_arrays(load_fixture("boxes8")) for _ in range(2)]
+    before = [engine_io.body_state(e) for e in engines]
+    bs = ST.BatchStepper()
+    A.simulate_batch(engines, engines[0].params.time_step, bs)
+    world = bs._world
+    x0 = np.concatenate([b[0] for b in before])
+    np.testing.assert_array_equal(world.uploaded[0], x0)
+    for e, (x, u) in zip(engines, before):
+        xn, un = engine_io.body_state(e)
+        np.testing.assert_array_equal(xn, x + 1.0)
+        np.testing.assert_array_equal(un, u + 2.0)
+        ids, _, _, _ = e.contact_points.arrays()
+        np.testing.assert_array_equal(ids, [[0, 1]])
+        names = list(e.bodies)
+        assert (e.contact_points[0].bodyA.name, e.contact_points[0].bodyB.name) == (names[0], names[1])
+    # edit one body's velocity in place and replace another's spin: the next upload carries both
+    b1 = list(engines[1].bodies.values())[3]
+    b1.v[0] += 0.25
+    b2 = list(engines[0].bodies.values())[2]
+    b2.w = np.array([0.0, 0.5, 0.0])
+    v_edited = b1.v.copy()
+    A.simulate_batch(engines, engines[0].params.time_step, bs)
+    assert bs._world is world and FakeWorld.built == 1
+    n0 = len(engines[0].bodies)
+    np.testing.assert_array_equal(world.uploaded[1][n0 + 3, :3], v_edited)
+    np.testing.assert_array_equal(world.uploaded[1][2, 3:], [0.0, 0.5, 0.0])
+    np.testing.assert_array_equal(b2.w, [2.0, 2.5, 2.0])   # and the step's result went back into the body
+    # a body added to an engine: the batch is rebuilt from the engines
+    from rainbow_b200.types import RigidBody
+    extra = RigidBody("extra")
+    src = list(engines[0].bodies.values())[1]
+    for f in ("shape", "mass", "inertia", "is_fixed", "material", "forces"):
+        setattr(extra, f, getattr(src, f))
+    extra.idx = len(engines[0].bodies)
+    extra.r, extra.q, extra.v, extra.w = src.r + 5.0, src.q.copy(), src.v.copy(), src.w.copy()
+    engines[0].bodies[extra.name] = extra
+    A.simulate_batch(engines, engines[0].params.time_step, bs)
+    assert FakeWorld.built == 2 and bs._world.n == sum(len(e.bodies) for e in engines)
