@@ -10,6 +10,13 @@ namespace rb {
 
 constexpr int kMaxClustersPerShape = 512;   // 16384 triangles per shape (mid-phase cluster masks in shared memory)
 constexpr int kScanBlocks = 1024;           // partial sums of the device-wide scans
+// Strides of the compact FP32 records.  A contact record (12 floats per row, 4 rows) is padded to an odd
+// number of float4s (13), so the 128-bit row loads of eight lanes reading eight different contacts fall on
+// eight different groups of four shared-memory banks (with 12 float4s every other contact shared its banks:
+// 4-way conflicts once a level holds several contacts).  Body records (w, m^-1, fixed, I^-1) are read two
+// per contact and often the same body by several lanes; padding them did not pay.
+constexpr int kS32Floats = 52;               // floats per contact record (48 used)
+constexpr int kS32BodyFloats = 16;           // floats per body record
 
 struct Workspace {
     // per body
@@ -44,7 +51,7 @@ struct Workspace {
     int32_t* bc_list;    // 2K
     double* J;           // 48K
     double* WJT;         // 48K
-    float* c32;          // 48K   compact FP32 contacts of the scenes whose copy does not fit in shared memory
+    float* c32;          // 52K   compact FP32 contacts of the scenes whose copy does not fit in shared memory
     uint32_t* blist32;   // 2K    ... their per-body contact lists
     uint16_t* pos32;     // K     ... and level-order positions
     float* body32;       // 16N   ... and, for scenes with too many bodies for the slab, their body records
@@ -98,7 +105,8 @@ inline size_t layout(Workspace* ws, char* base, int64_t N, int64_t NV, int64_t N
     take(w->item_pair, C); take(w->item_tri, C); take(w->item_flag, C);
     take(w->item_p, 3 * C); take(w->item_n, 3 * C); take(w->item_g, C);
     take(w->lohi, 2 * K); take(w->c_scene, K); take(w->bc_list, 2 * K);
-    take(w->J, 48 * K); take(w->WJT, 48 * K); take(w->c32, 48 * K); take(w->blist32, 2 * K); take(w->pos32, K); take(w->body32, 16 * N);
+    take(w->J, 48 * K); take(w->WJT, 48 * K); take(w->c32, (size_t)kS32Floats * K); take(w->blist32, 2 * K); take(w->pos32, K);
+    take(w->body32, (size_t)kS32BodyFloats * N);
     take(w->b, 4 * K); take(w->diag, 4 * K); take(w->r, 4 * K); take(w->x, 4 * K); take(w->xold, 4 * K);
     take(w->mu, K);
     take(w->ckey, 2 * K);

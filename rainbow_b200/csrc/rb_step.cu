@@ -1805,21 +1805,19 @@ __device__ void solve_scene_body(const StepArgs& a, const G& g, int s, int post,
 //
 // Compact form.  A contact's Jacobian rows are [lin_lo | ang_lo | lin_hi | ang_hi] with lin_hi = -lin_lo
 // (the frame direction, zero on the torsion row) and W J^T = (m^-1 lin, I_w^-1 ang) per body, so a contact
-// stores per row q: lin_lo (3), ang_lo (3), ang_hi (3), b, 1/diag and x -- 12 floats, 48 per contact
-// (192 bytes; the torsion row's unused lin slot holds mu) -- and a body stores its accumulator w (6), m^-1,
-// a fixed flag and the world inverse inertia (6, symmetric): 16 floats.  The update of w after a contact
-// changes by dx is m^-1 sum_q lin_q dx_q (negated on the hi side) and I^-1 sum_q ang_q dx_q.
+// stores per row q: lin_lo (3), ang_lo (3), ang_hi (3), b, 1/diag and x -- 12 floats, 48 per contact (the
+// torsion row's unused lin slot holds mu), in a record of kS32Floats -- and a body stores its accumulator
+// w (6), m^-1, a fixed flag and the world inverse inertia (6, symmetric), in a record of kS32BodyFloats
+// (m^-1 = I^-1 = 0 for a fixed body).  The update of w after a contact changes by dx is m^-1 sum_q lin_q dx_q
+// (negated on the hi side) and I^-1 sum_q ang_q dx_q.
 //
-// Execution.  Four lanes share a contact (lane q computes row q's J w; the four z values meet by shuffles;
-// every lane applies the prox; the three sums of the update are reduced over the quad and each lane writes
-// one of the four 3-vectors).  A team -- one warp for scenes of up to kS32WarpSlab bytes, a 128-thread block
-// above -- takes scenes from a queue and synchronises between levels.  Three launches cover three size
-// classes (warp teams with small and large slabs, block teams) and run concurrently on separate streams.
+// Execution.  A team -- one warp for scenes of up to the mid slab, a 128-thread block above, a 512-thread
+// block for the scenes whose rows stay in L2 -- takes scenes from its size class's queue; the slab scenes are
+// swept one lane per contact (s32_sweep_lane, by warp 0 in a block team), the L2 scenes four lanes per
+// contact (s32_sweep).  The four classes' launches run concurrently on separate streams.
 // ---------------------------------------------------------------------------------------------------------
-constexpr int kS32Floats = 48;                       // floats per contact
 constexpr int kQueueFp32 = 5;                        // counters[5..8]: scene queues of the four size classes
 constexpr int kClassEnd32 = 9;                       // counters[9..12]: end of each class's range in list32
-constexpr int kS32BodyFloats = 16;                   // floats per body
 constexpr int kFp32Block = 128;                      // threads per block of the FP32 launches
 constexpr int kFp32BlockMax = 256;                   // ... at most, in the launches for slab scenes
 constexpr int kFp32L2Block = 512;                    // threads of the launch for the scenes beyond any slab
@@ -1841,7 +1839,7 @@ constexpr double kS32RoundGain = 0.9;
 struct S32Scene {
     float* c;          // kS32Floats per contact, in level order; row q at 12 q as three float4 groups
                        // (lin[3], b | ang_lo[3], 1/diag | ang_hi[3], x); the torsion row's lin is (mu, 0, 0)
-    float* body;       // kS32BodyFloats per body: w[6], m^-1, fixed, I^-1 (xx, xy, xz, yy, yz, zz), pad[2]
+    float* body;       // kS32BodyFloats per body: w[6], m^-1, fixed, I^-1 (xx, xy, xz, yy, yz, zz), padding
     uint32_t* lohi;    // per contact in level order: scene-local lo | hi << 16
     uint16_t* pos;     // level-order position of each contact (scene-local contact index -> position)
     uint16_t* lptr;    // level starts (L + 1)
@@ -2457,7 +2455,7 @@ __global__ void __launch_bounds__(kL2 ? kFp32L2Block : kFp32BlockMax, 1) k_solve
         const S32Scene f = s32_carve(my_slab, K, nb, kL2 ? &a : nullptr, R.c0, bodies_global, R.b0);
         // scratch for the level relaxation: the rows' room of the slab, or with rows in L2 what the slab has left
         int16_t* scratch = nullptr;
-        if (!kL2) {   // 192 bytes per contact there, more than s32_level_scratch needs
+        if (!kL2) {   // a contact record's bytes per contact there, more than s32_level_scratch needs
             scratch = reinterpret_cast<int16_t*>(f.c);
         } else {
             const size_t off = (s32_bytes(K, nb, true, bodies_global) + 15) & ~size_t(15);
