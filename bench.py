@@ -45,13 +45,13 @@ sys.path.insert(0, ROOT)
 
 # DRAM bytes of a phase's kernels per step, from ncu captures of this build (dram__bytes_read.sum +
 # dram__bytes_write.sum), keyed by the phase's kernel and the (workload, precision, sweep cap) they hold for.
-# k_solve_fp32: 6.67 MB for the four size-class launches of one step of the first 128 scenes (3343 contacts),
+# k_solve_fp32: 5.84 MB for the four size-class launches of one step of the first 128 scenes (3343 contacts),
 # scaled by contacts to the 1024-scene step (78,787 contacts): the traffic is the per-contact copy-in, the FP64
 # corrections and the write-back, all proportional to the contacts.
 # k_narrow: 66.1 MB for one launch on the first 128 scenes (152,968 candidates) with a grid per body, scaled by
 # candidates to the 1024-scene step (4,374,974 candidates).
 PROFILED_DRAM_BYTES = {
-    "k_solve_fp32": (157_000_000, ("batch_1024_scenes_shape_per_body", "fp32_refine", 4000)),
+    "k_solve_fp32": (138_000_000, ("batch_1024_scenes_shape_per_body", "fp32_refine", 4000)),
     "k_narrow": (1_890_000_000, ("batch_1024_scenes_shape_per_body", "fp32_refine", 4000)),
 }
 EQUAL_RESIDUAL_SWEEPS = 4000   # default sweep cap of the equal-residual measurement
