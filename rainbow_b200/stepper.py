@@ -244,8 +244,13 @@ class BatchStepper:
         return True
 
     def step(self, dt, engines, profiling_on=False):
-        """Advance every engine by dt (steppers.py:47 SemiImplicitStepper.step, for all of them at once)."""
+        """Advance every engine by dt (steppers.py:47 SemiImplicitStepper.step, for all of them at once).
+        An engine without bodies only gets an empty contact list, as the reference stepper gives it."""
         engines = list(engines)
+        for e in engines:
+            if not e.bodies:
+                e.contact_points = []
+        engines = [e for e in engines if e.bodies]
         if not engines:
             return
         if (self._world is None or len(engines) != len(self._engines)

@@ -286,3 +286,10 @@ def test_batch_stepper_host_state_traffic(monkeypatch):
     engines[0].bodies[extra.name] = extra
     A.simulate_batch(engines, engines[0].params.time_step, bs)
     assert FakeWorld.built == 2 and bs._world.n == sum(len(e.bodies) for e in engines)
+    # an engine without bodies is left out of the batch and gets an empty contact list
+    from rainbow_b200.types import Engine
+    empty = Engine()
+    empty.params = engines[0].params
+    empty.contact_points = None
+    A.simulate_batch(engines + [empty], engines[0].params.time_step, bs)
+    assert empty.contact_points == [] and bs._world.n == sum(len(e.bodies) for e in engines)
