@@ -12,7 +12,7 @@ import numpy as np
 
 # knob -> candidate values (0 would mean the built-in default)
 CANDIDATES = {
-    "fp32_small_slab": [12288, 16384, 20480, 28672, 40960],
+    "fp32_small_slab": [8192, 12288, 16384, 20480, 28672, 40960],
     "fp32_mid_slab": [40960, 49152, 57344],
     "mid_blocks": [148 * 4, 148 * 8, 148 * 16, 148 * 32],
     "narrow_blocks": [148 * 4, 148 * 8, 148 * 16],
