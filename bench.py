@@ -54,6 +54,8 @@ PROFILED_DRAM_BYTES = {
     "k_solve_fp32": (138_000_000, ("batch_1024_scenes_shape_per_body", "fp32_refine", 4000)),
     "k_narrow": (1_890_000_000, ("batch_1024_scenes_shape_per_body", "fp32_refine", 4000)),
 }
+# the phases rb_profile_times reports, in its order
+PHASE_NAMES = ["bodies_bvh", "pairs_candidates", "contact_search", "dedup", "contact_setup_solve", "integrate", "total"]
 EQUAL_RESIDUAL_SWEEPS = 4000   # default sweep cap of the equal-residual measurement
 
 
@@ -842,7 +844,15 @@ def run_ours(args):
         t100, _, c100, _, after100 = batched_arm(world, rps["mode100"], args.steps, args.warmup, restore, flush, local)
         v100 = world.n_scenes * args.steps / (t100.sum() / 1000.0)
         p100 = plain_arm(world, arrays, sample, x0, u0, cache, rps["fp64_100"], args.plain_steps, flush, pre_cap)
+        rp100p = mk(prec, pre_cap, True)      # one profiled step from the saved state: the phase times
+        if tuning:
+            from rainbow_b200 import autotune
+            autotune.apply(rp100p, best100)
+        restore()
+        world.step(rp100p)
+        ph100 = world.profile_times()
         at100 = {"max_iterations": pre_cap, "value": v100, "unit": "scene-steps/s",
+                 "phases_ms_first_step": {k: v * 1000.0 for k, v in zip(PHASE_NAMES, ph100)},
                  "ms_per_step": float(t100.mean()), "p50_ms": float(np.percentile(t100, 50)),
                  "p99_ms": float(np.percentile(t100, 99)), "solve_last_step": solve_summary(after100, pre_cap),
                  "plain": p100, "speedup_vs_plain": v100 / p100["value"],
@@ -1000,8 +1010,7 @@ def run_ours(args):
         "equal_residual": equal,
         "at_100_sweeps": at100,
         "roofline": doms[dom], "roofline_phases": doms,
-        "phases_ms": {k: v * 1000.0 for k, v in zip(["bodies_bvh", "pairs_candidates", "contact_search", "dedup",
-                                                     "contact_setup_solve", "integrate", "total"], phases)},
+        "phases_ms": {k: v * 1000.0 for k, v in zip(PHASE_NAMES, phases)},
         "serving": serving_rep,
         "configs": configs,
         "cpu_baseline": cpu,
